@@ -1,0 +1,143 @@
+/*
+ * picomax.h - C-ABI of the B200 implementation of PicoMax's two hot stages:
+ * the EPM band solve and the chi(q, w) local-field accumulation.
+ *
+ * The reference exposes no library API: its only interface is the `picomax`
+ * executable (argv in, binary .dat/.gpt files out). These entry points are
+ * the functions that executable is built from, one per reference stage, with
+ * plain pointers and sizes. A status code replaces the reference's abort().
+ *
+ * Host buffers are caller-owned. Device work is ordered on the context's
+ * stream; every call below returns after its results are in the caller's
+ * buffers unless the name ends in _async.
+ */
+#ifndef PICOMAX_B200_H_
+#define PICOMAX_B200_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  PMX_OK = 0,
+  PMX_ERR_INVALID = 1,     /* bad argument or option (reference: abort()) */
+  PMX_ERR_CUDA = 2,        /* CUDA runtime error */
+  PMX_ERR_NOCONV = 3,      /* eigensolver did not converge (reference: abort() at src/pmx_epm.cpp:233) */
+  PMX_ERR_TIMEOUT = 4,     /* a bounded device wait ran out */
+  PMX_ERR_NO_DEVICE = 5,   /* no CUDA device: this library has no CPU path */
+  PMX_ERR_UNSUPPORTED = 6  /* input outside what this build implements */
+} pmx_status;
+
+typedef enum { PMX_SWITCH_NONE = 0, PMX_SWITCH_BAND = 1, PMX_SWITCH_EPSIJ = 2, PMX_SWITCH_EPSLL = 3 } pmx_switch;
+typedef enum { PMX_PREC_FP64 = 0, PMX_PREC_MIXED = 1 } pmx_precision;
+
+typedef struct pmx_problem pmx_problem; /* parsed picomax invocation (host) */
+typedef struct pmx_ctx pmx_ctx;         /* device context: stream, workspaces */
+
+typedef struct {
+  int npw;        /* plane waves N_G (NPW) */
+  int nh;         /* reference Hamiltonian dimension 2 N_G */
+  int soc;        /* 1 when any spin-orbit form factor is non-zero */
+  int neps;       /* local-field G count (NEPS) */
+  int nband;      /* NBAND */
+  int nvalence;   /* -nvalence */
+  int nk;         /* k-points (NKPT) */
+  int nq;         /* q-points (NQ) */
+  int nfreq;      /* NFREQ */
+  int natom;      /* NATOM */
+  int sw;         /* pmx_switch from -switch */
+  int debug;      /* -debug level */
+  int kk;         /* -kk */
+  int delta;      /* -delta */
+  double epsilon; /* -epsilon, eV */
+  double dfreq;   /* -dfreq, eV */
+  double a;       /* lattice constant, Angstrom */
+  double gcut;    /* cutoff in 2 pi / a */
+  double bz_volume;
+  long long chi_values; /* doubles in one of the Re/Im blocks of the chi .dat */
+} pmx_problem_info;
+
+/* ---------------------------------------------------------------- problem */
+
+/* Parses argv exactly as the reference does and builds the G list, loci table
+ * and k/q lists. Replaces inputParser + inputProcess + init_crystal +
+ * init_mater + generate_gpt/_rect + generate_loci + import_kpt/generate_kpt_*
+ * (src/pmx.hpp:190-245, src/pmx_io.cpp:108-503, src/pmx_basis.cpp:29-355,
+ * called from src/pmx.cpp:64-156). argv[0] is the program name. */
+int pmx_problem_create(int argc, const char* const* argv, pmx_problem** out);
+void pmx_problem_destroy(pmx_problem* p);
+int pmx_problem_get_info(const pmx_problem* p, pmx_problem_info* info);
+/* G vectors [npw][3] (units 2 pi / a) and their integer coordinates [npw][3];
+ * the order is the reference's (src/pmx_basis.cpp:54-80). Either may be NULL. */
+int pmx_problem_gvectors(const pmx_problem* p, double* G, int* hkl);
+/* loci[m][p] = index of G_p + G_m or -1, [neps][npw] (src/pmx_basis.cpp:142-179). */
+int pmx_problem_loci(const pmx_problem* p, int* loci);
+/* k-points [nk][3] and weights [nk] (src/pmx_basis.cpp:200-650). */
+int pmx_problem_kpoints(const pmx_problem* p, double* K, double* KW);
+/* q-points [nq][3] (src/pmx_io.cpp:255-309). */
+int pmx_problem_qpoints(const pmx_problem* p, double* Q);
+/* Writes the text of `-debug 2/3` (printInput, src/pmx_io.cpp:510-614) to buf
+ * (NUL-terminated, truncated at len). Returns the full length in *needed. */
+int pmx_problem_dump(const pmx_problem* p, char* buf, size_t len, size_t* needed);
+/* Writes ${wdir}/${out}.gpt (export_gpt, src/pmx_io.cpp:816-826). */
+int pmx_problem_write_gpt(const pmx_problem* p);
+
+/* ---------------------------------------------------------------- context */
+
+int pmx_ctx_create(int device, pmx_ctx** out);
+void pmx_ctx_destroy(pmx_ctx* ctx);
+/* Message of the last failing call on this context (NUL-terminated). */
+const char* pmx_ctx_last_error(const pmx_ctx* ctx);
+/* Device time of the stages of the last call, milliseconds:
+ * [0] H assembly + eigensolves, [1] overlaps, [2] contraction, [3] scaling + KK,
+ * [4] host<->device copies. Entries not run are 0. */
+int pmx_ctx_stage_times(const pmx_ctx* ctx, double* ms5);
+/* Launch count of this library's kernels since the context was created. */
+long long pmx_ctx_kernel_launches(const pmx_ctx* ctx);
+
+/* ---------------------------------------------------------------- stage 1 */
+
+/* Hamiltonian H(k) of every k in kpts [nk][3], full Hermitian storage,
+ * column-major, complex interleaved: out [nk][nh][nh][2] with nh = 2 npw
+ * (the spinor matrix of HamiltonianEPM, src/pmx_epm.cpp:56-153). */
+int pmx_hamiltonian(pmx_ctx* ctx, const pmx_problem* p, const double* kpts, int nk, double* out);
+
+/* Lowest nev eigenvalues (ascending) and optionally eigenvectors of a batch of
+ * Hermitian matrices A [batch][n][n][2] (column-major, complex interleaved).
+ * w [batch][nev]; z [batch][nev][n][2] or NULL. Replaces the
+ * Eigen::SelfAdjointEigenSolver calls at src/pmx_epm.cpp:232 and :402. */
+int pmx_heev_batched(pmx_ctx* ctx, int n, int batch, const double* A, int nev, double* w, double* z);
+
+/* Energy reference: midpoint of eigenvalues nvalence-1 and nvalence at
+ * -refpoint (setRefEnergy, src/pmx_epm.cpp:393-428). */
+int pmx_ref_energy(pmx_ctx* ctx, const pmx_problem* p, double* offset_eV);
+
+/* Band energies eband [nq][nband] in eV relative to the reference energy
+ * (empiricalpseudopotentialmethod, src/pmx_epm.cpp:219-253). */
+int pmx_band(pmx_ctx* ctx, const pmx_problem* p, double* eband);
+
+/* ---------------------------------------------------------------- stage 2 */
+
+/* Susceptibility of -switch epsij (chi_tensor, src/pmx_chi.cpp:319-713) or
+ * epsLL (chi_LL, src/pmx_chi_copy.cpp:320-676), including the Kramers-Kronig
+ * step when -kk 1. re/im each hold info.chi_values doubles in .dat order
+ * [i][j][q][m][n<=m][f]. precision: PMX_PREC_FP64 or PMX_PREC_MIXED. */
+int pmx_chi(pmx_ctx* ctx, const pmx_problem* p, int sw, int precision, double* re, double* im);
+
+/* Kramers-Kronig transform of nrows spectra in place, re/im [nrows][nfreq],
+ * w_f = dfreq f (kramerskronigtransform, src/pmx_chi.cpp:272-309). */
+int pmx_kk(pmx_ctx* ctx, int nrows, int nfreq, double dfreq, double* re, double* im);
+
+/* ---------------------------------------------------------------- driver */
+
+/* The whole picomax program: the reference main (src/pmx.cpp:43-206) plus
+ * the epsLL dispatch (src_bkp/pmx.cpp:206-222). Returns the exit code. */
+int pmx_main(int argc, const char* const* argv);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PICOMAX_B200_H_ */

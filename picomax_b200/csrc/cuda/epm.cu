@@ -1,0 +1,497 @@
+// Stage 1 kernels: H(k) assembly and the batched FP64 Hermitian eigensolver.
+//
+// H(k) follows HamiltonianEPM (src/pmx_epm.cpp:56-153): kinetic diagonal
+// KCON (2pi/a)^2 |k+G_i|^2, local pseudopotential V(G_i-G_j) off the diagonal,
+// and the spin-orbit block i VSO(G_j-G_i) ((k+G_j) x (k+G_i)) . sigma placed
+// at (2i, 2j) for j <= i. The reference only fills the lower triangle and its
+// eigensolver reads that triangle; here the upper triangle is written as the
+// conjugate transpose of the lower one, which is the matrix the reference
+// diagonalises.
+//
+// The eigensolver replaces Eigen::SelfAdjointEigenSolver (called at
+// src/pmx_epm.cpp:232, :402, src/pmx_chi.cpp:388, :476). One CTA owns one
+// matrix: Householder tridiagonalisation with the rank-2 update of step j-1
+// fused into the matrix-vector pass of step j (one read+write of the trailing
+// block per step), multisection bisection for the lowest nev eigenvalues,
+// inverse iteration with reorthogonalisation inside eigenvalue clusters for
+// the tridiagonal eigenvectors, then the back-transform by the stored
+// reflectors. Only the eigenpairs the caller needs are formed.
+#include <cfloat>
+#include <cmath>
+
+#include "pmx_common.cuh"
+#include "pmx_device.hpp"
+
+namespace pmx {
+namespace dev {
+
+// ------------------------------------------------------------------ assembly
+__global__ void __launch_bounds__(256) assemble_kernel(const CrystalDev* __restrict__ crystals,
+                                                       const EigItem* __restrict__ items,
+                                                       double2* __restrict__ hbuf) {
+  const EigItem it = items[blockIdx.y];
+  const CrystalDev C = crystals[it.crystal];
+  const int npw = C.npw, n = it.n, side = C.side, off = 2 * C.imax;
+  double2* H = hbuf + it.h_off;
+  const double kx = it.k[0], ky = it.k[1], kz = it.k[2];
+  const long long total = (long long)npw * npw;
+  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(idx % npw), j = (int)(idx / npw);
+    // (a, b) is the lower-triangle block this entry derives from.
+    const bool lower = i >= j;
+    const int a = lower ? i : j, b = lower ? j : i;
+    double2 h0;
+    if (a == b) {
+      const double gx = kx + C.G[3 * a], gy = ky + C.G[3 * a + 1], gz = kz + C.G[3 * a + 2];
+      h0 = make_double2(C.kin * ((gx * gx + gy * gy) + gz * gz), 0.0);
+    } else {
+      const int dh = C.hkl[3 * a] - C.hkl[3 * b] + off, dk = C.hkl[3 * a + 1] - C.hkl[3 * b + 1] + off,
+                dl = C.hkl[3 * a + 2] - C.hkl[3 * b + 2] + off;
+      h0 = C.vloc[((long long)dh * side + dk) * side + dl];
+    }
+    if (!C.soc) {
+      H[(long long)j * n + i] = lower ? h0 : cconj(h0);
+      continue;
+    }
+    // spin-orbit block of the lower pair (a, b): q = G_b - G_a
+    double2 blk[2][2];
+    blk[0][0] = h0;
+    blk[1][1] = h0;
+    blk[0][1] = make_double2(0, 0);
+    blk[1][0] = make_double2(0, 0);
+    if (a != b) {
+      const int dh = C.hkl[3 * b] - C.hkl[3 * a] + off, dk = C.hkl[3 * b + 1] - C.hkl[3 * a + 1] + off,
+                dl = C.hkl[3 * b + 2] - C.hkl[3 * a + 2] + off;
+      const double2 vso = C.vso[((long long)dh * side + dk) * side + dl];
+      if (vso.x != 0.0 || vso.y != 0.0) {
+        const double ax = kx + C.G[3 * a], ay = ky + C.G[3 * a + 1], az = kz + C.G[3 * a + 2];
+        const double bx = kx + C.G[3 * b], by = ky + C.G[3 * b + 1], bz = kz + C.G[3 * b + 2];
+        // (k+G_b) x (k+G_a)
+        const double cx = by * az - bz * ay, cy = bz * ax - bx * az, cz = bx * ay - by * ax;
+        const double2 iv = make_double2(-vso.y, vso.x);  // i * VSO
+        const double2 sx = cscale(iv, cx), sy = cscale(iv, cy), sz = cscale(iv, cz);
+        blk[0][0] = cadd(blk[0][0], sz);
+        blk[1][1] = csub(blk[1][1], sz);
+        blk[0][1] = make_double2(sx.x + sy.y, sx.y - sy.x);  // Sx - i Sy
+        blk[1][0] = make_double2(sx.x - sy.y, sx.y + sy.x);  // Sx + i Sy
+      }
+    }
+    double2* col0 = H + (long long)(2 * j) * n + 2 * i;
+    double2* col1 = col0 + n;
+    if (lower) {
+      col0[0] = blk[0][0];
+      col0[1] = blk[1][0];
+      col1[0] = blk[0][1];
+      col1[1] = blk[1][1];
+    } else {  // H[2i+s, 2j+t] = conj(block_(j,i)[t][s])
+      col0[0] = cconj(blk[0][0]);
+      col0[1] = cconj(blk[0][1]);
+      col1[0] = cconj(blk[1][0]);
+      col1[1] = cconj(blk[1][1]);
+    }
+  }
+}
+
+cudaError_t launch_assemble(const CrystalDev* crystals, const EigItem* items, int nitems, int max_npw,
+                            double2* hbuf, cudaStream_t st) {
+  if (nitems <= 0) return cudaSuccess;
+  long long total = (long long)max_npw * max_npw;
+  int bx = (int)((total + 255) / 256);
+  if (bx > 512) bx = 512;
+  dim3 grid(bx, nitems);
+  assemble_kernel<<<grid, 256, 0, st>>>(crystals, items, hbuf);
+  return cudaGetLastError();
+}
+
+// --------------------------------------------------------------- eigensolver
+namespace {
+
+constexpr int kHeevThreads = 512;
+constexpr int kMaxWarps = kHeevThreads / 32;
+constexpr int kBisectIters = 200;   // cap; multisection converges in ~20
+constexpr int kInvIters = 3;
+
+__device__ __forceinline__ int sturm_count(const double* d, const double* e2, int n, double x,
+                                           double pivmin) {
+  double q = d[0] - x;
+  if (fabs(q) < pivmin) q = -pivmin;
+  int c = q < 0.0;
+  for (int i = 1; i < n; ++i) {
+    q = d[i] - x - e2[i - 1] / q;
+    if (fabs(q) < pivmin) q = -pivmin;
+    c += q < 0.0;
+  }
+  return c;
+}
+
+__device__ __forceinline__ double hash_uniform(unsigned long long a, unsigned long long b) {
+  unsigned long long x = a * 0x9E3779B97F4A7C15ull ^ (b + 0x632BE59BD9B4E019ull);
+  x ^= x >> 31;
+  x *= 0xBF58476D1CE4E5B9ull;
+  x ^= x >> 27;
+  x *= 0x94D049BB133111EBull;
+  x ^= x >> 31;
+  return ((double)(x >> 11) * (1.0 / 9007199254740992.0)) * 2.0 - 1.0;  // (-1, 1)
+}
+
+// Solves (T - lam I) x = b in place by Gaussian elimination with partial
+// pivoting (the LU has two super-diagonals). u0/u1/u2 are scratch of length n.
+__device__ void tri_solve(const double* d, const double* e, int n, double lam, double tiny,
+                          double* x, double* u0, double* u1, double* u2) {
+  // Forward elimination applied to the right-hand side as the LU is formed.
+  double a = d[0] - lam;                  // current pivot-row diagonal
+  double c = n > 1 ? e[0] : 0.0;          // current pivot-row first super-diagonal
+  double c2 = 0.0;                         // current pivot-row second super-diagonal
+  for (int i = 0; i < n - 1; ++i) {
+    const double b = e[i];                // sub-diagonal below the pivot
+    const double dn = d[i + 1] - lam;     // next row diagonal
+    const double en = i + 1 < n - 1 ? e[i + 1] : 0.0;  // next row super-diagonal
+    if (fabs(a) >= fabs(b)) {
+      if (a == 0.0) a = tiny;
+      const double f = b / a;
+      u0[i] = a;
+      u1[i] = c;
+      u2[i] = c2;
+      x[i + 1] -= f * x[i];
+      a = dn - f * c;
+      c = en - f * c2;
+      c2 = 0.0;
+    } else {
+      // swap rows i and i+1
+      const double f = a / b;
+      u0[i] = b;
+      u1[i] = dn;
+      u2[i] = en;
+      const double xi = x[i];
+      x[i] = x[i + 1];
+      x[i + 1] = xi - f * x[i];
+      a = c - f * dn;
+      c = c2 - f * en;
+      c2 = 0.0;
+    }
+  }
+  if (a == 0.0 || fabs(a) < tiny) a = a < 0 ? -tiny : tiny;
+  u0[n - 1] = a;
+  // back substitution
+  x[n - 1] = x[n - 1] / u0[n - 1];
+  if (n > 1) x[n - 2] = (x[n - 2] - u1[n - 2] * x[n - 1]) / u0[n - 2];
+  for (int i = n - 3; i >= 0; --i) x[i] = (x[i] - u1[i] * x[i + 1] - u2[i] * x[i + 2]) / u0[i];
+}
+
+}  // namespace
+
+// Shared-memory layout (double2 units unless noted):
+//   [A: n*n if resident] vprev[n] wprev[n] vcur[n] y[n] tau[n] red2[kMaxWarps]
+//   doubles: d[n] e[n] e2[n] red[kMaxWarps] lam[nev] lo[nev] hi[nev] xs[kHeevThreads]
+//   ints: cnt[kHeevThreads] clus[nev+1] misc[4]
+__host__ __device__ inline size_t heev_smem_bytes(int n, int nev, bool resident) {
+  size_t b = 0;
+  if (resident) b += (size_t)n * n * sizeof(double2);
+  b += (size_t)5 * n * sizeof(double2) + kMaxWarps * sizeof(double2);
+  b += (size_t)(3 * n + kMaxWarps + 3 * nev + kHeevThreads) * sizeof(double);
+  b += (size_t)(kHeevThreads + nev + 1 + 4) * sizeof(int);
+  return b;
+}
+
+template <bool RESIDENT>
+__global__ void __launch_bounds__(kHeevThreads) heev_kernel(const EigItem* __restrict__ items,
+                                                            double2* __restrict__ hbuf,
+                                                            double* __restrict__ wbuf,
+                                                            double2* __restrict__ zbuf,
+                                                            double* __restrict__ scratch,
+                                                            int* __restrict__ info) {
+  const EigItem it = items[blockIdx.x];
+  const int n = it.n, nev = it.nev;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int nthr = blockDim.x, nw = nthr >> 5;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double2* sp = reinterpret_cast<double2*>(smraw);
+  double2* A;
+  if (RESIDENT) {
+    A = sp;
+    sp += (size_t)n * n;
+  } else {
+    A = hbuf + it.h_off;
+  }
+  double2* vprev = sp;
+  double2* wprev = vprev + n;
+  double2* vcur = wprev + n;
+  double2* y = vcur + n;
+  double2* tau = y + n;
+  double2* red2 = tau + n;
+  double* d = reinterpret_cast<double*>(red2 + kMaxWarps);
+  double* e = d + n;
+  double* e2 = e + n;
+  double* red = e2 + n;
+  double* lam = red + kMaxWarps;
+  double* lo = lam + nev;
+  double* hi = lo + nev;
+  double* xs = hi + nev;
+  int* cnt = reinterpret_cast<int*>(xs + kHeevThreads);
+  int* clus = cnt + kHeevThreads;
+  int* misc = clus + nev + 1;
+
+  if (RESIDENT) {
+    const double2* src = hbuf + it.h_off;
+    for (int i = tid; i < n * n; i += nthr) A[i] = src[i];
+  }
+  __syncthreads();
+
+  // ---------------------------------------------- Householder tridiagonalisation
+  bool pending = false;
+  for (int j = 0; j < n - 1; ++j) {
+    // (1) finish column j: apply the rank-2 update of step j-1.
+    for (int r = j + tid; r < n; r += nthr) {
+      double2 a = A[(long long)j * n + r];
+      if (pending) {
+        a = csub(a, cadd(cmul(vprev[r], cconj(wprev[j])), cmul(wprev[r], cconj(vprev[j]))));
+        A[(long long)j * n + r] = a;
+      }
+    }
+    __syncthreads();
+    // (2) reflector for x = A[j+1:n, j] (zlarfg convention, H = I - tau v v^H,
+    //     H^H x = beta e_1 with beta real)
+    double part = 0.0;
+    for (int r = j + 2 + tid; r < n; r += nthr) {
+      const double2 a = A[(long long)j * n + r];
+      part += a.x * a.x + a.y * a.y;
+    }
+    const double xnorm2 = block_sum(part, red);
+    const double2 alpha = A[(long long)j * n + j + 1];
+    double beta;
+    double2 tj, scal;
+    if (xnorm2 == 0.0 && alpha.y == 0.0) {
+      tj = make_double2(0, 0);
+      beta = alpha.x;
+      scal = make_double2(1, 0);
+    } else {
+      beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2), alpha.x);
+      tj = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
+      // scal = 1 / (alpha - beta)
+      const double2 den = make_double2(alpha.x - beta, alpha.y);
+      const double dd = den.x * den.x + den.y * den.y;
+      scal = make_double2(den.x / dd, -den.y / dd);
+    }
+    for (int r = j + 2 + tid; r < n; r += nthr) {
+      const double2 a = cmul(A[(long long)j * n + r], scal);
+      A[(long long)j * n + r] = a;
+      vcur[r] = a;
+    }
+    if (tid == 0) {
+      d[j] = A[(long long)j * n + j].x;
+      e[j] = beta;
+      tau[j] = tj;
+      vcur[j + 1] = make_double2(1, 0);
+      A[(long long)j * n + j + 1] = make_double2(1, 0);
+    }
+    __syncthreads();
+    const bool active = tj.x != 0.0 || tj.y != 0.0;
+    // (3) fused pass over the trailing columns: apply update j-1, then
+    //     y_c = tau (A[:,c])^H v  (A Hermitian, so this is tau (A v)_c).
+    for (int c = j + 1 + wid; c < n; c += nw) {
+      double2* col = A + (long long)c * n;
+      double2 acc = make_double2(0, 0);
+      const double2 wc = pending ? cconj(wprev[c]) : make_double2(0, 0);
+      const double2 vc = pending ? cconj(vprev[c]) : make_double2(0, 0);
+      for (int r = j + 1 + lane; r < n; r += 32) {
+        double2 a = col[r];
+        if (pending) {
+          a = csub(a, cadd(cmul(vprev[r], wc), cmul(wprev[r], vc)));
+          col[r] = a;
+        }
+        acc = cadd(acc, cmulc(a, vcur[r]));
+      }
+      acc = warp_sum2(acc);
+      if (lane == 0) y[c] = cmul(tj, acc);
+    }
+    __syncthreads();
+    // (4) w = y - 1/2 tau (y^H v) v becomes the pending update.
+    double2 pp = make_double2(0, 0);
+    if (active)
+      for (int r = j + 1 + tid; r < n; r += nthr) pp = cadd(pp, cmulc(y[r], vcur[r]));
+    const double2 yv = block_sum2(pp, red2);
+    const double2 al = cscale(cmul(tj, yv), -0.5);
+    for (int r = j + 1 + tid; r < n; r += nthr) {
+      vprev[r] = vcur[r];
+      wprev[r] = active ? cadd(y[r], cmul(al, vcur[r])) : make_double2(0, 0);
+    }
+    pending = active;
+    __syncthreads();
+  }
+  if (tid == 0) {
+    double2 a = A[(long long)(n - 1) * n + n - 1];
+    if (pending && n > 1)
+      a = csub(a, cadd(cmul(vprev[n - 1], cconj(wprev[n - 1])), cmul(wprev[n - 1], cconj(vprev[n - 1]))));
+    d[n - 1] = a.x;
+    if (n == 1) tau[0] = make_double2(0, 0);
+  }
+  __syncthreads();
+
+  // ------------------------------------------------------------- eigenvalues
+  // Gershgorin interval, pivmin, and negligible off-diagonals set to zero.
+  if (tid == 0) {
+    double glo = d[0], ghi = d[0], emax2 = 0.0, tnorm = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double el = i > 0 ? fabs(e[i - 1]) : 0.0, er = i < n - 1 ? fabs(e[i]) : 0.0;
+      glo = fmin(glo, d[i] - el - er);
+      ghi = fmax(ghi, d[i] + el + er);
+      tnorm = fmax(tnorm, fabs(d[i]) + el + er);
+    }
+    for (int i = 0; i < n - 1; ++i) {
+      if (fabs(e[i]) <= DBL_EPSILON * (fabs(d[i]) + fabs(d[i + 1]))) e[i] = 0.0;
+      e2[i] = e[i] * e[i];
+      emax2 = fmax(emax2, e2[i]);
+    }
+    const double pad = 2.0 * DBL_EPSILON * tnorm * n + DBL_MIN;
+    red[0] = glo - pad;
+    red[1] = ghi + pad;
+    red[2] = DBL_MIN * fmax(1.0, emax2);
+    red[3] = tnorm;
+  }
+  __syncthreads();
+  const double pivmin = red[2], tnorm = red[3];
+  for (int k = tid; k < nev; k += nthr) {
+    lo[k] = red[0];
+    hi[k] = red[1];
+  }
+  // multisection: G threads per eigenvalue probe G interior points at once
+  const int G = nev > 0 ? max(1, nthr / nev) : 1;
+  __syncthreads();
+  int converged = 0;
+  for (int iter = 0; iter < kBisectIters; ++iter) {
+    const int k = tid / G, g = tid % G;
+    if (k < nev) {
+      const double l = lo[k], h = hi[k];
+      const double x = l + (h - l) * (double)(g + 1) / (double)(G + 1);
+      xs[tid] = x;
+      cnt[tid] = sturm_count(d, e2, n, x, pivmin);
+    }
+    __syncthreads();
+    int done = 1;
+    if (tid < nev) {
+      const int kk = tid;
+      double l = lo[kk], h = hi[kk];
+      const double tol = 2.0 * DBL_EPSILON * fmax(fabs(l), fabs(h)) + 4.0 * pivmin;
+      if (h - l > tol) {
+        for (int gg = 0; gg < G; ++gg) {
+          const int t = kk * G + gg;
+          if (cnt[t] <= kk)
+            l = fmax(l, xs[t]);
+          else
+            h = fmin(h, xs[t]);
+        }
+        lo[kk] = l;
+        hi[kk] = h;
+        done = (h - l) <= tol;
+      }
+    }
+    done = __syncthreads_and(done);
+    if (done) {
+      converged = 1;
+      break;
+    }
+  }
+  int finite = 1;
+  for (int k = tid; k < nev; k += nthr) {
+    lam[k] = 0.5 * (lo[k] + hi[k]);
+    wbuf[it.w_off + k] = lam[k];
+    finite &= isfinite(lam[k]) ? 1 : 0;
+  }
+  finite = __syncthreads_and(finite);
+  const int status = !finite ? 2 : (!converged ? 1 : 0);
+  if (!it.want_vec || status != 0) {
+    if (tid == 0) info[blockIdx.x] = status;
+    return;
+  }
+
+  // ----------------------------------------------- tridiagonal eigenvectors
+  // clusters of eigenvalues closer than 1e-5 |T| are reorthogonalised.
+  if (tid == 0) {
+    int nc = 0;
+    const double gap = 1e-5 * tnorm;
+    for (int k = 0; k < nev; ++k)
+      if (k == 0 || lam[k] - lam[k - 1] > gap) clus[nc++] = k;
+    clus[nc] = nev;
+    misc[0] = nc;
+  }
+  __syncthreads();
+  const int ncl = misc[0];
+  const double tiny = DBL_EPSILON * fmax(tnorm, DBL_MIN);
+  for (int cl = tid; cl < ncl; cl += nthr) {
+    double* u0 = scratch + it.s_off + (size_t)4 * n * cl;
+    double* u1 = u0 + n;
+    double* u2 = u1 + n;
+    double* x = u2 + n;
+    for (int k = clus[cl]; k < clus[cl + 1]; ++k) {
+      for (int i = 0; i < n; ++i) x[i] = hash_uniform(((unsigned long long)blockIdx.x << 20) + k, i);
+      for (int iter = 0; iter < kInvIters; ++iter) {
+        tri_solve(d, e, n, lam[k], tiny, x, u0, u1, u2);
+        for (int kp = clus[cl]; kp < k; ++kp) {
+          const double2* zp = zbuf + it.z_off + (size_t)kp * n;
+          double s = 0.0;
+          for (int i = 0; i < n; ++i) s += zp[i].x * x[i];
+          for (int i = 0; i < n; ++i) x[i] -= s * zp[i].x;
+        }
+        double s = 0.0, mx = 0.0;
+        for (int i = 0; i < n; ++i) mx = fmax(mx, fabs(x[i]));
+        if (!(mx > 0.0) || !isfinite(mx)) mx = 1.0;
+        for (int i = 0; i < n; ++i) {
+          x[i] /= mx;
+          s += x[i] * x[i];
+        }
+        s = 1.0 / sqrt(s);
+        for (int i = 0; i < n; ++i) x[i] *= s;
+      }
+      double2* zk = zbuf + it.z_off + (size_t)k * n;
+      for (int i = 0; i < n; ++i) zk[i] = make_double2(x[i], 0.0);
+    }
+  }
+  __syncthreads();
+
+  // ----------------------------------------------------------- back-transform
+  // x = H_0 H_1 ... H_{n-2} z ; one warp per eigenvector, no block barriers.
+  for (int k = wid; k < nev; k += nw) {
+    double2* z = zbuf + it.z_off + (size_t)k * n;
+    for (int j = n - 2; j >= 0; --j) {
+      const double2 tj = tau[j];
+      if (tj.x == 0.0 && tj.y == 0.0) continue;
+      const double2* v = A + (long long)j * n;
+      double2 s = make_double2(0, 0);
+      for (int r = j + 1 + lane; r < n; r += 32) s = cadd(s, cmulc(v[r], z[r]));
+      s = cmul(tj, warp_sum2(s));
+      for (int r = j + 1 + lane; r < n; r += 32) z[r] = csub(z[r], cmul(v[r], s));
+      __syncwarp();
+    }
+  }
+  if (tid == 0) info[blockIdx.x] = 0;
+}
+
+int heev_smem_max_n() {
+  // largest n whose resident layout fits the 227 KB opt-in limit
+  const size_t lim = 227 * 1024;
+  int n = 1;
+  while (heev_smem_bytes(n + 1, 64, true) <= lim) ++n;
+  return n;
+}
+
+cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev, double2* hbuf,
+                        double* wbuf, double2* zbuf, double* scratch, int* info, cudaStream_t st) {
+  if (nitems <= 0) return cudaSuccess;
+  const bool resident = max_n <= heev_smem_max_n();
+  const size_t smem = heev_smem_bytes(max_n, max_nev, resident);
+  cudaError_t err;
+  if (resident) {
+    err = cudaFuncSetAttribute(heev_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    heev_kernel<true><<<nitems, kHeevThreads, smem, st>>>(items, hbuf, wbuf, zbuf, scratch, info);
+  } else {
+    err = cudaFuncSetAttribute(heev_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    heev_kernel<false><<<nitems, kHeevThreads, smem, st>>>(items, hbuf, wbuf, zbuf, scratch, info);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace dev
+}  // namespace pmx

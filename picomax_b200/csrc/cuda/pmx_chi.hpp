@@ -1,0 +1,74 @@
+// Argument blocks and launchers of the chi-stage kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace pmx {
+namespace dev {
+
+struct OverlapArgs {
+  int n;            // eigenvector length (npw, or 2 npw with SOC)
+  int npw;
+  int soc;          // eigenvectors are spinors
+  int nev;          // eigenvectors stored per k
+  int neps;
+  int nch;          // 1 or 4 output channels
+  int mode;         // 0 epsij, 1 epsLL
+  int cchunk;       // conduction states per CTA
+  int ncd_max, nvd_max;
+  const double2* zk;      // [nk][nev][n] eigenvectors at k
+  const double2* zq;      // [nk][nev][n] eigenvectors at k+q
+  const int* ncd;         // [nk] distinct conduction states
+  const int* nvd;         // [nk] distinct valence states
+  const int* cbase;       // [nk] offset into cidx
+  const int* vbase;       // [nk] offset into vidx
+  const int* cidx;        // eigenvector index of each conduction state
+  const int* vidx;        // eigenvector index of each valence state
+  const long long* blkoff;  // [nk] offset of the k block in dest
+  const long long* dest;    // sorted transition of (k, c, v), -1 if unused
+  const int* loci;        // [neps][npw]
+  const double* G;        // [npw][3]
+  const double* kpts;     // [nk][3]
+  double q[3];
+  const double2* uvec;    // [neps][3][3]  u_i of q + G_m
+  const double2* ssoc;    // [neps][3]     u_i^H v_soc(G_m)
+  double2* M;             // [T][3 neps][nch]
+};
+
+struct ContractArgs {
+  const double2* M;     // [T][3 neps][nch]
+  const double* dE;     // [T]
+  const double* wgt;    // [T] k weight times spin multiplicity
+  const int* f0;        // [T] window centre int((dE - w0)/dw)
+  const int2* trange;   // [n f-tiles] transition range of each frequency tile
+  int neps, np, nf, nch;
+  int window;           // half width, or -1 for all frequencies
+  int delta;            // broadening model
+  double eps, dfreq;
+  double* acc;          // [2][9][np][nf] Re then Im
+  double* acc_pv;       // principal-value accumulators (epsLL, kk = 0) or null
+};
+
+struct ScaleArgs {
+  int mode;             // 0 epsij, 1 epsLL
+  int np, nf;
+  double dfreq;
+  double sf;            // epsij SCALEFACTOR
+  double sf_ll, sf_lt, sf_tt;
+  const double* qgn;    // [neps] |q + G_m|
+  const double* acc;
+  const double* acc_pv;
+  double* out;
+};
+
+cudaError_t launch_overlap(const OverlapArgs& a, int nk, cudaStream_t st);
+size_t overlap_smem_bytes(int cchunk, int nvd_max, int n, int npw);
+cudaError_t launch_contract_f64(const ContractArgs& a, cudaStream_t st);
+int contract_ftile();
+cudaError_t launch_scale(const ScaleArgs& s, cudaStream_t st);
+cudaError_t launch_kk(const double* chi, double* out, int rows, int nf, double dfreq, cudaStream_t st);
+
+}  // namespace dev
+}  // namespace pmx

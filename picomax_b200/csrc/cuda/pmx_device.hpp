@@ -1,0 +1,54 @@
+// Device-side data structures and kernel launchers of the picomax B200 path.
+//
+// Stage 1 (EPM): every (crystal, k) work item builds H(k) in HBM and is
+// diagonalised by one CTA of the batched FP64 eigensolver. Stage 2 (chi):
+// overlaps, transition list, the delta-weighted contraction and the
+// Kramers-Kronig transform. Everything is stream-ordered on the caller's
+// stream; nothing here allocates.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pmx {
+namespace dev {
+
+// One crystal as the kernels see it. Tables are indexed by an hkl difference
+// d = (dh, dk, dl) through ((dh+2imax)*side + dk+2imax)*side + dl+2imax.
+struct CrystalDev {
+  int npw;        // plane waves N_G
+  int soc;        // 1: spinor H of size 2 N_G; 0: H0 of size N_G (spectrum doubled)
+  int imax;       // |h|,|k|,|l| <= imax for every G
+  int side;       // 4*imax+1
+  double kin;     // KCON (2 pi / a)^2, eV
+  const double* G;      // [npw][3], units 2 pi / a
+  const int* hkl;       // [npw][3]
+  const double2* vloc;  // V(G_i - G_j) in eV for d = hkl_i - hkl_j (0 beyond g2max)
+  const double2* vso;   // VSO(q) = lambda_S cos_sum + i lambda_A sin_sum, eV, d = hkl_j - hkl_i
+};
+
+// One eigenproblem of the batch.
+struct EigItem {
+  int crystal;        // index into the crystal table
+  int n;              // matrix dimension (npw, or 2 npw with SOC)
+  int nev;            // lowest eigenpairs returned
+  int want_vec;       // 1: also eigenvectors
+  double k[3];        // wave vector, units 2 pi / a
+  long long h_off;    // double2 offset of the n*n column-major workspace
+  long long w_off;    // double offset of nev eigenvalues
+  long long z_off;    // double2 offset of nev eigenvectors (column s at z_off + s*n)
+  long long s_off;    // double offset of 4*n*nev inverse-iteration scratch
+};
+
+// Fills H(k) of every item (full Hermitian storage) into hbuf.
+cudaError_t launch_assemble(const CrystalDev* crystals, const EigItem* items, int nitems,
+                            int max_npw, double2* hbuf, cudaStream_t st);
+
+// Eigensolve of every item. Matrices with n <= smem_max_n run with the matrix
+// resident in shared memory. info[i] != 0 flags a failure of item i.
+cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev, double2* hbuf,
+                        double* wbuf, double2* zbuf, double* scratch, int* info, cudaStream_t st);
+int heev_smem_max_n();
+
+}  // namespace dev
+}  // namespace pmx

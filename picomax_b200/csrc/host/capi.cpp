@@ -1,0 +1,872 @@
+// C-ABI of the picomax B200 library (include/picomax.h): problem objects,
+// device context, and the host orchestration of the two GPU stages.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <ctime>
+#include <fstream>
+#include <iostream>
+#include <memory>
+#include <numeric>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../../include/picomax.h"
+#include "../cuda/pmx_chi.hpp"
+#include "../cuda/pmx_device.hpp"
+#include "../cuda/pmx_mixed.hpp"
+#include "pmx_host.hpp"
+
+using pmx::Problem;
+using pmx::Vec3;
+
+// ======================================================================= problem
+struct pmx_problem {
+  Problem p;
+  // form-factor tables over hkl differences (see CrystalDev)
+  std::vector<double> vloc, vso;  // complex interleaved [side^3][2]
+  int soc = 0;
+};
+
+namespace {
+
+void build_tables(pmx_problem& P) {
+  Problem& p = P.p;
+  const int side = 4 * p.imax + 1, off = 2 * p.imax;
+  const size_t n3 = (size_t)side * side * side;
+  P.vloc.assign(2 * n3, 0.0);
+  P.vso.assign(2 * n3, 0.0);
+  const Vec3 b1 = p.lat.reciprocal[0], b2 = p.lat.reciprocal[1];
+  const Vec3 b3 = p.lat.dim == 3 ? p.lat.reciprocal[2] : Vec3{0, 0, 0};
+  P.soc = 0;
+  for (int h = -off; h <= off; ++h)
+    for (int k = -off; k <= off; ++k)
+      for (int l = -off; l <= off; ++l) {
+        if (p.lat.dim == 2 && l != 0) continue;
+        const Vec3 dG = (double(h) * b1 + double(k) * b2) + double(l) * b3;
+        const size_t idx = ((size_t)(h + off) * side + (k + off)) * side + (l + off);
+        double re, im;
+        pmx::local_potential(p, dG, re, im);
+        P.vloc[2 * idx] = re;
+        P.vloc[2 * idx + 1] = im;
+        pmx::soc_scalar(p, dG, re, im);
+        P.vso[2 * idx] = re;
+        P.vso[2 * idx + 1] = im;
+        if ((h || k || l) && (re != 0.0 || im != 0.0)) P.soc = 1;
+      }
+}
+
+// SOC current of socCurrent (src/pmx_chi.cpp:203-266) for q = G_m: lambda_S is
+// looked up in the -us_so map only, even when -use_uniform_us_so is set.
+void soc_current(const Problem& p, const Vec3& q, std::complex<double> out[3]) {
+  const std::complex<double> I(0.0, 1.0);
+  const double q2 = pmx::sqnorm(q);
+  const double la = pmx::soc_form_factor(p.mat.Ua, q2) * pmx::kRy2eV;
+  const double ls = pmx::soc_form_factor(p.mat.Us, q2) * pmx::kRy2eV;
+  double cs = 0, sn = 0;
+  if (p.natom > 0) {
+    for (const Vec3& t : p.lat.atomic) {
+      cs += std::cos(2.0 * pmx::kPi * pmx::dot(q, t));
+      sn += std::sin(2.0 * pmx::kPi * pmx::dot(q, t));
+    }
+    cs /= p.natom;
+    sn /= p.natom;
+  }
+  const std::complex<double> vso = ls * cs + I * la * sn;
+  out[0] = I * vso * (q.y + I * q.z);
+  out[1] = I * vso * (q.z - q.x);
+  out[2] = I * vso * (-I * q.x - q.y);
+}
+
+}  // namespace
+
+extern "C" int pmx_problem_create(int argc, const char* const* argv, pmx_problem** out) {
+  if (!out) return PMX_ERR_INVALID;
+  *out = nullptr;
+  auto P = std::make_unique<pmx_problem>();
+  try {
+    pmx::build_problem(argc, argv, P->p);
+    build_tables(*P);
+  } catch (const std::exception& e) {
+    std::cerr << "picomax: " << e.what() << std::endl;
+    return PMX_ERR_INVALID;
+  }
+  *out = P.release();
+  return PMX_OK;
+}
+
+extern "C" void pmx_problem_destroy(pmx_problem* p) { delete p; }
+
+extern "C" int pmx_problem_get_info(const pmx_problem* P, pmx_problem_info* info) {
+  if (!P || !info) return PMX_ERR_INVALID;
+  const Problem& p = P->p;
+  std::memset(info, 0, sizeof(*info));
+  info->npw = p.npw();
+  info->nh = 2 * p.npw();
+  info->soc = P->soc;
+  info->neps = p.neps;
+  info->nband = p.nband;
+  info->nvalence = p.nvalence;
+  info->nk = p.nk();
+  info->nq = p.nq();
+  info->nfreq = p.nfreq;
+  info->natom = p.natom;
+  info->sw = (int)p.sw;
+  info->debug = p.debug;
+  info->kk = p.kk;
+  info->delta = p.delta;
+  info->epsilon = p.epsilon;
+  info->dfreq = p.dfreq;
+  info->a = p.lat.a;
+  info->gcut = p.lat.gcut;
+  info->bz_volume = p.lat.bz_volume;
+  info->chi_values = 9LL * p.nq() * ((long long)p.neps * (p.neps + 1) / 2) * p.nfreq;
+  return PMX_OK;
+}
+
+extern "C" int pmx_problem_gvectors(const pmx_problem* P, double* G, int* hkl) {
+  if (!P) return PMX_ERR_INVALID;
+  for (int i = 0; i < P->p.npw(); ++i)
+    for (int x = 0; x < 3; ++x) {
+      if (G) G[3 * i + x] = P->p.G[i][x];
+      if (hkl) hkl[3 * i + x] = P->p.hkl[i][x];
+    }
+  return PMX_OK;
+}
+
+extern "C" int pmx_problem_loci(const pmx_problem* P, int* loci) {
+  if (!P || !loci) return PMX_ERR_INVALID;
+  std::copy(P->p.loci.begin(), P->p.loci.end(), loci);
+  return PMX_OK;
+}
+
+extern "C" int pmx_problem_kpoints(const pmx_problem* P, double* K, double* KW) {
+  if (!P) return PMX_ERR_INVALID;
+  for (int k = 0; k < P->p.nk(); ++k) {
+    if (K)
+      for (int x = 0; x < 3; ++x) K[3 * k + x] = P->p.K[k][x];
+    if (KW) KW[k] = P->p.KW[k];
+  }
+  return PMX_OK;
+}
+
+extern "C" int pmx_problem_qpoints(const pmx_problem* P, double* Q) {
+  if (!P || !Q) return PMX_ERR_INVALID;
+  for (int q = 0; q < P->p.nq(); ++q)
+    for (int x = 0; x < 3; ++x) Q[3 * q + x] = P->p.lat.Q[q][x];
+  return PMX_OK;
+}
+
+extern "C" int pmx_problem_dump(const pmx_problem* P, char* buf, size_t len, size_t* needed) {
+  if (!P) return PMX_ERR_INVALID;
+  std::ostringstream os;
+  std::streambuf* old = std::cout.rdbuf(os.rdbuf());
+  pmx::print_input(P->p);
+  std::cout.rdbuf(old);
+  const std::string s = os.str();
+  if (needed) *needed = s.size() + 1;
+  if (buf && len > 0) {
+    const size_t n = std::min(len - 1, s.size());
+    std::memcpy(buf, s.data(), n);
+    buf[n] = 0;
+  }
+  return PMX_OK;
+}
+
+extern "C" int pmx_problem_write_gpt(const pmx_problem* P) {
+  if (!P) return PMX_ERR_INVALID;
+  try {
+    pmx::write_gpt(P->p);
+  } catch (const std::exception& e) {
+    std::cerr << "picomax: " << e.what() << std::endl;
+    return PMX_ERR_INVALID;
+  }
+  return PMX_OK;
+}
+
+// ======================================================================= context
+namespace {
+
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  ~DevBuf() {
+    if (ptr) cudaFree(ptr);
+  }
+  cudaError_t ensure(size_t b) {
+    if (b <= bytes) return cudaSuccess;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMalloc(&ptr, b);
+    if (e == cudaSuccess) bytes = b;
+    return e;
+  }
+  template <class T>
+  T* as() const {
+    return reinterpret_cast<T*>(ptr);
+  }
+};
+
+struct CudaFail : std::runtime_error {
+  int code;
+  CudaFail(const std::string& m, int c) : std::runtime_error(m), code(c) {}
+};
+
+#define CK(x)                                                                                        \
+  do {                                                                                               \
+    cudaError_t e_ = (x);                                                                            \
+    if (e_ != cudaSuccess)                                                                           \
+      throw CudaFail(std::string(#x) + ": " + cudaGetErrorString(e_), PMX_ERR_CUDA);                 \
+  } while (0)
+
+}  // namespace
+
+struct pmx_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  double stage_ms[5] = {0, 0, 0, 0, 0};
+  long long launches = 0;
+  // named workspaces
+  DevBuf crystal, g, hkl, vloc, vso, items, hbuf, wbuf, zk, zq, scratch, info;
+  DevBuf loci, kpts, uvec, ssoc, qgn, ncd, nvd, cbase, vbase, cidx, vidx, blkoff, dest;
+  DevBuf M, dE, wgt, f0, trange, acc, accpv, chi, chi2, mixws;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+};
+
+namespace {
+
+struct Timer {
+  pmx_ctx* c;
+  int slot;
+  Timer(pmx_ctx* ctx, int s) : c(ctx), slot(s) { cudaEventRecord(c->ev[0], c->stream); }
+  ~Timer() {
+    cudaEventRecord(c->ev[1], c->stream);
+    cudaEventSynchronize(c->ev[1]);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    c->stage_ms[slot] += ms;
+  }
+};
+
+template <class F>
+int guarded(pmx_ctx* ctx, F&& f) {
+  if (!ctx) return PMX_ERR_INVALID;
+  ctx->err.clear();
+  try {
+    CK(cudaSetDevice(ctx->device));
+    return f();
+  } catch (const CudaFail& e) {
+    ctx->err = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    ctx->err = e.what();
+    return PMX_ERR_INVALID;
+  }
+}
+
+void h2d(pmx_ctx* c, DevBuf& b, const void* src, size_t bytes) {
+  CK(b.ensure(std::max<size_t>(bytes, 16)));
+  if (bytes) CK(cudaMemcpyAsync(b.ptr, src, bytes, cudaMemcpyHostToDevice, c->stream));
+}
+
+// The crystal as the kernels see it, uploaded into the context.
+struct DevCrystal {
+  pmx::dev::CrystalDev host;
+  pmx::dev::CrystalDev* dev = nullptr;
+  int soc = 0;
+  int npw = 0;
+  int n = 0;        // eigenproblem dimension
+};
+
+DevCrystal upload_crystal(pmx_ctx* c, const pmx_problem* P, int force_spinor) {
+  const Problem& p = P->p;
+  DevCrystal d;
+  d.npw = p.npw();
+  d.soc = (P->soc || force_spinor) ? 1 : 0;
+  d.n = d.soc ? 2 * d.npw : d.npw;
+  std::vector<double> G(3 * d.npw);
+  std::vector<int> H(3 * d.npw);
+  for (int i = 0; i < d.npw; ++i)
+    for (int x = 0; x < 3; ++x) {
+      G[3 * i + x] = p.G[i][x];
+      H[3 * i + x] = p.hkl[i][x];
+    }
+  h2d(c, c->g, G.data(), G.size() * sizeof(double));
+  h2d(c, c->hkl, H.data(), H.size() * sizeof(int));
+  h2d(c, c->vloc, P->vloc.data(), P->vloc.size() * sizeof(double));
+  h2d(c, c->vso, P->vso.data(), P->vso.size() * sizeof(double));
+  pmx::dev::CrystalDev& cd = d.host;
+  cd.npw = d.npw;
+  cd.soc = d.soc;
+  cd.imax = p.imax;
+  cd.side = 4 * p.imax + 1;
+  const double s = 2.0 * pmx::kPi / p.lat.a;
+  cd.kin = pmx::kKCON * (s * s);
+  cd.G = c->g.as<double>();
+  cd.hkl = c->hkl.as<int>();
+  cd.vloc = c->vloc.as<double2>();
+  cd.vso = c->vso.as<double2>();
+  h2d(c, c->crystal, &cd, sizeof(cd));
+  d.dev = c->crystal.as<pmx::dev::CrystalDev>();
+  return d;
+}
+
+// Assembles and diagonalises H(k) for every k; eigenvalues to w (host,
+// [nk][nev]); eigenvectors to zdev ([nk][nev][n]) when non-null.
+void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int nev, double2* zdev,
+             std::vector<double>& w) {
+  const int nk = (int)ks.size(), n = dc.n;
+  w.assign((size_t)nk * nev, 0.0);
+  if (nk == 0) return;
+  const size_t hbytes = (size_t)n * n * sizeof(double2);
+  int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)nk, ((size_t)2 << 30) / hbytes));
+  chunk = std::min(chunk, 4096);
+  CK(c->hbuf.ensure(hbytes * chunk));
+  CK(c->wbuf.ensure(sizeof(double) * (size_t)nk * nev));
+  CK(c->scratch.ensure(sizeof(double) * 4 * (size_t)n * nev * (zdev ? chunk : 1)));
+  CK(c->info.ensure(sizeof(int) * chunk));
+  DevBuf ztmp;
+  double2* zbuf = zdev;
+  if (!zbuf) {
+    CK(ztmp.ensure(16));
+    zbuf = ztmp.as<double2>();
+  }
+  std::vector<pmx::dev::EigItem> items(chunk);
+  std::vector<int> info(chunk);
+  for (int k0 = 0; k0 < nk; k0 += chunk) {
+    const int cnt = std::min(chunk, nk - k0);
+    for (int i = 0; i < cnt; ++i) {
+      pmx::dev::EigItem& it = items[i];
+      it.crystal = 0;
+      it.n = n;
+      it.nev = nev;
+      it.want_vec = zdev ? 1 : 0;
+      for (int x = 0; x < 3; ++x) it.k[x] = ks[k0 + i][x];
+      it.h_off = (long long)i * n * n;
+      it.w_off = (long long)(k0 + i) * nev;
+      it.z_off = (long long)(k0 + i) * nev * n;
+      it.s_off = (long long)i * 4 * n * nev;
+    }
+    h2d(c, c->items, items.data(), sizeof(pmx::dev::EigItem) * cnt);
+    CK(pmx::dev::launch_assemble(dc.dev, c->items.as<pmx::dev::EigItem>(), cnt, dc.npw, c->hbuf.as<double2>(),
+                                 c->stream));
+    CK(pmx::dev::launch_heev(c->items.as<pmx::dev::EigItem>(), cnt, n, nev, c->hbuf.as<double2>(),
+                             c->wbuf.as<double>(), zbuf, c->scratch.as<double>(), c->info.as<int>(), c->stream));
+    c->launches += 2;
+    CK(cudaMemcpyAsync(info.data(), c->info.ptr, sizeof(int) * cnt, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < cnt; ++i)
+      if (info[i] != 0)
+        throw CudaFail("eigensolver failed (status " + std::to_string(info[i]) + ") at k-point " +
+                           std::to_string(k0 + i),
+                       PMX_ERR_NOCONV);
+  }
+  CK(cudaMemcpyAsync(w.data(), c->wbuf.ptr, sizeof(double) * w.size(), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+}
+
+// Spinor eigenvalue s of a solved item (spatial spectrum doubled without SOC).
+inline double spinor_eig(const std::vector<double>& w, int nev, int k, int s, int soc) {
+  return soc ? w[(size_t)k * nev + s] : w[(size_t)k * nev + s / 2];
+}
+
+// Number of solved states needed to cover `spinor` spinor states.
+inline int solved_states(int spinor, int soc) { return soc ? spinor : (spinor + 1) / 2; }
+
+double ref_energy(pmx_ctx* c, const pmx_problem* P, const DevCrystal& dc) {
+  const Problem& p = P->p;
+  const int nh = 2 * p.npw();
+  if (!(p.nvalence > 0 && p.nvalence < nh)) {
+    std::cout << "WARNING::setRefEnergy:: nvalence is out of bounds for eigenvalues. Setting offset to 0."
+              << std::endl;
+    return 0.0;
+  }
+  const int nev = solved_states(p.nvalence + 1, dc.soc);
+  std::vector<double> w;
+  solve_k(c, dc, {p.refpoint}, nev, nullptr, w);
+  return (spinor_eig(w, nev, 0, p.nvalence - 1, dc.soc) + spinor_eig(w, nev, 0, p.nvalence, dc.soc)) / 2.0;
+}
+
+}  // namespace
+
+extern "C" int pmx_ctx_create(int device, pmx_ctx** out) {
+  if (!out) return PMX_ERR_INVALID;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return PMX_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev) return PMX_ERR_INVALID;
+  auto c = std::make_unique<pmx_ctx>();
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) return PMX_ERR_CUDA;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return PMX_ERR_CUDA;
+  if (cudaEventCreate(&c->ev[0]) != cudaSuccess || cudaEventCreate(&c->ev[1]) != cudaSuccess) return PMX_ERR_CUDA;
+  *out = c.release();
+  return PMX_OK;
+}
+
+extern "C" void pmx_ctx_destroy(pmx_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+extern "C" const char* pmx_ctx_last_error(const pmx_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+extern "C" int pmx_ctx_stage_times(const pmx_ctx* c, double* ms5) {
+  if (!c || !ms5) return PMX_ERR_INVALID;
+  for (int i = 0; i < 5; ++i) ms5[i] = c->stage_ms[i];
+  return PMX_OK;
+}
+
+extern "C" long long pmx_ctx_kernel_launches(const pmx_ctx* c) { return c ? c->launches : -1; }
+
+// ======================================================================= stage 1
+extern "C" int pmx_hamiltonian(pmx_ctx* ctx, const pmx_problem* P, const double* kpts, int nk, double* out) {
+  if (!P || (nk > 0 && (!kpts || !out)) || nk < 0) return PMX_ERR_INVALID;
+  return guarded(ctx, [&]() {
+    DevCrystal dc = upload_crystal(ctx, P, 1);
+    const int n = dc.n;
+    std::vector<pmx::dev::EigItem> items(nk);
+    for (int i = 0; i < nk; ++i) {
+      items[i].crystal = 0;
+      items[i].n = n;
+      for (int x = 0; x < 3; ++x) items[i].k[x] = kpts[3 * i + x];
+      items[i].h_off = (long long)i * n * n;
+    }
+    const size_t bytes = sizeof(double2) * (size_t)n * n * nk;
+    CK(ctx->hbuf.ensure(std::max<size_t>(bytes, 16)));
+    h2d(ctx, ctx->items, items.data(), sizeof(pmx::dev::EigItem) * nk);
+    CK(pmx::dev::launch_assemble(dc.dev, ctx->items.as<pmx::dev::EigItem>(), nk, dc.npw, ctx->hbuf.as<double2>(),
+                                 ctx->stream));
+    ctx->launches += 1;
+    CK(cudaMemcpyAsync(out, ctx->hbuf.ptr, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return (int)PMX_OK;
+  });
+}
+
+extern "C" int pmx_heev_batched(pmx_ctx* ctx, int n, int batch, const double* A, int nev, double* w, double* z) {
+  if (n <= 0 || batch < 0 || nev <= 0 || nev > n || nev > 512 || (batch > 0 && (!A || !w)))
+    return PMX_ERR_INVALID;
+  return guarded(ctx, [&]() {
+    const size_t hb = sizeof(double2) * (size_t)n * n;
+    CK(ctx->hbuf.ensure(std::max<size_t>(hb * batch, 16)));
+    CK(ctx->wbuf.ensure(std::max<size_t>(sizeof(double) * (size_t)batch * nev, 16)));
+    CK(ctx->zk.ensure(std::max<size_t>(sizeof(double2) * (size_t)batch * nev * n, 16)));
+    CK(ctx->scratch.ensure(std::max<size_t>(sizeof(double) * 4 * (size_t)n * nev * batch, 16)));
+    CK(ctx->info.ensure(std::max<size_t>(sizeof(int) * batch, 16)));
+    std::vector<pmx::dev::EigItem> items(batch);
+    for (int i = 0; i < batch; ++i) {
+      items[i] = pmx::dev::EigItem{};
+      items[i].n = n;
+      items[i].nev = nev;
+      items[i].want_vec = z ? 1 : 0;
+      items[i].h_off = (long long)i * n * n;
+      items[i].w_off = (long long)i * nev;
+      items[i].z_off = (long long)i * nev * n;
+      items[i].s_off = (long long)i * 4 * n * nev;
+    }
+    if (batch == 0) return (int)PMX_OK;
+    CK(cudaMemcpyAsync(ctx->hbuf.ptr, A, hb * batch, cudaMemcpyHostToDevice, ctx->stream));
+    h2d(ctx, ctx->items, items.data(), sizeof(pmx::dev::EigItem) * batch);
+    CK(pmx::dev::launch_heev(ctx->items.as<pmx::dev::EigItem>(), batch, n, nev, ctx->hbuf.as<double2>(),
+                             ctx->wbuf.as<double>(), ctx->zk.as<double2>(), ctx->scratch.as<double>(),
+                             ctx->info.as<int>(), ctx->stream));
+    ctx->launches += 1;
+    std::vector<int> info(batch);
+    CK(cudaMemcpyAsync(info.data(), ctx->info.ptr, sizeof(int) * batch, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(w, ctx->wbuf.ptr, sizeof(double) * batch * nev, cudaMemcpyDeviceToHost, ctx->stream));
+    if (z)
+      CK(cudaMemcpyAsync(z, ctx->zk.ptr, sizeof(double2) * (size_t)batch * nev * n, cudaMemcpyDeviceToHost,
+                         ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int i = 0; i < batch; ++i)
+      if (info[i]) throw CudaFail("eigensolver failed for matrix " + std::to_string(i), PMX_ERR_NOCONV);
+    return (int)PMX_OK;
+  });
+}
+
+extern "C" int pmx_ref_energy(pmx_ctx* ctx, const pmx_problem* P, double* off) {
+  if (!P || !off) return PMX_ERR_INVALID;
+  return guarded(ctx, [&]() {
+    DevCrystal dc = upload_crystal(ctx, P, 0);
+    *off = ref_energy(ctx, P, dc);
+    return (int)PMX_OK;
+  });
+}
+
+extern "C" int pmx_band(pmx_ctx* ctx, const pmx_problem* P, double* eband) {
+  if (!P || (!eband && P->p.nq() > 0)) return PMX_ERR_INVALID;
+  return guarded(ctx, [&]() {
+    const Problem& p = P->p;
+    for (double& t : ctx->stage_ms) t = 0;
+    Timer tm(ctx, 0);
+    DevCrystal dc = upload_crystal(ctx, P, 0);
+    const double off = ref_energy(ctx, P, dc);
+    const int nh = 2 * p.npw();
+    const int nkeep = std::min(p.nband, nh);
+    if (nkeep <= 0) {
+      std::fill(eband, eband + (size_t)p.nq() * std::max(p.nband, 0), 0.0);
+      return (int)PMX_OK;
+    }
+    const int nev = solved_states(nkeep, dc.soc);
+    std::vector<double> w;
+    solve_k(ctx, dc, p.lat.Q, nev, nullptr, w);
+    for (int q = 0; q < p.nq(); ++q)
+      for (int n = 0; n < p.nband; ++n)
+        eband[(size_t)q * p.nband + n] = n < nh ? spinor_eig(w, nev, q, n, dc.soc) - off : 0.0;
+    return (int)PMX_OK;
+  });
+}
+
+// ======================================================================= stage 2
+namespace {
+
+struct Transitions {
+  std::vector<int> ncd, nvd, cbase, vbase, cidx, vidx;
+  std::vector<long long> blkoff, dest;
+  std::vector<double> dE, wgt;
+  std::vector<int> f0;
+  long long T = 0;
+};
+
+// Occupations and transition list of one q (src/pmx_chi.cpp:391-397, :477-483):
+// conduction states are counted down from the top of the NBAND window while
+// E - E_ref > 0, valence states up from the bottom while E - E_ref <= 0.
+Transitions build_transitions(const Problem& p, int soc, int nev, const std::vector<double>& wk,
+                              const std::vector<double>& wq, double off, bool sort_by_window) {
+  Transitions T;
+  const int nk = p.nk(), NB = p.nband;
+  T.ncd.resize(nk);
+  T.nvd.resize(nk);
+  T.cbase.resize(nk);
+  T.vbase.resize(nk);
+  T.blkoff.resize(nk);
+  struct Raw {
+    long long src;
+    double dE, w;
+    int f0;
+  };
+  std::vector<Raw> raw;
+  long long blk = 0;
+  const double df = p.dfreq, w0 = p.freq.empty() ? 0.0 : p.freq[0];
+  for (int k = 0; k < nk; ++k) {
+    int nc = 0, nv = 0;
+    while (nc < NB && spinor_eig(wk, nev, k, NB - 1 - nc, soc) - off > 0) ++nc;
+    while (nv < NB && spinor_eig(wq, nev, k, nv, soc) - off <= 0) ++nv;
+    // distinct solved states
+    std::vector<int> cs, vs;
+    for (int c = 0; c < nc; ++c) {
+      const int st = soc ? NB - 1 - c : (NB - 1 - c) / 2;
+      if (cs.empty() || cs.back() != st) cs.push_back(st);
+    }
+    for (int v = 0; v < nv; ++v) {
+      const int st = soc ? v : v / 2;
+      if (vs.empty() || vs.back() != st) vs.push_back(st);
+    }
+    T.ncd[k] = (int)cs.size();
+    T.nvd[k] = (int)vs.size();
+    T.cbase[k] = (int)T.cidx.size();
+    T.vbase[k] = (int)T.vidx.size();
+    T.cidx.insert(T.cidx.end(), cs.begin(), cs.end());
+    T.vidx.insert(T.vidx.end(), vs.begin(), vs.end());
+    T.blkoff[k] = blk;
+    for (size_t ic = 0; ic < cs.size(); ++ic)
+      for (size_t iv = 0; iv < vs.size(); ++iv) {
+        int mult = 1;
+        if (!soc) {
+          // spin copies (2 st + sigma) present on both sides with equal spin
+          mult = 0;
+          for (int sg = 0; sg < 2; ++sg) {
+            const int sc = 2 * cs[ic] + sg, sv = 2 * vs[iv] + sg;
+            const int c = NB - 1 - sc;
+            if (sc <= NB - 1 && c >= 0 && c < nc && sv < nv) ++mult;
+          }
+        }
+        const long long src = blk + (long long)ic * vs.size() + iv;
+        if (mult == 0) continue;
+        const int s_c = soc ? cs[ic] : 2 * cs[ic];
+        const int s_v = soc ? vs[iv] : 2 * vs[iv];
+        const double ec = spinor_eig(wk, nev, k, s_c, soc) - off;
+        const double ev = spinor_eig(wq, nev, k, s_v, soc) - off;
+        const double de = ec - ev;
+        raw.push_back({src, de, p.KW[k] * mult, (int)((de - w0) / df)});
+      }
+    blk += (long long)cs.size() * vs.size();
+  }
+  if (sort_by_window)
+    std::stable_sort(raw.begin(), raw.end(), [](const Raw& a, const Raw& b) { return a.f0 < b.f0; });
+  T.T = (long long)raw.size();
+  T.dest.assign(std::max<long long>(blk, 1), -1);
+  T.dE.resize(raw.size());
+  T.wgt.resize(raw.size());
+  T.f0.resize(raw.size());
+  for (size_t t = 0; t < raw.size(); ++t) {
+    T.dest[raw[t].src] = (long long)t;
+    T.dE[t] = raw[t].dE;
+    T.wgt[t] = raw[t].w;
+    T.f0[t] = raw[t].f0;
+  }
+  return T;
+}
+
+int window_half(const Problem& p) {
+  const double df = p.dfreq;
+  const int g = std::max(1, int(6.0 * p.epsilon / df));
+  const int l = std::max(1, int(50.0 * p.epsilon / df));
+  return p.delta == 1 ? l : g;
+}
+
+}  // namespace
+
+extern "C" int pmx_chi(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision, double* re, double* im) {
+  if (!P || (sw != PMX_SWITCH_EPSIJ && sw != PMX_SWITCH_EPSLL)) return PMX_ERR_INVALID;
+  if (precision != PMX_PREC_FP64 && precision != PMX_PREC_MIXED) return PMX_ERR_INVALID;
+  return guarded(ctx, [&]() -> int {
+    const Problem& p = P->p;
+    cudaStream_t st = ctx->stream;
+    for (double& t : ctx->stage_ms) t = 0;
+    if (!p.have_freq || p.nfreq <= 0 || !(p.dfreq > 0))
+      throw std::runtime_error("-nfreq and -dfreq are required for the chi switches");
+    if (p.nband > 2 * p.npw()) throw std::runtime_error("-nband exceeds the Hamiltonian dimension");
+    if (p.nband <= 0) throw std::runtime_error("-nband must be positive");
+    if (!re || !im) return (int)PMX_ERR_INVALID;
+    const int mode = sw == PMX_SWITCH_EPSLL ? 1 : 0;
+    const int nk = p.nk(), nq = p.nq(), neps = p.neps, nf = p.nfreq;
+    const int np = neps * (neps + 1) / 2;
+    const size_t blkvals = (size_t)9 * np * nf;  // one q, one of Re/Im
+    DevCrystal dc;
+    double off;
+    std::vector<double> wk;
+    {
+      Timer tm(ctx, 0);
+      dc = upload_crystal(ctx, P, 0);
+      off = ref_energy(ctx, P, dc);
+    }
+    const int nev = solved_states(p.nband, dc.soc);
+    const int n = dc.n;
+    const int nch = (mode == 0 && dc.soc) ? 4 : 1;
+    CK(ctx->zk.ensure(std::max<size_t>(sizeof(double2) * (size_t)nk * nev * n, 16)));
+    CK(ctx->zq.ensure(std::max<size_t>(sizeof(double2) * (size_t)nk * nev * n, 16)));
+    {
+      Timer tm(ctx, 0);
+      solve_k(ctx, dc, p.K, nev, ctx->zk.as<double2>(), wk);
+    }
+    // static tables of the chi stage
+    h2d(ctx, ctx->loci, p.loci.data(), sizeof(int) * p.loci.size());
+    std::vector<double> kp(3 * (size_t)nk);
+    for (int k = 0; k < nk; ++k)
+      for (int x = 0; x < 3; ++x) kp[3 * k + x] = p.K[k][x];
+    h2d(ctx, ctx->kpts, kp.data(), sizeof(double) * kp.size());
+    // scale factors (src/pmx_chi.cpp:341, src/pmx_chi_copy.cpp:351-360)
+    const double a_cm = p.lat.a * pmx::kAngstrom, bz = p.lat.bz_volume;
+    pmx::dev::ScaleArgs sa{};
+    sa.mode = mode;
+    sa.np = np;
+    sa.nf = nf;
+    sa.dfreq = p.dfreq;
+    sa.sf = 4.0 * bz * std::pow(pmx::kPi, 5) * std::pow(pmx::kHbar, 4) * std::pow(pmx::kE, 2) /
+            (std::pow(pmx::kEV, 3) * std::pow(pmx::kEm, 2) * std::pow(a_cm, 5));
+    sa.sf_ll = 2.0 * bz * std::pow(pmx::kE, 2) / (pmx::kPi * pmx::kEV * a_cm);
+    sa.sf_tt = 32.0 * bz * std::pow(pmx::kPi, 3) * std::pow(pmx::kHbar, 4) * std::pow(pmx::kE, 2) /
+               (std::pow(pmx::kEV, 3) * std::pow(pmx::kEm, 2) * std::pow(a_cm, 5));
+    sa.sf_lt = 8.0 * bz * pmx::kPi * std::pow(pmx::kHbar, 2) * std::pow(pmx::kE, 2) /
+               (std::pow(pmx::kEV, 2) * pmx::kEm * std::pow(a_cm, 3));
+    const int W = mode == 0 ? window_half(p) : -1;
+    const int FT = pmx::dev::contract_ftile();
+    const int nft = (nf + FT - 1) / FT;
+    CK(ctx->acc.ensure(sizeof(double) * 2 * blkvals));
+    CK(ctx->chi.ensure(sizeof(double) * 2 * blkvals));
+    CK(ctx->chi2.ensure(sizeof(double) * 2 * blkvals));
+    const bool pv = mode == 1 && p.kk == 0;
+    if (pv) CK(ctx->accpv.ensure(sizeof(double) * 2 * blkvals));
+
+    for (int q = 0; q < nq; ++q) {
+      const Vec3 Q = p.lat.Q[q];
+      std::vector<Vec3> kq(nk);
+      for (int k = 0; k < nk; ++k) kq[k] = p.K[k] + Q;
+      std::vector<double> wq;
+      {
+        Timer tm(ctx, 0);
+        solve_k(ctx, dc, kq, nev, ctx->zq.as<double2>(), wq);
+      }
+      Transitions T = build_transitions(p, dc.soc, nev, wk, wq, off, mode == 0);
+      // per-m polarisation and SOC-current tables
+      std::vector<double2> uv((size_t)neps * 9), ss((size_t)neps * 3);
+      std::vector<double> qg(neps);
+      for (int m = 0; m < neps; ++m) {
+        const Vec3 v = Q + p.G[m];
+        qg[m] = pmx::norm(v);
+        double u[3][3][2];
+        pmx::uvec_LT(v, u);
+        std::complex<double> vs[3];
+        soc_current(p, p.G[m], vs);
+        for (int i = 0; i < 3; ++i) {
+          std::complex<double> s(0, 0);
+          for (int x = 0; x < 3; ++x) {
+            uv[((size_t)m * 3 + i) * 3 + x] = make_double2(u[i][x][0], u[i][x][1]);
+            s += std::conj(std::complex<double>(u[i][x][0], u[i][x][1])) * vs[x];
+          }
+          ss[(size_t)m * 3 + i] = make_double2(s.real(), s.imag());
+        }
+      }
+      h2d(ctx, ctx->uvec, uv.data(), sizeof(double2) * uv.size());
+      h2d(ctx, ctx->ssoc, ss.data(), sizeof(double2) * ss.size());
+      h2d(ctx, ctx->qgn, qg.data(), sizeof(double) * qg.size());
+      h2d(ctx, ctx->ncd, T.ncd.data(), sizeof(int) * T.ncd.size());
+      h2d(ctx, ctx->nvd, T.nvd.data(), sizeof(int) * T.nvd.size());
+      h2d(ctx, ctx->cbase, T.cbase.data(), sizeof(int) * T.cbase.size());
+      h2d(ctx, ctx->vbase, T.vbase.data(), sizeof(int) * T.vbase.size());
+      h2d(ctx, ctx->cidx, T.cidx.data(), sizeof(int) * T.cidx.size());
+      h2d(ctx, ctx->vidx, T.vidx.data(), sizeof(int) * T.vidx.size());
+      h2d(ctx, ctx->blkoff, T.blkoff.data(), sizeof(long long) * T.blkoff.size());
+      h2d(ctx, ctx->dest, T.dest.data(), sizeof(long long) * T.dest.size());
+      h2d(ctx, ctx->dE, T.dE.data(), sizeof(double) * T.dE.size());
+      h2d(ctx, ctx->wgt, T.wgt.data(), sizeof(double) * T.wgt.size());
+      h2d(ctx, ctx->f0, T.f0.data(), sizeof(int) * T.f0.size());
+      // frequency-tile transition ranges
+      std::vector<int2> tr(nft);
+      for (int ft = 0; ft < nft; ++ft) {
+        if (W < 0) {
+          tr[ft] = make_int2(0, (int)T.T);
+        } else {
+          const int flo = ft * FT, fhi = std::min(nf, flo + FT) - 1;
+          const auto b = std::lower_bound(T.f0.begin(), T.f0.end(), flo - W);
+          const auto e = std::upper_bound(T.f0.begin(), T.f0.end(), fhi + W);
+          tr[ft] = make_int2((int)(b - T.f0.begin()), (int)(e - T.f0.begin()));
+        }
+      }
+      h2d(ctx, ctx->trange, tr.data(), sizeof(int2) * tr.size());
+      const int A = 3 * neps;
+      CK(ctx->M.ensure(std::max<size_t>(sizeof(double2) * (size_t)T.T * A * nch, 16)));
+      // overlaps
+      if (T.T > 0) {
+        Timer tm(ctx, 1);
+        pmx::dev::OverlapArgs oa{};
+        oa.n = n;
+        oa.npw = dc.npw;
+        oa.soc = dc.soc;
+        oa.nev = nev;
+        oa.neps = neps;
+        oa.nch = nch;
+        oa.mode = mode;
+        oa.ncd_max = *std::max_element(T.ncd.begin(), T.ncd.end());
+        oa.nvd_max = *std::max_element(T.nvd.begin(), T.nvd.end());
+        int cchunk = std::max(1, oa.ncd_max);
+        while (cchunk > 1 && pmx::dev::overlap_smem_bytes(cchunk, oa.nvd_max, n, dc.npw) > 200 * 1024) --cchunk;
+        if (pmx::dev::overlap_smem_bytes(cchunk, oa.nvd_max, n, dc.npw) > 220 * 1024)
+          throw CudaFail("overlap tile does not fit in shared memory", PMX_ERR_UNSUPPORTED);
+        oa.cchunk = cchunk;
+        oa.zk = ctx->zk.as<double2>();
+        oa.zq = ctx->zq.as<double2>();
+        oa.ncd = ctx->ncd.as<int>();
+        oa.nvd = ctx->nvd.as<int>();
+        oa.cbase = ctx->cbase.as<int>();
+        oa.vbase = ctx->vbase.as<int>();
+        oa.cidx = ctx->cidx.as<int>();
+        oa.vidx = ctx->vidx.as<int>();
+        oa.blkoff = ctx->blkoff.as<long long>();
+        oa.dest = ctx->dest.as<long long>();
+        oa.loci = ctx->loci.as<int>();
+        oa.G = ctx->g.as<double>();
+        oa.kpts = ctx->kpts.as<double>();
+        oa.q[0] = Q.x;
+        oa.q[1] = Q.y;
+        oa.q[2] = Q.z;
+        oa.uvec = ctx->uvec.as<double2>();
+        oa.ssoc = ctx->ssoc.as<double2>();
+        oa.M = ctx->M.as<double2>();
+        CK(pmx::dev::launch_overlap(oa, nk, st));
+        ctx->launches += 1;
+      }
+      // contraction
+      {
+        Timer tm(ctx, 2);
+        pmx::dev::ContractArgs ca{};
+        ca.M = ctx->M.as<double2>();
+        ca.dE = ctx->dE.as<double>();
+        ca.wgt = ctx->wgt.as<double>();
+        ca.f0 = ctx->f0.as<int>();
+        ca.trange = ctx->trange.as<int2>();
+        ca.neps = neps;
+        ca.np = np;
+        ca.nf = nf;
+        ca.nch = nch;
+        ca.window = W;
+        ca.delta = p.delta;
+        ca.eps = p.epsilon;
+        ca.dfreq = p.dfreq;
+        ca.acc = ctx->acc.as<double>();
+        ca.acc_pv = pv ? ctx->accpv.as<double>() : nullptr;
+        if (precision == PMX_PREC_FP64 || pv) {
+          CK(pmx::dev::launch_contract_f64(ca, st));
+          ctx->launches += 1;
+        } else {
+          int nl = 0;
+          CK(ctx->mixws.ensure(std::max<size_t>(pmx::dev::mixed_workspace_bytes(ca, (long long)T.T), 16)));
+          CK(pmx::dev::launch_contract_mixed(ca, (long long)T.T, ctx->mixws.ptr, nl, st));
+          ctx->launches += nl;
+        }
+      }
+      // scaling and Kramers-Kronig
+      {
+        Timer tm(ctx, 3);
+        sa.qgn = ctx->qgn.as<double>();
+        sa.acc = ctx->acc.as<double>();
+        sa.acc_pv = pv ? ctx->accpv.as<double>() : nullptr;
+        sa.out = ctx->chi.as<double>();
+        CK(pmx::dev::launch_scale(sa, st));
+        ctx->launches += 1;
+        if (p.kk) {
+          CK(pmx::dev::launch_kk(ctx->chi.as<double>(), ctx->chi2.as<double>(), 9 * np, nf, p.dfreq, st));
+          ctx->launches += 1;
+        }
+      }
+      // copy out into [i][j][q][m][n][f]
+      {
+        Timer tm(ctx, 4);
+        const double* res = p.kk ? ctx->chi2.as<double>() : ctx->chi.as<double>();
+        const size_t row = (size_t)np * nf * sizeof(double);
+        CK(cudaMemcpy2DAsync(re + (size_t)q * np * nf, row * nq, res, row, row, 9, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpy2DAsync(im + (size_t)q * np * nf, row * nq, res + blkvals, row, row, 9,
+                             cudaMemcpyDeviceToHost, st));
+      }
+    }
+    CK(cudaStreamSynchronize(st));
+    return (int)PMX_OK;
+  });
+}
+
+extern "C" int pmx_kk(pmx_ctx* ctx, int nrows, int nfreq, double dfreq, double* re, double* im) {
+  if (nrows < 0 || nfreq <= 0 || (nrows > 0 && (!re || !im))) return PMX_ERR_INVALID;
+  return guarded(ctx, [&]() {
+    const size_t blk = (size_t)nrows * nfreq;
+    if (blk == 0) return (int)PMX_OK;
+    CK(ctx->chi.ensure(sizeof(double) * 2 * blk));
+    CK(ctx->chi2.ensure(sizeof(double) * 2 * blk));
+    CK(cudaMemcpyAsync(ctx->chi.ptr, re, sizeof(double) * blk, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->chi.as<double>() + blk, im, sizeof(double) * blk, cudaMemcpyHostToDevice, ctx->stream));
+    CK(pmx::dev::launch_kk(ctx->chi.as<double>(), ctx->chi2.as<double>(), nrows, nfreq, dfreq, ctx->stream));
+    ctx->launches += 1;
+    CK(cudaMemcpyAsync(re, ctx->chi2.ptr, sizeof(double) * blk, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(im, ctx->chi2.as<double>() + blk, sizeof(double) * blk, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return (int)PMX_OK;
+  });
+}
