@@ -1,0 +1,254 @@
+"""ctypes binding of the picomax B200 C-ABI (include/picomax.h).
+
+The shared library is built in-tree by ``picomax_b200/csrc/Makefile`` into
+``picomax_b200/lib/libpicomax_b200.so``. There is no CPU implementation of the
+two GPU stages: if the library is missing this module raises, and the stage
+functions return ``PMX_ERR_NO_DEVICE`` when no CUDA device is visible.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_char_p, c_double, c_int, c_longlong, c_size_t, c_void_p
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libpicomax_b200.so")
+CLI_PATH = os.path.join(_HERE, "bin", "picomax")
+
+PMX_OK = 0
+PMX_ERR_INVALID = 1
+PMX_ERR_CUDA = 2
+PMX_ERR_NOCONV = 3
+PMX_ERR_TIMEOUT = 4
+PMX_ERR_NO_DEVICE = 5
+PMX_ERR_UNSUPPORTED = 6
+
+SWITCH_NONE, SWITCH_BAND, SWITCH_EPSIJ, SWITCH_EPSLL = 0, 1, 2, 3
+PREC_FP64, PREC_MIXED = 0, 1
+
+# Every entry point declared in include/picomax.h.
+EXPORTS = (
+    "pmx_problem_create", "pmx_problem_destroy", "pmx_problem_get_info", "pmx_problem_gvectors",
+    "pmx_problem_loci", "pmx_problem_kpoints", "pmx_problem_qpoints", "pmx_problem_dump",
+    "pmx_problem_write_gpt", "pmx_ctx_create", "pmx_ctx_destroy", "pmx_ctx_last_error",
+    "pmx_ctx_stage_times", "pmx_ctx_kernel_launches", "pmx_hamiltonian", "pmx_heev_batched",
+    "pmx_ref_energy", "pmx_band", "pmx_chi", "pmx_kk", "pmx_main",
+)
+
+
+class ProblemInfo(ctypes.Structure):
+    _fields_ = [
+        ("npw", c_int), ("nh", c_int), ("soc", c_int), ("neps", c_int), ("nband", c_int),
+        ("nvalence", c_int), ("nk", c_int), ("nq", c_int), ("nfreq", c_int), ("natom", c_int),
+        ("sw", c_int), ("debug", c_int), ("kk", c_int), ("delta", c_int), ("epsilon", c_double),
+        ("dfreq", c_double), ("a", c_double), ("gcut", c_double), ("bz_volume", c_double),
+        ("chi_values", c_longlong),
+    ]
+
+
+class PicomaxError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{msg} (status {status})")
+        self.status = status
+
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Loads the in-tree shared library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C picomax_b200/csrc`")
+    lib = ctypes.CDLL(LIB_PATH)
+    dp, ip = POINTER(c_double), POINTER(c_int)
+    sig = {
+        "pmx_problem_create": (c_int, [c_int, POINTER(c_char_p), POINTER(c_void_p)]),
+        "pmx_problem_destroy": (None, [c_void_p]),
+        "pmx_problem_get_info": (c_int, [c_void_p, POINTER(ProblemInfo)]),
+        "pmx_problem_gvectors": (c_int, [c_void_p, dp, ip]),
+        "pmx_problem_loci": (c_int, [c_void_p, ip]),
+        "pmx_problem_kpoints": (c_int, [c_void_p, dp, dp]),
+        "pmx_problem_qpoints": (c_int, [c_void_p, dp]),
+        "pmx_problem_dump": (c_int, [c_void_p, c_char_p, c_size_t, POINTER(c_size_t)]),
+        "pmx_problem_write_gpt": (c_int, [c_void_p]),
+        "pmx_ctx_create": (c_int, [c_int, POINTER(c_void_p)]),
+        "pmx_ctx_destroy": (None, [c_void_p]),
+        "pmx_ctx_last_error": (c_char_p, [c_void_p]),
+        "pmx_ctx_stage_times": (c_int, [c_void_p, dp]),
+        "pmx_ctx_kernel_launches": (c_longlong, [c_void_p]),
+        "pmx_hamiltonian": (c_int, [c_void_p, c_void_p, dp, c_int, dp]),
+        "pmx_heev_batched": (c_int, [c_void_p, c_int, c_int, dp, c_int, dp, dp]),
+        "pmx_ref_energy": (c_int, [c_void_p, c_void_p, dp]),
+        "pmx_band": (c_int, [c_void_p, c_void_p, dp]),
+        "pmx_chi": (c_int, [c_void_p, c_void_p, c_int, c_int, dp, dp]),
+        "pmx_kk": (c_int, [c_void_p, c_int, c_int, c_double, dp, dp]),
+        "pmx_main": (c_int, [c_int, POINTER(c_char_p)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(POINTER(c_double))
+
+
+def _iptr(a: np.ndarray):
+    return a.ctypes.data_as(POINTER(c_int))
+
+
+def _argv(args) -> tuple:
+    toks = ["picomax"] + [str(a) for a in args]
+    arr = (c_char_p * len(toks))(*[t.encode() for t in toks])
+    return len(toks), arr
+
+
+class Problem:
+    """A parsed picomax invocation (argv without the program name)."""
+
+    def __init__(self, args):
+        lib = load()
+        self._lib = lib
+        self.args = list(args)
+        argc, argv = _argv(self.args)
+        h = c_void_p()
+        st = lib.pmx_problem_create(argc, argv, ctypes.byref(h))
+        if st != PMX_OK:
+            raise PicomaxError(st, "pmx_problem_create rejected the options")
+        self.handle = h
+        info = ProblemInfo()
+        lib.pmx_problem_get_info(h, ctypes.byref(info))
+        self.info = info
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.pmx_problem_destroy(self.handle)
+            self.handle = None
+
+    __del__ = close
+
+    def gvectors(self):
+        n = self.info.npw
+        G = np.zeros((n, 3), np.float64)
+        H = np.zeros((n, 3), np.int32)
+        self._lib.pmx_problem_gvectors(self.handle, _dptr(G), _iptr(H))
+        return G, H
+
+    def loci(self):
+        L = np.zeros((self.info.neps, self.info.npw), np.int32)
+        self._lib.pmx_problem_loci(self.handle, _iptr(L))
+        return L
+
+    def kpoints(self):
+        K = np.zeros((self.info.nk, 3), np.float64)
+        W = np.zeros(self.info.nk, np.float64)
+        self._lib.pmx_problem_kpoints(self.handle, _dptr(K), _dptr(W))
+        return K, W
+
+    def qpoints(self):
+        Q = np.zeros((self.info.nq, 3), np.float64)
+        if self.info.nq:
+            self._lib.pmx_problem_qpoints(self.handle, _dptr(Q))
+        return Q
+
+    def dump(self) -> str:
+        need = c_size_t()
+        self._lib.pmx_problem_dump(self.handle, None, 0, ctypes.byref(need))
+        buf = ctypes.create_string_buffer(need.value)
+        self._lib.pmx_problem_dump(self.handle, buf, need.value, ctypes.byref(need))
+        return buf.value.decode()
+
+
+class Context:
+    """Device context (one CUDA stream and its workspaces) on `device`."""
+
+    def __init__(self, device: int = 0):
+        lib = load()
+        self._lib = lib
+        h = c_void_p()
+        st = lib.pmx_ctx_create(device, ctypes.byref(h))
+        if st != PMX_OK:
+            raise PicomaxError(st, "pmx_ctx_create failed (a CUDA device is required)")
+        self.handle = h
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.pmx_ctx_destroy(self.handle)
+            self.handle = None
+
+    __del__ = close
+
+    def _check(self, st, what):
+        if st != PMX_OK:
+            raise PicomaxError(st, f"{what}: {self._lib.pmx_ctx_last_error(self.handle).decode()}")
+
+    def stage_times(self):
+        ms = np.zeros(5, np.float64)
+        self._lib.pmx_ctx_stage_times(self.handle, _dptr(ms))
+        return ms
+
+    def kernel_launches(self) -> int:
+        return int(self._lib.pmx_ctx_kernel_launches(self.handle))
+
+    def hamiltonian(self, prob: Problem, kpts) -> np.ndarray:
+        k = np.ascontiguousarray(kpts, np.float64).reshape(-1, 3)
+        nh = prob.info.nh
+        out = np.zeros((len(k), nh, nh, 2), np.float64)
+        self._check(self._lib.pmx_hamiltonian(self.handle, prob.handle, _dptr(k), len(k), _dptr(out)), "hamiltonian")
+        # stored column-major: out[k][col][row]
+        return (out[..., 0] + 1j * out[..., 1]).transpose(0, 2, 1)
+
+    def heev(self, A, nev: int, vectors: bool = True):
+        """Lowest `nev` eigenpairs of Hermitian matrices A [batch, n, n]."""
+        A = np.asarray(A, np.complex128)
+        b, n, _ = A.shape
+        colmajor = np.ascontiguousarray(A.transpose(0, 2, 1))
+        buf = np.ascontiguousarray(np.stack([colmajor.real, colmajor.imag], -1))
+        w = np.zeros((b, nev), np.float64)
+        z = np.zeros((b, nev, n, 2), np.float64) if vectors else None
+        st = self._lib.pmx_heev_batched(self.handle, n, b, _dptr(buf), nev, _dptr(w),
+                                        _dptr(z) if vectors else None)
+        self._check(st, "heev_batched")
+        if not vectors:
+            return w, None
+        zc = z[..., 0] + 1j * z[..., 1]  # [b][nev][n]
+        return w, zc.transpose(0, 2, 1)
+
+    def ref_energy(self, prob: Problem) -> float:
+        off = c_double()
+        self._check(self._lib.pmx_ref_energy(self.handle, prob.handle, ctypes.byref(off)), "ref_energy")
+        return off.value
+
+    def band(self, prob: Problem) -> np.ndarray:
+        out = np.zeros((prob.info.nq, prob.info.nband), np.float64)
+        self._check(self._lib.pmx_band(self.handle, prob.handle, _dptr(out)), "band")
+        return out
+
+    def chi(self, prob: Problem, switch: int, precision: int = PREC_FP64):
+        n = prob.info.chi_values
+        re = np.zeros(n, np.float64)
+        im = np.zeros(n, np.float64)
+        self._check(self._lib.pmx_chi(self.handle, prob.handle, switch, precision, _dptr(re), _dptr(im)), "chi")
+        return re, im
+
+    def kk(self, re, im, dfreq: float):
+        re = np.ascontiguousarray(re, np.float64).copy()
+        im = np.ascontiguousarray(im, np.float64).copy()
+        rows, nf = re.shape
+        self._check(self._lib.pmx_kk(self.handle, rows, nf, dfreq, _dptr(re), _dptr(im)), "kk")
+        return re, im
+
+
+def run_main(args) -> int:
+    """Runs the whole picomax program in-process (pmx_main)."""
+    lib = load()
+    argc, argv = _argv(args)
+    return int(lib.pmx_main(argc, argv))

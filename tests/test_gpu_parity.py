@@ -1,0 +1,111 @@
+"""CUDA path (through the C-ABI) against the reference rebuilt from source
+(golden fixtures) and against the numpy restatement.
+
+Tolerances (FP64 path): band energies 1e-9 eV absolute; chi spectra 1e-8 of
+the largest |value| of the spectrum set (the reference itself is not
+bit-reproducible run to run, ~3e-16 relative); Kramers-Kronig 1e-10 relative.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import golden_args, load_golden
+
+import picomax_b200 as pm
+import pmx_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+CHI_CASES = ["si_epsij", "gaas_soc_epsij", "si_epsLL", "gaas_soc_epsLL_pv", "wz_epsij_rect"]
+
+
+@pytest.mark.parametrize("name", ["si_band", "gaas_soc_band"])
+def test_band_vs_reference(ctx, name, tmp_path):
+    g = load_golden(name)
+    p = pm.Problem(golden_args(g, tmp_path))
+    eb = ctx.band(p)
+    assert np.max(np.abs(eb.ravel() - g["dat"])) < 1e-9
+
+
+@pytest.mark.parametrize("name", CHI_CASES)
+def test_chi_fp64_vs_reference(ctx, name, tmp_path):
+    g = load_golden(name)
+    args = golden_args(g, tmp_path)
+    p = pm.Problem(args)
+    sw = pm.SWITCH_EPSLL if "epsLL" in args else pm.SWITCH_EPSIJ
+    re, im = ctx.chi(p, sw, pm.PREC_FP64)
+    n = re.size
+    ref_re, ref_im = g["dat"][:n], g["dat"][n:]
+    scale = max(np.abs(ref_re).max(), np.abs(ref_im).max())
+    assert np.max(np.abs(re - ref_re)) <= 1e-8 * scale
+    assert np.max(np.abs(im - ref_im)) <= 1e-8 * scale
+
+
+def test_hamiltonian_vs_oracle(ctx):
+    args = ("-crystal zb -a 5.65 -encut 40 -vg 3,4,8,11,0.1,-0.2,0.05,0.02,-0.1,0.1,0.03,-0.01 "
+            "-use_uniform_us_so -uniform_us_so_val 0.01 -ua_so 3:0.004,8:0.002").split()
+    p = pm.Problem(args)
+    cr, mat, gcut, _ = O.from_args(args)
+    G, _ = p.gvectors()
+    ks = np.array([[0.1, 0.2, 0.3], [0.5, 0.5, 0.5]])
+    H = ctx.hamiltonian(p, ks)
+    for k, h in zip(ks, H):
+        ref = O.hamiltonian(cr, mat, G, k)
+        assert np.max(np.abs(h - ref)) < 1e-12 * np.max(np.abs(ref))
+
+
+def _random_hermitian(rng, n, degenerate=False):
+    A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    A = (A + A.conj().T) / 2
+    if degenerate:  # exact pairs, as the doubled spinor spectrum without SOC
+        h = n // 2
+        B = A[:h, :h]
+        U, _ = np.linalg.qr(rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+        A = U @ np.kron(B, np.eye(2)) @ U.conj().T
+        A = (A + A.conj().T) / 2
+    return A
+
+
+@pytest.mark.parametrize("n,degenerate", [(40, False), (113, False), (120, True), (226, False), (300, True)])
+def test_heev_vs_numpy(ctx, n, degenerate):
+    rng = np.random.default_rng(n)
+    A = np.stack([_random_hermitian(rng, n, degenerate) for _ in range(3)])
+    nev = 16
+    w, Z = ctx.heev(A, nev)
+    for b in range(3):
+        ref = np.linalg.eigvalsh(A[b])[:nev]
+        scale = np.max(np.abs(np.linalg.eigvalsh(A[b])))
+        assert np.max(np.abs(w[b] - ref)) < 1e-12 * scale * n
+        R = A[b] @ Z[b] - Z[b] * w[b]
+        assert np.max(np.linalg.norm(R, axis=0)) < 1e-10 * scale
+        assert np.max(np.abs(Z[b].conj().T @ Z[b] - np.eye(nev))) < 1e-10
+
+
+def test_kk_vs_oracle(ctx):
+    rng = np.random.default_rng(3)
+    nf, rows, dw = 300, 7, 0.05
+    re = rng.standard_normal((rows, nf))
+    im = rng.standard_normal((rows, nf))
+    r1, i1 = ctx.kk(re, im, dw)
+    r0, i0 = O.kk_transform(re, im, dw * np.arange(nf), dw)
+    assert np.max(np.abs(r1 - r0)) < 1e-10 * np.max(np.abs(r0))
+    assert np.max(np.abs(i1 - i0)) < 1e-10 * np.max(np.abs(i0))
+
+
+@pytest.mark.parametrize("name", ["si_band", "si_epsLL", "gaas_soc_epsij"])
+def test_cli_files_vs_reference(name, tmp_path):
+    """The picomax executable writes byte-compatible .dat/.gpt files."""
+    g = load_golden(name)
+    args = golden_args(g, tmp_path)
+    r = subprocess.run([pm.CLI_PATH] + args + ["-wdir", str(tmp_path), "-outputfile", "out"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout[-2000:]
+    dat = np.fromfile(os.path.join(tmp_path, "out.dat"), np.float64)
+    assert dat.size == g["dat"].size
+    scale = np.abs(g["dat"]).max()
+    tol = 1e-9 if name.endswith("band") else 1e-8 * scale
+    assert np.max(np.abs(dat - g["dat"])) <= tol
+    if "gpt" in g:
+        assert np.array_equal(np.fromfile(os.path.join(tmp_path, "out.gpt"), np.float64), g["gpt"])
