@@ -283,7 +283,6 @@ __global__ void __launch_bounds__(kHeevThreads) heev_kernel(const EigItem* __res
       e[j] = beta;
       tau[j] = tj;
       vcur[j + 1] = make_double2(1, 0);
-      A[(long long)j * n + j + 1] = make_double2(1, 0);
     }
     __syncthreads();
     const bool active = tj.x != 0.0 || tj.y != 0.0;
@@ -316,6 +315,9 @@ __global__ void __launch_bounds__(kHeevThreads) heev_kernel(const EigItem* __res
       vprev[r] = vcur[r];
       wprev[r] = active ? cadd(y[r], cmul(al, vcur[r])) : make_double2(0, 0);
     }
+    // v_j(0) = 1 is stored for the back-transform only after every thread
+    // has read alpha = A[j+1, j] above.
+    if (tid == 0) A[(long long)j * n + j + 1] = make_double2(1, 0);
     pending = active;
     __syncthreads();
   }
