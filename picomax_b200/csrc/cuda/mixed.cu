@@ -1,14 +1,583 @@
-// Mixed-precision chi contraction (split-BF16 tcgen05). See pmx_mixed.hpp.
+// Mixed-precision chi contraction on the sm_100a tensor cores.
+//
+// The contraction acc[p, f] = sum_t P[p, t] W[t, f] of the FP64 path (pair
+// products P of the overlaps, broadening weights W inside each transition's
+// window) runs as a GEMM with
+//   rows  = 64 (a, b) pairs x {P1 = w reO, P2 = -w imO}      (M = 128)
+//   cols  = 256 frequencies                                 (N = 256)
+//   depth = transitions of the frequency tile, 32 per chunk (K)
+// Operands are split into BF16 pairs, x = hi + lo, and every chunk issues
+// hi*hi + hi*lo + lo*hi as tcgen05.mma kind::f16 with an FP32 accumulator in
+// TMEM (products dropped: lo*lo, ~2^-16 of each term). The transition range
+// of a frequency tile is cut into pieces; each piece's FP32 partial tile is
+// written out and the pieces are summed in FP64 in a fixed order, so results
+// are deterministic.
+//
+// Pipeline of one CTA (256 threads, two shared-memory stages):
+//   thread 0   bulk-copies the precomputed W chunk (hi and lo, 32 KB, already
+//              in the canonical K-major UMMA layout) into the stage
+//   all        stage the overlaps of the chunk and write the split P tile
+//   thread 0   waits for the W copy, issues 6 MMAs, commits to the stage's
+//              mbarrier; the stage is refilled two chunks later.
+// Every mbarrier wait is bounded; on expiry the CTA records an error code,
+// drains its own MMAs (bounded), frees its TMEM and returns.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <climits>
+#include <cmath>
+#include <vector>
+
+#include "pmx_common.cuh"
 #include "pmx_mixed.hpp"
 
 namespace pmx {
 namespace dev {
 
-size_t mixed_workspace_bytes(const ContractArgs&, long long) { return 0; }
+namespace {
 
-cudaError_t launch_contract_mixed(const ContractArgs&, long long, void*, int& nlaunch, cudaStream_t) {
+constexpr int kM = 128;        // MMA rows
+constexpr int kPairs = 64;     // pairs per tile (kM / 2)
+constexpr int kN = 256;        // frequencies per tile
+constexpr int kKC = 32;        // transitions per chunk
+constexpr int kThreads = 256;
+constexpr int kPieceChunks = 64;  // chunks per K-split piece (2048 transitions)
+constexpr unsigned kWaitLimit = 1u << 24;
+
+// canonical K-major, no-swizzle layout: core matrices of 8 rows x 16 bytes;
+// rows of a core matrix 16 B apart, row groups SBO = 128 B apart, 8-element
+// K chunks LBO = rows/8 * 128 B apart.
+constexpr int kABytes = kM * kKC * 2;  // one of hi/lo: 8 KB
+constexpr int kBBytes = kN * kKC * 2;  // one of hi/lo: 16 KB
+constexpr int kWChunkBytes = 2 * kBBytes;  // hi + lo in global and in the stage
+
+__host__ __device__ constexpr int core_off(int r, int k, int rows) {
+  return ((k >> 3) * (rows >> 3) + (r >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+// kind::f16 instruction descriptor: BF16 x BF16 -> F32, A and B K-major.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kN >> 3) << 17) |
+                            ((uint32_t)(kM >> 4) << 24);
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (unsigned it = 0; it < kWaitLimit; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+      "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(acc)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void async_proxy_fence() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+
+// hi/lo split of 8 values into two 16-byte rows of a core matrix.
+__device__ __forceinline__ void split8(const float* x, uint4& hi, uint4& lo) {
+  float h[8], l[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const __nv_bfloat16 b = __float2bfloat16_rn(x[i]);
+    h[i] = __bfloat162float(b);
+    l[i] = x[i] - h[i];
+  }
+  hi = make_uint4(pack_bf16(h[0], h[1]), pack_bf16(h[2], h[3]), pack_bf16(h[4], h[5]), pack_bf16(h[6], h[7]));
+  lo = make_uint4(pack_bf16(l[0], l[1]), pack_bf16(l[2], l[3]), pack_bf16(l[4], l[5]), pack_bf16(l[6], l[7]));
+}
+
+__device__ __forceinline__ double broaden_m(int model, double eps, double x) {
+  switch (model) {
+    case 0:
+      return exp(-0.5 * x * x / (eps * eps)) / (eps * sqrt(2.0 * 3.14159265358979323846));
+    case 1:
+      return eps / 3.14159265358979323846 / (eps * eps + x * x);
+    case 2:
+      return fabs(x) < 0.5 * eps ? 4.0 / eps * (0.5 - fabs(x) / eps) : 0.0;
+    default:
+      return fabs(x) < 0.5 * eps ? 1.0 / eps : 0.0;
+  }
+}
+
+// ------------------------------------------------------------- work plan
+struct Plan {
+  int nft;           // frequency tiles
+  int ntile;         // pair tiles
+  int nchunk;        // W chunks over all frequency tiles
+  int nitem;         // (frequency tile, piece) items
+  // device arrays inside the workspace
+  int* chunk_ft;     // [nchunk] frequency tile of the chunk
+  int* chunk_t0;     // [nchunk] first sorted transition of the chunk
+  int* chunk_t1;     // [nchunk] end of the frequency tile's range
+  int4* item;        // [nitem] (ft, first chunk, end chunk, -)
+  int2* ft_items;    // [nft] (first item, end item)
+  int2* tiles;       // [ntile] (a block, b block)
+  float* wgt32;      // [T]
+  uint8_t* wbuf;     // [nchunk][32 KB]
+  float* part;       // [nitem][ntile][128][256]
+  int* err;          // error flag
+};
+
+}  // namespace
+
+// -------------------------------------------------------- W chunk producer
+__global__ void __launch_bounds__(256) wgen_kernel(Plan pl, ContractArgs a) {
+  const int c = blockIdx.x;
+  const int ft = pl.chunk_ft[c], t0 = pl.chunk_t0[c], t1 = pl.chunk_t1[c];
+  uint8_t* out = pl.wbuf + (size_t)c * kWChunkBytes;
+  // each thread writes 16-byte rows: (freq n, k-group kg) -> 8 transitions
+  for (int idx = threadIdx.x; idx < kN * (kKC / 8); idx += blockDim.x) {
+    const int n = idx % kN, kg = idx / kN;
+    const int f = ft * kN + n;
+    float x[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int t = t0 + kg * 8 + q;
+      double v = 0.0;
+      if (t < t1 && f < a.nf) {
+        const bool in = a.window < 0 || abs(f - a.f0[t]) <= a.window;
+        if (in) v = broaden_m(a.delta, a.eps, a.dE[t] - a.dfreq * f);
+      }
+      x[q] = (float)v;
+    }
+    uint4 hi, lo;
+    split8(x, hi, lo);
+    const int off = core_off(n, kg * 8, kN);
+    *reinterpret_cast<uint4*>(out + off) = hi;
+    *reinterpret_cast<uint4*>(out + kBBytes + off) = lo;
+  }
+}
+
+// ------------------------------------------------------------- main GEMM
+template <int NCH>
+__global__ void __launch_bounds__(kThreads, 1) mixed_kernel(Plan pl, ContractArgs a, const float2* __restrict__ M32) {
+  const int tile = blockIdx.x, item_id = blockIdx.y;
+  const int2 tb = pl.tiles[tile];
+  const int4 it = pl.item[item_id];
+  const int c_begin = it.y, c_end = it.z;
+  const int A = 3 * a.neps;
+  const int a0 = tb.x * 8, b0 = tb.y * 8;
+  const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31;
+
+  extern __shared__ __align__(1024) uint8_t smem[];
+  // stage layout: [A hi 8K][A lo 8K][B hi 16K][B lo 16K] x 2
+  uint8_t* stage[2] = {smem, smem + 2 * kABytes + kWChunkBytes};
+  float2* sM = reinterpret_cast<float2*>(smem + 2 * (2 * kABytes + kWChunkBytes));  // [kKC][16][NCH]
+  float* sw = reinterpret_cast<float*>(sM + kKC * 16 * NCH);                        // [kKC]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sw + kKC);                            // wfull[2], mdone[2]
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(bars + 4);
+  int* s_abort = reinterpret_cast<int*>(s_tmem + 1);  // s_abort[0], last committed chunk s_abort[1]
+
+  if (wid == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(s_tmem)),
+                 "r"(kN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    for (int i = 0; i < 4; ++i) mbar_init(&bars[i], 1);
+    *s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s_tmem;
+  uint64_t* wfull = bars;
+  uint64_t* mdone = bars + 2;
+
+  // pair handled by this thread for P production: 64 pairs x 4 groups of 8 transitions
+  const int pp = tid >> 2, kg = tid & 3;
+  const int ia = pp >> 3, ib = pp & 7;
+  const int av = a0 + ia, bv = b0 + ib;
+  const bool valid = av < A && bv < A && (av / 3) >= (bv / 3);
+
+  int* s_last = s_abort + 1;  // index (from c_begin) of the last committed chunk, -1 if none
+  if (tid == 0) *s_last = -1;
+  for (int c = c_begin; c < c_end; ++c) {
+    const int n = c - c_begin, s = n & 1;
+    uint8_t* st = stage[s];
+    // the stage is free once the MMAs of chunk n-2 (same stage) completed
+    if (tid == 0 && n >= 2 && !*s_abort && !mbar_wait(&mdone[s], ((n - 2) >> 1) & 1)) {
+      atomicExch(pl.err, 1);
+      *s_abort = 1;
+    }
+    __syncthreads();
+    tc_fence_after();
+    if (*s_abort) break;
+    if (tid == 0) bulk_load(st + 2 * kABytes, pl.wbuf + (size_t)c * kWChunkBytes, kWChunkBytes, &wfull[s]);
+    // stage overlaps and weights of the chunk
+    const int t0 = pl.chunk_t0[c], t1 = pl.chunk_t1[c];
+    for (int idx = tid; idx < kKC * 16 * NCH; idx += kThreads) {
+      const int t = idx / (16 * NCH), rem = idx % (16 * NCH);
+      const int slot = rem / NCH, ch = rem % NCH;
+      const int gt = t0 + t;
+      const int ab = slot < 8 ? a0 + slot : b0 + slot - 8;
+      float2 v = make_float2(0.f, 0.f);
+      if (gt < t1 && ab < A) v = M32[((size_t)gt * A + ab) * NCH + ch];
+      sM[idx] = v;
+    }
+    if (tid < kKC) sw[tid] = (t0 + tid < t1) ? pl.wgt32[t0 + tid] : 0.f;
+    __syncthreads();
+    // split pair products into the A tile: row pp (P1) and 64 + pp (P2)
+    {
+      float p1[8], p2[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int t = kg * 8 + q;
+        float reO = 0.f, imO = 0.f;
+        if (valid) {
+          const float2* ma = sM + ((size_t)t * 16 + ia) * NCH;
+          const float2* mb = sM + ((size_t)t * 16 + 8 + ib) * NCH;
+          if (NCH == 1) {
+            reO = ma[0].x * mb[0].x + ma[0].y * mb[0].y;
+            imO = ma[0].y * mb[0].x - ma[0].x * mb[0].y;
+          } else {
+            // reO = Re(S_a S_b*) - Re(X_a X_b*), S = up + dn, X = ud + du
+            // imO = Im(up_a up_b* + dn_a dn_b* - ud_a ud_b* - du_a du_b*)
+            const float sax = ma[0].x + ma[1].x, say = ma[0].y + ma[1].y;
+            const float sbx = mb[0].x + mb[1].x, sby = mb[0].y + mb[1].y;
+            const float xax = ma[2].x + ma[3].x, xay = ma[2].y + ma[3].y;
+            const float xbx = mb[2].x + mb[3].x, xby = mb[2].y + mb[3].y;
+            reO = (sax * sbx + say * sby) - (xax * xbx + xay * xby);
+            imO = (ma[0].y * mb[0].x - ma[0].x * mb[0].y) + (ma[1].y * mb[1].x - ma[1].x * mb[1].y) -
+                  (ma[2].y * mb[2].x - ma[2].x * mb[2].y) - (ma[3].y * mb[3].x - ma[3].x * mb[3].y);
+          }
+        }
+        p1[q] = sw[t] * reO;
+        p2[q] = -sw[t] * imO;
+      }
+      uint4 h1, l1, h2, l2;
+      split8(p1, h1, l1);
+      split8(p2, h2, l2);
+      const int o1 = core_off(pp, kg * 8, kM), o2 = core_off(kPairs + pp, kg * 8, kM);
+      *reinterpret_cast<uint4*>(st + o1) = h1;
+      *reinterpret_cast<uint4*>(st + kABytes + o1) = l1;
+      *reinterpret_cast<uint4*>(st + o2) = h2;
+      *reinterpret_cast<uint4*>(st + kABytes + o2) = l2;
+    }
+    async_proxy_fence();
+    __syncthreads();
+    if (tid == 0) {
+      if (!mbar_wait(&wfull[s], (n >> 1) & 1)) {
+        atomicExch(pl.err, 2);
+        *s_abort = 1;
+      } else {
+        tc_fence_after();
+        const uint32_t sa = smem_u32(st);
+        const uint32_t sb = sa + 2 * kABytes;
+#pragma unroll
+        for (int ks = 0; ks < kKC / 16; ++ks) {
+          // K step ks covers k-groups 2ks, 2ks+1: +2*LBO bytes
+          const uint64_t ahi = umma_desc(sa + ks * 2 * (kM / 8) * 128, (kM / 8) * 128, 128);
+          const uint64_t alo = umma_desc(sa + kABytes + ks * 2 * (kM / 8) * 128, (kM / 8) * 128, 128);
+          const uint64_t bhi = umma_desc(sb + ks * 2 * (kN / 8) * 128, (kN / 8) * 128, 128);
+          const uint64_t blo = umma_desc(sb + kBBytes + ks * 2 * (kN / 8) * 128, (kN / 8) * 128, 128);
+          const uint32_t acc0 = (n > 0 || ks > 0) ? 1u : 0u;
+          mma_bf16(tmem, ahi, bhi, acc0);
+          mma_bf16(tmem, ahi, blo, 1u);
+          mma_bf16(tmem, alo, bhi, 1u);
+        }
+        mma_commit(&mdone[s]);
+        *s_last = n;
+      }
+    }
+  }
+  __syncthreads();
+  // drain: the last commit completes after every earlier MMA of this thread;
+  // it is waited for on every path before TMEM is read or freed.
+  const int nlast = *s_last;
+  if (tid == 0 && nlast >= 0 && !mbar_wait(&mdone[nlast & 1], (nlast >> 1) & 1)) {
+    atomicExch(pl.err, 3);
+    *s_abort = 1;
+  }
+  __syncthreads();
+  tc_fence_after();
+  const bool have = nlast >= 0 && !*s_abort;
+  // epilogue: TMEM lane r = row r; warps 0-3 read 32 rows each
+  float* out = pl.part + ((size_t)item_id * pl.ntile + tile) * (kM * kN);
+  if (wid < 4) {
+    const int row = wid * 32 + lane;
+    for (int cb = 0; cb < kN; cb += 32) {
+      uint32_t r[32];
+      const uint32_t taddr = tmem + ((uint32_t)(wid * 32) << 16) + cb;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+            "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+            "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+            "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      float4* dst = reinterpret_cast<float4*>(out + (size_t)row * kN + cb);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        float4 v = make_float4(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1]),
+                               __uint_as_float(r[4 * q + 2]), __uint_as_float(r[4 * q + 3]));
+        if (!have) v = make_float4(0.f, 0.f, 0.f, 0.f);
+        dst[q] = v;
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (wid == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kN));
+}
+
+// Sums the FP32 partials of each frequency tile's pieces in FP64, in piece
+// order, and scatters rows to acc[2][9][np][nf] (P1 -> Im, P2 -> Re).
+__global__ void __launch_bounds__(256) reduce_kernel(Plan pl, ContractArgs a) {
+  const int tile = blockIdx.x, ft = blockIdx.y;
+  const int2 tb = pl.tiles[tile];
+  const int2 ir = pl.ft_items[ft];
+  const int A = 3 * a.neps;
+  const size_t blk = (size_t)9 * a.np * a.nf;
+  for (int idx = threadIdx.x; idx < kM * kN; idx += blockDim.x) {
+    const int row = idx / kN, col = idx % kN;
+    const int f = ft * kN + col;
+    if (f >= a.nf) continue;
+    const int pp = row & (kPairs - 1);
+    const int av = tb.x * 8 + (pp >> 3), bv = tb.y * 8 + (pp & 7);
+    if (av >= A || bv >= A) continue;
+    const int m = av / 3, i = av % 3, n = bv / 3, j = bv % 3;
+    if (n > m) continue;
+    double s = 0.0;
+    for (int itm = ir.x; itm < ir.y; ++itm)
+      s += (double)pl.part[((size_t)itm * pl.ntile + tile) * (kM * kN) + idx];
+    const size_t o = ((size_t)(i * 3 + j) * a.np + (size_t)m * (m + 1) / 2 + n) * a.nf + f;
+    if (row < kPairs)
+      a.acc[blk + o] = s;  // Im part
+    else
+      a.acc[o] = s;  // Re part
+  }
+}
+
+// ----------------------------------------------------------------- host side
+namespace {
+
+struct HostPlan {
+  std::vector<int> chunk_ft, chunk_t0, chunk_t1;
+  std::vector<int4> items;
+  std::vector<int2> ft_items, tiles;
+};
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+HostPlan make_plan(const ContractArgs& a, const int2* trange_host, int nft) {
+  HostPlan h;
+  h.ft_items.resize(nft);
+  for (int ft = 0; ft < nft; ++ft) {
+    const int tb = trange_host[ft].x, te = trange_host[ft].y;
+    const int c0 = (int)h.chunk_ft.size();
+    for (int t = tb; t < te; t += kKC) {
+      h.chunk_ft.push_back(ft);
+      h.chunk_t0.push_back(t);
+      h.chunk_t1.push_back(te);
+    }
+    const int c1 = (int)h.chunk_ft.size();
+    const int i0 = (int)h.items.size();
+    for (int c = c0; c < c1; c += kPieceChunks) h.items.push_back(make_int4(ft, c, std::min(c1, c + kPieceChunks), 0));
+    h.ft_items[ft] = make_int2(i0, (int)h.items.size());
+  }
+  const int A = 3 * a.neps, nb = (A + 7) / 8;
+  for (int i = 0; i < nb; ++i)
+    for (int j = 0; j < nb; ++j) {
+      const int amax = std::min(8 * i + 7, A - 1), bmin = 8 * j;
+      if (amax / 3 >= bmin / 3) h.tiles.push_back(make_int2(i, j));
+    }
+  return h;
+}
+}  // namespace
+
+size_t mixed_workspace_bytes(const ContractArgs& a, long long T) {
+  // upper bound: every transition in at most ceil((2W+N)/N)+1 frequency tiles
+  const int nft = (a.nf + kN - 1) / kN;
+  const long long span = a.window < 0 ? nft : std::min<long long>(nft, (2LL * a.window + kN) / kN + 2);
+  const long long nchunk = (T * span + kKC - 1) / kKC + nft + 1;
+  const long long nitem = nchunk / kPieceChunks + nft + 1;
+  const int A = 3 * a.neps, nb = (A + 7) / 8;
+  const long long ntile = (long long)nb * nb;
+  size_t b = 0;
+  b += align256(sizeof(int) * 3 * nchunk);
+  b += align256(sizeof(int4) * nitem);
+  b += align256(sizeof(int2) * nft);
+  b += align256(sizeof(int2) * ntile);
+  b += align256(sizeof(float) * (T + 1));
+  b += align256((size_t)kWChunkBytes * nchunk);
+  b += align256(sizeof(float) * (size_t)nitem * ntile * kM * kN);
+  b += align256(sizeof(int) * 4);
+  b += align256(sizeof(float2) * (size_t)(T + 1) * A * a.nch);
+  return b;
+}
+
+size_t mixed_smem_bytes(int nch) {
+  return (size_t)2 * (2 * kABytes + kWChunkBytes) + (size_t)kKC * 16 * nch * sizeof(float2) + kKC * sizeof(float) +
+         4 * sizeof(uint64_t) + 4 * sizeof(int);
+}
+
+__global__ void m_to_f32_kernel(const double2* __restrict__ M, float2* __restrict__ M32, size_t n,
+                                const double* __restrict__ w, float* __restrict__ w32, long long T) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double2 v = M[i];
+    M32[i] = make_float2((float)v.x, (float)v.y);
+    if (i < (size_t)T) w32[i] = (float)w[i];
+  }
+}
+
+cudaError_t launch_contract_mixed(const ContractArgs& a, long long T, void* ws, int& nlaunch, cudaStream_t st) {
   nlaunch = 0;
-  return cudaErrorNotSupported;
+  const int nft = (a.nf + kN - 1) / kN;
+  // transition range of every 256-wide frequency tile (the FP64 tiles are 64 wide)
+  std::vector<int2> tr(nft);
+  {
+    const int ft64 = contract_ftile();
+    const int n64 = (a.nf + ft64 - 1) / ft64;
+    std::vector<int2> t64(n64);
+    cudaError_t e = cudaMemcpyAsync(t64.data(), a.trange, sizeof(int2) * n64, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return e;
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+    for (int ft = 0; ft < nft; ++ft) {
+      int lo = INT32_MAX, hi = 0;
+      for (int q = ft * (kN / ft64); q < std::min(n64, (ft + 1) * (kN / ft64)); ++q) {
+        lo = std::min(lo, t64[q].x);
+        hi = std::max(hi, t64[q].y);
+      }
+      if (lo > hi) lo = hi;
+      tr[ft] = make_int2(lo, hi);
+    }
+  }
+  HostPlan h = make_plan(a, tr.data(), nft);
+  Plan pl{};
+  pl.nft = nft;
+  pl.ntile = (int)h.tiles.size();
+  pl.nchunk = (int)h.chunk_ft.size();
+  pl.nitem = (int)h.items.size();
+  const int A = 3 * a.neps;
+  uint8_t* p = reinterpret_cast<uint8_t*>(ws);
+  auto take = [&](size_t bytes) {
+    uint8_t* r = p;
+    p += align256(bytes);
+    return r;
+  };
+  pl.chunk_ft = reinterpret_cast<int*>(take(sizeof(int) * std::max(1, pl.nchunk)));
+  pl.chunk_t0 = reinterpret_cast<int*>(take(sizeof(int) * std::max(1, pl.nchunk)));
+  pl.chunk_t1 = reinterpret_cast<int*>(take(sizeof(int) * std::max(1, pl.nchunk)));
+  pl.item = reinterpret_cast<int4*>(take(sizeof(int4) * std::max(1, pl.nitem)));
+  pl.ft_items = reinterpret_cast<int2*>(take(sizeof(int2) * nft));
+  pl.tiles = reinterpret_cast<int2*>(take(sizeof(int2) * std::max(1, pl.ntile)));
+  pl.wgt32 = reinterpret_cast<float*>(take(sizeof(float) * (T + 1)));
+  pl.wbuf = take((size_t)kWChunkBytes * std::max(1, pl.nchunk));
+  pl.part = reinterpret_cast<float*>(take(sizeof(float) * (size_t)std::max(1, pl.nitem) * pl.ntile * kM * kN));
+  pl.err = reinterpret_cast<int*>(take(sizeof(int) * 4));
+  float2* M32 = reinterpret_cast<float2*>(take(sizeof(float2) * (size_t)(T + 1) * A * a.nch));
+  if ((size_t)(p - reinterpret_cast<uint8_t*>(ws)) > mixed_workspace_bytes(a, T)) return cudaErrorInvalidValue;
+  cudaError_t e;
+#define PMX_CP(dst, src, n)                                                                            \
+  if ((n) > 0) {                                                                                      \
+    e = cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, st);                                     \
+    if (e != cudaSuccess) return e;                                                                   \
+  }
+  PMX_CP(pl.chunk_ft, h.chunk_ft.data(), sizeof(int) * pl.nchunk);
+  PMX_CP(pl.chunk_t0, h.chunk_t0.data(), sizeof(int) * pl.nchunk);
+  PMX_CP(pl.chunk_t1, h.chunk_t1.data(), sizeof(int) * pl.nchunk);
+  PMX_CP(pl.item, h.items.data(), sizeof(int4) * pl.nitem);
+  PMX_CP(pl.ft_items, h.ft_items.data(), sizeof(int2) * nft);
+  PMX_CP(pl.tiles, h.tiles.data(), sizeof(int2) * pl.ntile);
+#undef PMX_CP
+  e = cudaMemsetAsync(pl.err, 0, sizeof(int) * 4, st);
+  if (e != cudaSuccess) return e;
+  // zero the accumulators: tiles with no transitions are written by reduce_kernel only where pieces exist
+  e = cudaMemsetAsync(a.acc, 0, sizeof(double) * 2 * 9 * (size_t)a.np * a.nf, st);
+  if (e != cudaSuccess) return e;
+  if (T > 0) {
+    m_to_f32_kernel<<<1184, 256, 0, st>>>(a.M, M32, (size_t)T * A * a.nch, a.wgt, pl.wgt32, T);
+    ++nlaunch;
+  }
+  if (pl.nchunk > 0) {
+    wgen_kernel<<<pl.nchunk, 256, 0, st>>>(pl, a);
+    ++nlaunch;
+  }
+  if (pl.nitem > 0 && pl.ntile > 0) {
+    const size_t sm = mixed_smem_bytes(a.nch);
+    dim3 grid(pl.ntile, pl.nitem);
+    if (a.nch == 1) {
+      e = cudaFuncSetAttribute(mixed_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      if (e != cudaSuccess) return e;
+      mixed_kernel<1><<<grid, kThreads, sm, st>>>(pl, a, M32);
+    } else {
+      e = cudaFuncSetAttribute(mixed_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      if (e != cudaSuccess) return e;
+      mixed_kernel<4><<<grid, kThreads, sm, st>>>(pl, a, M32);
+    }
+    ++nlaunch;
+    reduce_kernel<<<dim3(pl.ntile, nft), 256, 0, st>>>(pl, a);
+    ++nlaunch;
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  int err = 0;
+  e = cudaMemcpyAsync(&err, pl.err, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e != cudaSuccess) return e;
+  e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return e;
+  if (err != 0) return cudaErrorTimeout;
+  return cudaSuccess;
 }
 
 }  // namespace dev

@@ -1,0 +1,112 @@
+"""The benchmark workloads as picomax argv, with seeded synthetic form factors.
+
+Each workload is the restatement of one benchmark configuration as concrete
+options; form factors that the configuration only describes ("drawn from a
+seed within +-0.3 Ry") are drawn here from fixed numpy seeds, so every run and
+every implementation sees identical inputs. k-point files are Gamma-centred
+uniform grids written by picomax_b200.kgrid (same file for every
+implementation compared).
+"""
+from __future__ import annotations
+
+import math
+import os
+
+import numpy as np
+
+from .kgrid import make_kfile
+
+SI_VG = "3,4,8,11,-0.21,0,0.04,0.08,-0.21,0,0.04,0.08"
+
+
+def _fmt(xs):
+    return ",".join(f"{float(x):.6f}" for x in xs)
+
+
+def gaas_form_factors(seed: int = 1965):
+    """V_S, V_A ~ U(-0.3, 0.3) Ry on |G|^2 = 3, 4, 8, 11 (2 pi/a)^2; per-atom
+    V = V_S +- V_A; SOC: lambda_S ~ U(0.002, 0.01) Ry (uniform over |G|^2),
+    lambda_A ~ U(0, 0.005) Ry per shell."""
+    r = np.random.default_rng(seed)
+    vs = r.uniform(-0.3, 0.3, 4)
+    va = r.uniform(-0.3, 0.3, 4)
+    lam_s = r.uniform(0.002, 0.01)
+    lam_a = r.uniform(0.0, 0.005, 4)
+    vg = "3,4,8,11," + _fmt(vs + va) + "," + _fmt(vs - va)
+    soc = ["-use_uniform_us_so", "-uniform_us_so_val", f"{lam_s:.6f}",
+           "-ua_so", ",".join(f"{g}:{x:.6f}" for g, x in zip((3, 4, 8, 11), lam_a))]
+    return vg, soc
+
+
+def wz_form_factors(seed: int = 1967, f: float = 1.626):
+    """Per-atom V ~ U(-0.3, 0.3) Ry on the first five |G|^2 shells of the
+    wurtzite reciprocal lattice (cation pair = atoms 1, 2; anion pair = 3, 4)."""
+    s3 = math.sqrt(3.0)
+    b = np.array([[1, -1 / s3, 0], [1, 1 / s3, 0], [0, 0, 1.0 / f]])
+    r3 = np.arange(-3, 4)
+    hkl = np.array(np.meshgrid(r3, r3, r3, indexing="ij")).reshape(3, -1).T
+    g2 = np.unique(np.round(((hkl @ b) ** 2).sum(1), 6))
+    keys = g2[1:6]
+    r = np.random.default_rng(seed)
+    vc = r.uniform(-0.3, 0.3, 5)
+    van = r.uniform(-0.3, 0.3, 5)
+    vg = _fmt(keys) + "," + ",".join([_fmt(vc), _fmt(vc), _fmt(van), _fmt(van)])
+    return vg
+
+
+def te_form_factors(seed: int = 1968, f: float = 1.33):
+    """8 form factors on the first 8 |G|^2 shells of trigonal Te (same value
+    for the 3 atoms); SOC lambda_S uniform and lambda_A on the listed shells."""
+    s3 = math.sqrt(3.0)
+    b = np.array([[1, -1 / s3, 0], [1, 1 / s3, 0], [0, 0, 1.0 / f]])
+    r3 = np.arange(-3, 4)
+    hkl = np.array(np.meshgrid(r3, r3, r3, indexing="ij")).reshape(3, -1).T
+    g2 = np.unique(np.round(((hkl @ b) ** 2).sum(1), 6))
+    keys = g2[1:9]
+    r = np.random.default_rng(seed)
+    v = r.uniform(-0.3, 0.3, 8)
+    vg = _fmt(keys) + "," + ",".join([_fmt(v)] * 3)
+    soc = ["-use_uniform_us_so", "-uniform_us_so_val", f"{r.uniform(0.002, 0.01):.6f}",
+           "-ua_so", ",".join(f"{k:.6f}:{x:.6f}" for k, x in zip(keys[:4], r.uniform(0, 0.005, 4)))]
+    return vg, soc
+
+
+def workload(name: str, workdir: str):
+    """Returns (argv, nspectra, nsolves) of a named workload; k-files go to workdir."""
+    os.makedirs(workdir, exist_ok=True)
+    if name == "si_band":
+        argv = ["-switch", "band", "-crystal", "zb", "-a", "5.43", "-vg", SI_VG, "-encut", "110",
+                "-nband", "16", "-nvalence", "8", "-qpath", "G,X,W,L,G", "-qnum", "30,30,30,30"]
+        return argv, 0, 122
+    if name == "si_epsLL":
+        kf = os.path.join(workdir, "k_zb_8.txt")
+        nk = make_kfile(kf, "zb", 8, 8, 8)
+        argv = ["-switch", "epsLL", "-crystal", "zb", "-a", "5.43", "-vg", SI_VG, "-encut", "110",
+                "-kpoint", "0", "-kpointfile", kf, "-qvec", "0.01,0,0", "-neps", "15", "-nband", "16",
+                "-nvalence", "8", "-nfreq", "1000", "-dfreq", "0.02", "-delta", "0", "-epsilon", "0.1", "-kk", "1"]
+        return argv, 1, 1 + 2 * nk
+    if name.startswith("gaas_epsij"):
+        n = int(name.split("_")[-1]) if name.count("_") == 2 else 16
+        kf = os.path.join(workdir, f"k_zb_{n}.txt")
+        nk = make_kfile(kf, "zb", n, n, n)
+        vg, soc = gaas_form_factors()
+        argv = ["-switch", "epsij", "-crystal", "zb", "-a", "5.65", "-vg", vg, "-encut", "120",
+                "-kpoint", "0", "-kpointfile", kf, "-qvec", "0.01,0,0", "-neps", "27", "-nband", "16",
+                "-nvalence", "8", "-nfreq", "2000", "-dfreq", "0.0125", "-delta", "1", "-epsilon", "0.05",
+                "-kk", "1"] + soc
+        return argv, 1, 1 + 2 * nk
+    if name == "wz_epsLL":
+        kf = os.path.join(workdir, "k_wz_24_16.txt")
+        nk = make_kfile(kf, "wz", 24, 24, 16, f=1.626)
+        argv = ["-switch", "epsLL", "-crystal", "wz", "-a", "3.19", "-f", "1.626", "-u", "0.375",
+                "-vg", wz_form_factors(), "-encut", "200", "-kpoint", "0", "-kpointfile", kf,
+                "-qvec", "0.01,0,0", "-neps", "59", "-nband", "48", "-nvalence", "16", "-nfreq", "2000",
+                "-dfreq", "0.015", "-delta", "0", "-epsilon", "0.1", "-kk", "1"]
+        return argv, 1, 1 + 2 * nk
+    if name == "te_band":
+        vg, soc = te_form_factors()
+        argv = ["-switch", "band", "-crystal", "te", "-a", "4.45", "-f", "1.33", "-u", "0.264", "-vg", vg,
+                "-encut", "60", "-nband", "24", "-nvalence", "18", "-qpath", "G,A,H,K,G",
+                "-qnum", "30,30,30,30"] + soc
+        return argv, 0, 122
+    raise KeyError(name)

@@ -109,3 +109,18 @@ def test_cli_files_vs_reference(name, tmp_path):
     assert np.max(np.abs(dat - g["dat"])) <= tol
     if "gpt" in g:
         assert np.array_equal(np.fromfile(os.path.join(tmp_path, "out.gpt"), np.float64), g["gpt"])
+
+
+@pytest.mark.parametrize("name", CHI_CASES)
+def test_chi_mixed_vs_reference(ctx, name, tmp_path):
+    """Split-BF16 tensor-core contraction: within 1e-4 of the largest |value|."""
+    g = load_golden(name)
+    args = golden_args(g, tmp_path)
+    p = pm.Problem(args)
+    sw = pm.SWITCH_EPSLL if "epsLL" in args else pm.SWITCH_EPSIJ
+    re, im = ctx.chi(p, sw, pm.PREC_MIXED)
+    n = re.size
+    ref_re, ref_im = g["dat"][:n], g["dat"][n:]
+    scale = max(np.abs(ref_re).max(), np.abs(ref_im).max())
+    assert np.max(np.abs(re - ref_re)) <= 1e-4 * scale
+    assert np.max(np.abs(im - ref_im)) <= 1e-4 * scale
