@@ -43,7 +43,8 @@ constexpr int kN = 256;        // frequencies per tile
 constexpr int kKC = 32;        // transitions per chunk
 constexpr int kThreads = 256;
 constexpr int kPieceChunks = 64;  // chunks per K-split piece (2048 transitions)
-constexpr unsigned kWaitLimit = 1u << 24;
+constexpr unsigned kWaitLimit = 1u << 26;
+constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s
 
 // canonical K-major, no-swizzle layout: core matrices of 8 rows x 16 bytes;
 // rows of a core matrix 16 B apart, row groups SBO = 128 B apart, 8-element
@@ -73,9 +74,19 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
 }
 
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait on an mbarrier phase: gives up after kWaitNs nanoseconds (a
+// healthy wait takes microseconds) or kWaitLimit polls, whichever is first.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   const uint32_t a = smem_u32(bar);
+  const uint64_t t0 = global_ns();
   for (unsigned it = 0; it < kWaitLimit; ++it) {
+    if ((it & 1023u) == 1023u && global_ns() - t0 > kWaitNs) return false;
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
