@@ -96,6 +96,21 @@ const char* pmx_ctx_last_error(const pmx_ctx* ctx);
 int pmx_ctx_stage_times(const pmx_ctx* ctx, double* ms5);
 /* Launch count of this library's kernels since the context was created. */
 long long pmx_ctx_kernel_launches(const pmx_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or timing events after the library's. */
+void* pmx_ctx_stream(const pmx_ctx* ctx);
+/* Accumulated device time (CUDA events on the context stream around each
+ * launch) and launch count of one kernel family since the context was
+ * created: "assemble", "heev", "overlap", "contract_f64", "contract_mixed",
+ * "scale", "kk". */
+int pmx_ctx_kernel_time(const pmx_ctx* ctx, const char* family, double* ms, long long* launches);
+/* Bytes copied host->device and device->host by this context so far. */
+int pmx_ctx_transfer_bytes(const pmx_ctx* ctx, long long* h2d_bytes, long long* d2h_bytes);
+/* k and k+q points of the last pmx_chi* call at which the NBAND window cut a
+ * degenerate set (|E_NBAND-1 - E_NBAND| < 1e-8 eV). There the reference's
+ * result depends on its eigensolver's basis inside the set; a warning is
+ * printed on stderr. No reference counterpart (new diagnostic). */
+int pmx_ctx_degenerate_cuts(const pmx_ctx* ctx);
 
 /* ---------------------------------------------------------------- stage 1 */
 
@@ -125,6 +140,25 @@ int pmx_band(pmx_ctx* ctx, const pmx_problem* p, double* eband);
  * step when -kk 1. re/im each hold info.chi_values doubles in .dat order
  * [i][j][q][m][n<=m][f]. precision: PMX_PREC_FP64 or PMX_PREC_MIXED. */
 int pmx_chi(pmx_ctx* ctx, const pmx_problem* p, int sw, int precision, double* re, double* im);
+
+/* pmx_chi with the spectra left in device memory: re_dev/im_dev are device
+ * pointers with the same layout; epsm_dev (device, [nq][nfreq][2]) receives
+ * eps_M of every (q, w) when non-NULL (requires neps <= 64). */
+int pmx_chi_device(pmx_ctx* ctx, const pmx_problem* p, int sw, int precision, double* re_dev, double* im_dev,
+                   double* epsm_dev);
+
+/* pmx_chi plus eps_M(q, w) [nq][nfreq][2] of the (L, L) block, as
+ * pmx_eps_macroscopic computes it. */
+int pmx_chi_epsm(pmx_ctx* ctx, const pmx_problem* p, int sw, int precision, double* re, double* im, double* epsm);
+
+/* Macroscopic dielectric function eps_M(q, w) = 1 / [eps^-1]_00 with
+ * eps_mn = delta_mn + chi^LL_mn and eps_nm = conj(eps_mn) for n > m, from the
+ * (L, L) block of a chi .dat laid out [q][m][n<=m][f] (re and im arrays);
+ * epsm [nq][nfreq][2]. Restates the reference's post-processing
+ * include/matlab_wrapper/+picomax/+eps/macroscopic.m:13-29, :79 (MATLAB; the
+ * C++ reference has no counterpart). neps <= 64. */
+int pmx_eps_macroscopic(pmx_ctx* ctx, int neps, int nq, int nfreq, const double* chi_re, const double* chi_im,
+                        double* epsm);
 
 /* Kramers-Kronig transform of nrows spectra in place, re/im [nrows][nfreq],
  * w_f = dfreq f (kramerskronigtransform, src/pmx_chi.cpp:272-309). */

@@ -34,7 +34,9 @@ EXPORTS = (
     "pmx_problem_loci", "pmx_problem_kpoints", "pmx_problem_qpoints", "pmx_problem_dump",
     "pmx_problem_write_gpt", "pmx_ctx_create", "pmx_ctx_destroy", "pmx_ctx_last_error",
     "pmx_ctx_stage_times", "pmx_ctx_kernel_launches", "pmx_hamiltonian", "pmx_heev_batched",
-    "pmx_ref_energy", "pmx_band", "pmx_chi", "pmx_kk", "pmx_main",
+    "pmx_ref_energy", "pmx_band", "pmx_chi", "pmx_kk", "pmx_main", "pmx_ctx_stream",
+    "pmx_ctx_transfer_bytes", "pmx_ctx_degenerate_cuts", "pmx_chi_device", "pmx_chi_epsm",
+    "pmx_eps_macroscopic", "pmx_ctx_kernel_time",
 )
 
 
@@ -88,6 +90,13 @@ def load() -> ctypes.CDLL:
         "pmx_chi": (c_int, [c_void_p, c_void_p, c_int, c_int, dp, dp]),
         "pmx_kk": (c_int, [c_void_p, c_int, c_int, c_double, dp, dp]),
         "pmx_main": (c_int, [c_int, POINTER(c_char_p)]),
+        "pmx_ctx_stream": (c_void_p, [c_void_p]),
+        "pmx_ctx_transfer_bytes": (c_int, [c_void_p, POINTER(c_longlong), POINTER(c_longlong)]),
+        "pmx_ctx_degenerate_cuts": (c_int, [c_void_p]),
+        "pmx_chi_device": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p]),
+        "pmx_chi_epsm": (c_int, [c_void_p, c_void_p, c_int, c_int, dp, dp, dp]),
+        "pmx_eps_macroscopic": (c_int, [c_void_p, c_int, c_int, c_int, dp, dp, dp]),
+        "pmx_ctx_kernel_time": (c_int, [c_void_p, c_char_p, dp, POINTER(c_longlong)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -238,6 +247,48 @@ class Context:
         im = np.zeros(n, np.float64)
         self._check(self._lib.pmx_chi(self.handle, prob.handle, switch, precision, _dptr(re), _dptr(im)), "chi")
         return re, im
+
+    def stream(self) -> int:
+        return int(self._lib.pmx_ctx_stream(self.handle) or 0)
+
+    def transfer_bytes(self):
+        a, b = c_longlong(), c_longlong()
+        self._lib.pmx_ctx_transfer_bytes(self.handle, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def kernel_time(self, family: str):
+        """(device ms, launches) of one kernel family since the context was created."""
+        ms, n = c_double(), c_longlong()
+        self._lib.pmx_ctx_kernel_time(self.handle, family.encode(), ctypes.byref(ms), ctypes.byref(n))
+        return ms.value, n.value
+
+    def degenerate_cuts(self) -> int:
+        return int(self._lib.pmx_ctx_degenerate_cuts(self.handle))
+
+    def chi_epsm(self, prob: Problem, switch: int, precision: int = PREC_FP64):
+        n = prob.info.chi_values
+        re = np.zeros(n, np.float64)
+        im = np.zeros(n, np.float64)
+        eps = np.zeros((prob.info.nq, prob.info.nfreq, 2), np.float64)
+        self._check(self._lib.pmx_chi_epsm(self.handle, prob.handle, switch, precision, _dptr(re), _dptr(im),
+                                           _dptr(eps)), "chi_epsm")
+        return re, im, eps[..., 0] + 1j * eps[..., 1]
+
+    def chi_device(self, prob: Problem, switch: int, precision: int, re_ptr: int, im_ptr: int, epsm_ptr: int = 0):
+        """pmx_chi_device on caller-owned device buffers (raw pointers, e.g. torch .data_ptr())."""
+        st = self._lib.pmx_chi_device(self.handle, prob.handle, switch, precision, c_void_p(re_ptr),
+                                      c_void_p(im_ptr), c_void_p(epsm_ptr) if epsm_ptr else None)
+        self._check(st, "chi_device")
+
+    def eps_macroscopic(self, neps: int, chi_re, chi_im):
+        """eps_M [nq, nf] from the LL block [nq, npairs, nf] of a chi spectrum."""
+        chi_re = np.ascontiguousarray(chi_re, np.float64)
+        chi_im = np.ascontiguousarray(chi_im, np.float64)
+        nq, _, nf = chi_re.shape
+        out = np.zeros((nq, nf, 2), np.float64)
+        self._check(self._lib.pmx_eps_macroscopic(self.handle, neps, nq, nf, _dptr(chi_re), _dptr(chi_im),
+                                                  _dptr(out)), "eps_macroscopic")
+        return out[..., 0] + 1j * out[..., 1]
 
     def kk(self, re, im, dfreq: float):
         re = np.ascontiguousarray(re, np.float64).copy()

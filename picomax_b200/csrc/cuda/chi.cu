@@ -518,3 +518,100 @@ cudaError_t launch_kk(const double* chi, double* out, int rows, int nf, double d
 
 }  // namespace dev
 }  // namespace pmx
+
+namespace pmx {
+namespace dev {
+
+// ------------------------------------------------------------ macroscopic eps
+// eps_M(q, w) = 1 / [eps^-1]_00 with eps_mn = delta_mn + chi^LL_mn and the
+// n > m half filled by conj(eps_nm), as in the reference's post-processing
+// (include/matlab_wrapper/+picomax/+eps/macroscopic.m:13-29, :79). One warp
+// per (q, w): Gaussian elimination with partial pivoting of eps x = e_0 in
+// shared memory; [eps^-1]_00 = x_0.
+__global__ void __launch_bounds__(128) epsm_kernel(const double* __restrict__ re, const double* __restrict__ im,
+                                                   int neps, int nq, int nf, double2* __restrict__ out) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int job = blockIdx.x * (blockDim.x >> 5) + w;
+  if (job >= nq * nf) return;
+  const int q = job / nf, f = job % nf;
+  const int n = neps, ld = n + 1;
+  double2* E = reinterpret_cast<double2*>(smraw) + (size_t)w * n * ld;  // row-major, column n = rhs
+  const int np = n * (n + 1) / 2;
+  // chi LL block: [i=0][j=0][q][pair][f]
+  for (int idx = lane; idx < n * n; idx += 32) {
+    const int r = idx / n, c = idx % n;
+    const int m = r > c ? r : c, nn = r > c ? c : r;
+    const size_t o = ((size_t)q * np + (size_t)m * (m + 1) / 2 + nn) * nf + f;
+    double2 v = make_double2(re[o], im[o]);
+    if (r < c) v.y = -v.y;  // eps_nm = conj(eps_mn) above the diagonal
+    if (r == c) v.x += 1.0;
+    E[r * ld + c] = v;
+  }
+  for (int r = lane; r < n; r += 32) E[r * ld + n] = make_double2(r == 0 ? 1.0 : 0.0, 0.0);
+  __syncwarp();
+  for (int k = 0; k < n; ++k) {
+    // pivot search (lane-strided, then warp argmax)
+    double best = -1.0;
+    int bi = k;
+    for (int r = k + lane; r < n; r += 32) {
+      const double2 v = E[r * ld + k];
+      const double a = v.x * v.x + v.y * v.y;
+      if (a > best) {
+        best = a;
+        bi = r;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
+    if (bi != k)
+      for (int c = lane; c <= n; c += 32) {
+        const double2 t = E[k * ld + c];
+        E[k * ld + c] = E[bi * ld + c];
+        E[bi * ld + c] = t;
+      }
+    __syncwarp();
+    const double2 p = E[k * ld + k];
+    const double pd = p.x * p.x + p.y * p.y;
+    const double2 inv = make_double2(p.x / pd, -p.y / pd);
+    for (int r = k + 1; r < n; ++r) {
+      const double2 fct = cmul(E[r * ld + k], inv);
+      for (int c = k + lane; c <= n; c += 32) E[r * ld + c] = csub(E[r * ld + c], cmul(fct, E[k * ld + c]));
+    }
+    __syncwarp();
+  }
+  if (lane == 0) {
+    // back substitution for x_0 only needs the full solve; do it serially
+    double2 x[64];
+    for (int r = n - 1; r >= 0; --r) {
+      double2 s = E[r * ld + n];
+      for (int c = r + 1; c < n; ++c) s = csub(s, cmul(E[r * ld + c], x[c]));
+      const double2 d = E[r * ld + r];
+      const double dd = d.x * d.x + d.y * d.y;
+      x[r] = cmul(s, make_double2(d.x / dd, -d.y / dd));
+    }
+    const double2 x0 = x[0];
+    const double xx = x0.x * x0.x + x0.y * x0.y;
+    out[job] = make_double2(x0.x / xx, -x0.y / xx);
+  }
+}
+
+cudaError_t launch_epsm(const double* re, const double* im, int neps, int nq, int nf, double2* out, cudaStream_t st) {
+  if (neps > 64 || neps < 1) return cudaErrorInvalidValue;
+  const int warps = 4;
+  const size_t smem = (size_t)warps * neps * (neps + 1) * sizeof(double2);
+  cudaError_t e = cudaFuncSetAttribute(epsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int jobs = nq * nf;
+  epsm_kernel<<<(jobs + warps - 1) / warps, 32 * warps, smem, st>>>(re, im, neps, nq, nf, out);
+  return cudaGetLastError();
+}
+
+}  // namespace dev
+}  // namespace pmx

@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(kHeevThreads) heev_kernel(const EigItem* __res
                                                             double* __restrict__ scratch,
                                                             int* __restrict__ info) {
   const EigItem it = items[blockIdx.x];
-  const int n = it.n, nev = it.nev;
+  const int n = it.n, nev = it.nval, nvec = it.want_vec ? it.nev : 0;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int nthr = blockDim.x, nw = nthr >> 5;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -412,9 +412,9 @@ __global__ void __launch_bounds__(kHeevThreads) heev_kernel(const EigItem* __res
   if (tid == 0) {
     int nc = 0;
     const double gap = 1e-5 * tnorm;
-    for (int k = 0; k < nev; ++k)
+    for (int k = 0; k < nvec; ++k)
       if (k == 0 || lam[k] - lam[k - 1] > gap) clus[nc++] = k;
-    clus[nc] = nev;
+    clus[nc] = nvec;
     misc[0] = nc;
   }
   __syncthreads();
@@ -453,7 +453,7 @@ __global__ void __launch_bounds__(kHeevThreads) heev_kernel(const EigItem* __res
 
   // ----------------------------------------------------------- back-transform
   // x = H_0 H_1 ... H_{n-2} z ; one warp per eigenvector, no block barriers.
-  for (int k = wid; k < nev; k += nw) {
+  for (int k = wid; k < nvec; k += nw) {
     double2* z = zbuf + it.z_off + (size_t)k * n;
     for (int j = n - 2; j >= 0; --j) {
       const double2 tj = tau[j];

@@ -72,3 +72,11 @@ cudaError_t launch_kk(const double* chi, double* out, int rows, int nf, double d
 
 }  // namespace dev
 }  // namespace pmx
+
+namespace pmx {
+namespace dev {
+// eps_M per (q, w) from the chi LL block laid out [q][pair][f] (re, im);
+// out [nq][nf] complex. neps <= 64.
+cudaError_t launch_epsm(const double* re, const double* im, int neps, int nq, int nf, double2* out, cudaStream_t st);
+}  // namespace dev
+}  // namespace pmx

@@ -31,11 +31,12 @@ struct CrystalDev {
 struct EigItem {
   int crystal;        // index into the crystal table
   int n;              // matrix dimension (npw, or 2 npw with SOC)
-  int nev;            // lowest eigenpairs returned
+  int nev;            // lowest eigenvectors returned (when want_vec)
+  int nval;           // lowest eigenvalues returned, nval >= nev
   int want_vec;       // 1: also eigenvectors
   double k[3];        // wave vector, units 2 pi / a
   long long h_off;    // double2 offset of the n*n column-major workspace
-  long long w_off;    // double offset of nev eigenvalues
+  long long w_off;    // double offset of nval eigenvalues
   long long z_off;    // double2 offset of nev eigenvectors (column s at z_off + s*n)
   long long s_off;    // double offset of 4*n*nev inverse-iteration scratch
 };

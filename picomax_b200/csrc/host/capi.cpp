@@ -11,6 +11,7 @@
 #include <ctime>
 #include <fstream>
 #include <iostream>
+#include <map>
 #include <memory>
 #include <numeric>
 #include <sstream>
@@ -235,10 +236,16 @@ struct pmx_ctx {
   std::string err;
   double stage_ms[5] = {0, 0, 0, 0, 0};
   long long launches = 0;
+  long long h2d = 0, d2h = 0;  // bytes copied by the library since creation
+  int degenerate_cuts = 0;     // k-points of the last chi call whose NBAND window cut a degenerate set
+  // per kernel family: device time (CUDA events around the launches) and launches
+  std::map<std::string, std::pair<double, long long>> ktime;
+  std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> kpending;
+  std::vector<cudaEvent_t> evpool;
   // named workspaces
   DevBuf crystal, g, hkl, vloc, vso, items, hbuf, wbuf, zk, zq, scratch, info;
   DevBuf loci, kpts, uvec, ssoc, qgn, ncd, nvd, cbase, vbase, cidx, vidx, blkoff, dest;
-  DevBuf M, dE, wgt, f0, trange, acc, accpv, chi, chi2, mixws;
+  DevBuf M, dE, wgt, f0, trange, acc, accpv, chi, chi2, mixws, epsm;
   cudaEvent_t ev[2] = {nullptr, nullptr};
 };
 
@@ -257,13 +264,57 @@ struct Timer {
   }
 };
 
+// Brackets the launches of one kernel family with CUDA events on the context
+// stream; durations are collected when the stream is next synchronised.
+struct KTime {
+  pmx_ctx* c;
+  std::string name;
+  cudaEvent_t a, b;
+  KTime(pmx_ctx* ctx, const char* n) : c(ctx), name(n) {
+    a = take();
+    b = take();
+    cudaEventRecord(a, c->stream);
+  }
+  cudaEvent_t take() {
+    if (!c->evpool.empty()) {
+      cudaEvent_t e = c->evpool.back();
+      c->evpool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+  }
+  ~KTime() {
+    cudaEventRecord(b, c->stream);
+    c->kpending.push_back({name, {a, b}});
+  }
+};
+
+void collect_ktimes(pmx_ctx* c) {
+  for (auto& kp : c->kpending) {
+    float ms = 0;
+    if (cudaEventSynchronize(kp.second.second) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, kp.second.first, kp.second.second) == cudaSuccess) {
+      auto& t = c->ktime[kp.first];
+      t.first += ms;
+      t.second += 1;
+    }
+    c->evpool.push_back(kp.second.first);
+    c->evpool.push_back(kp.second.second);
+  }
+  c->kpending.clear();
+}
+
 template <class F>
 int guarded(pmx_ctx* ctx, F&& f) {
   if (!ctx) return PMX_ERR_INVALID;
   ctx->err.clear();
   try {
     CK(cudaSetDevice(ctx->device));
-    return f();
+    const int rc = f();
+    collect_ktimes(ctx);
+    return rc;
   } catch (const CudaFail& e) {
     ctx->err = e.what();
     return e.code;
@@ -276,6 +327,7 @@ int guarded(pmx_ctx* ctx, F&& f) {
 void h2d(pmx_ctx* c, DevBuf& b, const void* src, size_t bytes) {
   CK(b.ensure(std::max<size_t>(bytes, 16)));
   if (bytes) CK(cudaMemcpyAsync(b.ptr, src, bytes, cudaMemcpyHostToDevice, c->stream));
+  c->h2d += (long long)bytes;
 }
 
 // The crystal as the kernels see it, uploaded into the context.
@@ -320,50 +372,57 @@ DevCrystal upload_crystal(pmx_ctx* c, const pmx_problem* P, int force_spinor) {
   return d;
 }
 
-// Assembles and diagonalises H(k) for every k; eigenvalues to w (host,
-// [nk][nev]); eigenvectors to zdev ([nk][nev][n]) when non-null.
-void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int nev, double2* zdev,
+// Assembles and diagonalises H(k) for every k; the lowest nval eigenvalues
+// go to w (host, [nk][nval]); with zdev the lowest nvec eigenvectors go to
+// zdev ([nk][nvec][n]).
+void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int nval, int nvec, double2* zdev,
              std::vector<double>& w) {
   const int nk = (int)ks.size(), n = dc.n;
-  w.assign((size_t)nk * nev, 0.0);
+  w.assign((size_t)nk * nval, 0.0);
   if (nk == 0) return;
+  if (nval > 512 || nval > n) throw CudaFail("too many eigenvalues requested", PMX_ERR_INVALID);
+  const bool vec = zdev != nullptr && nvec > 0;
   const size_t hbytes = (size_t)n * n * sizeof(double2);
   int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)nk, ((size_t)2 << 30) / hbytes));
   chunk = std::min(chunk, 4096);
   CK(c->hbuf.ensure(hbytes * chunk));
-  CK(c->wbuf.ensure(sizeof(double) * (size_t)nk * nev));
-  CK(c->scratch.ensure(sizeof(double) * 4 * (size_t)n * nev * (zdev ? chunk : 1)));
+  CK(c->wbuf.ensure(sizeof(double) * (size_t)nk * nval));
+  CK(c->scratch.ensure(sizeof(double) * 4 * (size_t)n * std::max(nvec, 1) * (vec ? chunk : 1)));
   CK(c->info.ensure(sizeof(int) * chunk));
-  DevBuf ztmp;
-  double2* zbuf = zdev;
-  if (!zbuf) {
-    CK(ztmp.ensure(16));
-    zbuf = ztmp.as<double2>();
-  }
   std::vector<pmx::dev::EigItem> items(chunk);
   std::vector<int> info(chunk);
   for (int k0 = 0; k0 < nk; k0 += chunk) {
     const int cnt = std::min(chunk, nk - k0);
     for (int i = 0; i < cnt; ++i) {
       pmx::dev::EigItem& it = items[i];
+      it = pmx::dev::EigItem{};
       it.crystal = 0;
       it.n = n;
-      it.nev = nev;
-      it.want_vec = zdev ? 1 : 0;
+      it.nev = vec ? nvec : 0;
+      it.nval = nval;
+      it.want_vec = vec ? 1 : 0;
       for (int x = 0; x < 3; ++x) it.k[x] = ks[k0 + i][x];
       it.h_off = (long long)i * n * n;
-      it.w_off = (long long)(k0 + i) * nev;
-      it.z_off = (long long)(k0 + i) * nev * n;
-      it.s_off = (long long)i * 4 * n * nev;
+      it.w_off = (long long)(k0 + i) * nval;
+      it.z_off = (long long)(k0 + i) * nvec * n;
+      it.s_off = (long long)i * 4 * n * std::max(nvec, 1);
     }
     h2d(c, c->items, items.data(), sizeof(pmx::dev::EigItem) * cnt);
-    CK(pmx::dev::launch_assemble(dc.dev, c->items.as<pmx::dev::EigItem>(), cnt, dc.npw, c->hbuf.as<double2>(),
-                                 c->stream));
-    CK(pmx::dev::launch_heev(c->items.as<pmx::dev::EigItem>(), cnt, n, nev, c->hbuf.as<double2>(),
-                             c->wbuf.as<double>(), zbuf, c->scratch.as<double>(), c->info.as<int>(), c->stream));
+    {
+      KTime kt(c, "assemble");
+      CK(pmx::dev::launch_assemble(dc.dev, c->items.as<pmx::dev::EigItem>(), cnt, dc.npw, c->hbuf.as<double2>(),
+                                   c->stream));
+    }
+    {
+      KTime kt(c, "heev");
+      CK(pmx::dev::launch_heev(c->items.as<pmx::dev::EigItem>(), cnt, n, nval, c->hbuf.as<double2>(),
+                               c->wbuf.as<double>(), vec ? zdev : c->hbuf.as<double2>(), c->scratch.as<double>(),
+                               c->info.as<int>(), c->stream));
+    }
     c->launches += 2;
     CK(cudaMemcpyAsync(info.data(), c->info.ptr, sizeof(int) * cnt, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    c->d2h += sizeof(int) * cnt;
     for (int i = 0; i < cnt; ++i)
       if (info[i] != 0)
         throw CudaFail("eigensolver failed (status " + std::to_string(info[i]) + ") at k-point " +
@@ -372,6 +431,7 @@ void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int 
   }
   CK(cudaMemcpyAsync(w.data(), c->wbuf.ptr, sizeof(double) * w.size(), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  c->d2h += sizeof(double) * w.size();
 }
 
 // Spinor eigenvalue s of a solved item (spatial spectrum doubled without SOC).
@@ -392,7 +452,7 @@ double ref_energy(pmx_ctx* c, const pmx_problem* P, const DevCrystal& dc) {
   }
   const int nev = solved_states(p.nvalence + 1, dc.soc);
   std::vector<double> w;
-  solve_k(c, dc, {p.refpoint}, nev, nullptr, w);
+  solve_k(c, dc, {p.refpoint}, nev, 0, nullptr, w);
   return (spinor_eig(w, nev, 0, p.nvalence - 1, dc.soc) + spinor_eig(w, nev, 0, p.nvalence, dc.soc)) / 2.0;
 }
 
@@ -422,6 +482,11 @@ extern "C" void pmx_ctx_destroy(pmx_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
+  for (auto& kp : c->kpending) {
+    cudaEventDestroy(kp.second.first);
+    cudaEventDestroy(kp.second.second);
+  }
+  for (auto& e : c->evpool) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -527,7 +592,7 @@ extern "C" int pmx_band(pmx_ctx* ctx, const pmx_problem* P, double* eband) {
     }
     const int nev = solved_states(nkeep, dc.soc);
     std::vector<double> w;
-    solve_k(ctx, dc, p.lat.Q, nev, nullptr, w);
+    solve_k(ctx, dc, p.lat.Q, nev, 0, nullptr, w);
     for (int q = 0; q < p.nq(); ++q)
       for (int n = 0; n < p.nband; ++n)
         eband[(size_t)q * p.nband + n] = n < nh ? spinor_eig(w, nev, q, n, dc.soc) - off : 0.0;
@@ -549,8 +614,10 @@ struct Transitions {
 // Occupations and transition list of one q (src/pmx_chi.cpp:391-397, :477-483):
 // conduction states are counted down from the top of the NBAND window while
 // E - E_ref > 0, valence states up from the bottom while E - E_ref <= 0.
-Transitions build_transitions(const Problem& p, int soc, int nev, const std::vector<double>& wk,
-                              const std::vector<double>& wq, double off, bool sort_by_window) {
+// wk/wq hold nval eigenvalues per k (spatial states without SOC). `cuts`
+// counts k and k+q points where state NBAND-1 and NBAND are degenerate.
+Transitions build_transitions(const Problem& p, int soc, int nval, const std::vector<double>& wk,
+                              const std::vector<double>& wq, double off, bool sort_by_window, int& cuts) {
   Transitions T;
   const int nk = p.nk(), NB = p.nband;
   T.ncd.resize(nk);
@@ -566,10 +633,16 @@ Transitions build_transitions(const Problem& p, int soc, int nev, const std::vec
   std::vector<Raw> raw;
   long long blk = 0;
   const double df = p.dfreq, w0 = p.freq.empty() ? 0.0 : p.freq[0];
+  const int nh = 2 * p.npw();
   for (int k = 0; k < nk; ++k) {
+    if (NB < nh) {
+      const bool cut_k = std::abs(spinor_eig(wk, nval, k, NB, soc) - spinor_eig(wk, nval, k, NB - 1, soc)) < 1e-8;
+      const bool cut_q = std::abs(spinor_eig(wq, nval, k, NB, soc) - spinor_eig(wq, nval, k, NB - 1, soc)) < 1e-8;
+      cuts += (int)cut_k + (int)cut_q;
+    }
     int nc = 0, nv = 0;
-    while (nc < NB && spinor_eig(wk, nev, k, NB - 1 - nc, soc) - off > 0) ++nc;
-    while (nv < NB && spinor_eig(wq, nev, k, nv, soc) - off <= 0) ++nv;
+    while (nc < NB && spinor_eig(wk, nval, k, NB - 1 - nc, soc) - off > 0) ++nc;
+    while (nv < NB && spinor_eig(wq, nval, k, nv, soc) - off <= 0) ++nv;
     // distinct solved states
     std::vector<int> cs, vs;
     for (int c = 0; c < nc; ++c) {
@@ -603,8 +676,8 @@ Transitions build_transitions(const Problem& p, int soc, int nev, const std::vec
         if (mult == 0) continue;
         const int s_c = soc ? cs[ic] : 2 * cs[ic];
         const int s_v = soc ? vs[iv] : 2 * vs[iv];
-        const double ec = spinor_eig(wk, nev, k, s_c, soc) - off;
-        const double ev = spinor_eig(wq, nev, k, s_v, soc) - off;
+        const double ec = spinor_eig(wk, nval, k, s_c, soc) - off;
+        const double ev = spinor_eig(wq, nval, k, s_v, soc) - off;
         const double de = ec - ev;
         raw.push_back({src, de, p.KW[k] * mult, (int)((de - w0) / df)});
       }
@@ -635,7 +708,8 @@ int window_half(const Problem& p) {
 
 }  // namespace
 
-extern "C" int pmx_chi(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision, double* re, double* im) {
+static int run_chi(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision, double* re, double* im,
+                   bool device_out, double* epsm) {
   if (!P || (sw != PMX_SWITCH_EPSIJ && sw != PMX_SWITCH_EPSLL)) return PMX_ERR_INVALID;
   if (precision != PMX_PREC_FP64 && precision != PMX_PREC_MIXED) return PMX_ERR_INVALID;
   return guarded(ctx, [&]() -> int {
@@ -660,13 +734,15 @@ extern "C" int pmx_chi(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision
       off = ref_energy(ctx, P, dc);
     }
     const int nev = solved_states(p.nband, dc.soc);
+    const int nval = std::min(solved_states(p.nband + 1, dc.soc), dc.n);
     const int n = dc.n;
+    ctx->degenerate_cuts = 0;
     const int nch = (mode == 0 && dc.soc) ? 4 : 1;
     CK(ctx->zk.ensure(std::max<size_t>(sizeof(double2) * (size_t)nk * nev * n, 16)));
     CK(ctx->zq.ensure(std::max<size_t>(sizeof(double2) * (size_t)nk * nev * n, 16)));
     {
       Timer tm(ctx, 0);
-      solve_k(ctx, dc, p.K, nev, ctx->zk.as<double2>(), wk);
+      solve_k(ctx, dc, p.K, nval, nev, ctx->zk.as<double2>(), wk);
     }
     // static tables of the chi stage
     h2d(ctx, ctx->loci, p.loci.data(), sizeof(int) * p.loci.size());
@@ -704,9 +780,9 @@ extern "C" int pmx_chi(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision
       std::vector<double> wq;
       {
         Timer tm(ctx, 0);
-        solve_k(ctx, dc, kq, nev, ctx->zq.as<double2>(), wq);
+        solve_k(ctx, dc, kq, nval, nev, ctx->zq.as<double2>(), wq);
       }
-      Transitions T = build_transitions(p, dc.soc, nev, wk, wq, off, mode == 0);
+      Transitions T = build_transitions(p, dc.soc, nval, wk, wq, off, mode == 0, ctx->degenerate_cuts);
       // per-m polarisation and SOC-current tables
       std::vector<double2> uv((size_t)neps * 9), ss((size_t)neps * 3);
       std::vector<double> qg(neps);
@@ -792,6 +868,7 @@ extern "C" int pmx_chi(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision
         oa.uvec = ctx->uvec.as<double2>();
         oa.ssoc = ctx->ssoc.as<double2>();
         oa.M = ctx->M.as<double2>();
+        KTime kt(ctx, "overlap");
         CK(pmx::dev::launch_overlap(oa, nk, st));
         ctx->launches += 1;
       }
@@ -815,11 +892,13 @@ extern "C" int pmx_chi(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision
         ca.acc = ctx->acc.as<double>();
         ca.acc_pv = pv ? ctx->accpv.as<double>() : nullptr;
         if (precision == PMX_PREC_FP64 || pv) {
+          KTime kt(ctx, "contract_f64");
           CK(pmx::dev::launch_contract_f64(ca, st));
           ctx->launches += 1;
         } else {
           int nl = 0;
           CK(ctx->mixws.ensure(std::max<size_t>(pmx::dev::mixed_workspace_bytes(ca, (long long)T.T), 16)));
+          KTime kt(ctx, "contract_mixed");
           CK(pmx::dev::launch_contract_mixed(ca, (long long)T.T, ctx->mixws.ptr, nl, st));
           ctx->launches += nl;
         }
@@ -831,9 +910,13 @@ extern "C" int pmx_chi(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision
         sa.acc = ctx->acc.as<double>();
         sa.acc_pv = pv ? ctx->accpv.as<double>() : nullptr;
         sa.out = ctx->chi.as<double>();
-        CK(pmx::dev::launch_scale(sa, st));
+        {
+          KTime kt(ctx, "scale");
+          CK(pmx::dev::launch_scale(sa, st));
+        }
         ctx->launches += 1;
         if (p.kk) {
+          KTime kt(ctx, "kk");
           CK(pmx::dev::launch_kk(ctx->chi.as<double>(), ctx->chi2.as<double>(), 9 * np, nf, p.dfreq, st));
           ctx->launches += 1;
         }
@@ -843,12 +926,84 @@ extern "C" int pmx_chi(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision
         Timer tm(ctx, 4);
         const double* res = p.kk ? ctx->chi2.as<double>() : ctx->chi.as<double>();
         const size_t row = (size_t)np * nf * sizeof(double);
-        CK(cudaMemcpy2DAsync(re + (size_t)q * np * nf, row * nq, res, row, row, 9, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpy2DAsync(im + (size_t)q * np * nf, row * nq, res + blkvals, row, row, 9,
-                             cudaMemcpyDeviceToHost, st));
+        const cudaMemcpyKind kind = device_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+        CK(cudaMemcpy2DAsync(re + (size_t)q * np * nf, row * nq, res, row, row, 9, kind, st));
+        CK(cudaMemcpy2DAsync(im + (size_t)q * np * nf, row * nq, res + blkvals, row, row, 9, kind, st));
+        if (!device_out) ctx->d2h += (long long)(2 * 9 * row);
+        if (epsm) {
+          // eps_M of this q from the (L, L) block: [i=0][j=0] rows of res
+          CK(ctx->epsm.ensure(sizeof(double2) * nf));
+          CK(pmx::dev::launch_epsm(res, res + blkvals, neps, 1, nf, ctx->epsm.as<double2>(), st));
+          ctx->launches += 1;
+          CK(cudaMemcpyAsync(epsm + (size_t)2 * q * nf, ctx->epsm.ptr, sizeof(double2) * nf,
+                             device_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+          if (!device_out) ctx->d2h += (long long)(sizeof(double2) * nf);
+        }
       }
     }
     CK(cudaStreamSynchronize(st));
+    if (ctx->degenerate_cuts > 0)
+      std::cerr << "WARNING: -nband " << p.nband << " cuts a degenerate set at " << ctx->degenerate_cuts
+                << " k / k+q points (|E_NBAND - E_NBAND+1| < 1e-8 eV); chi then depends on the eigenvector "
+                   "basis inside that set, for the reference's eigensolver as for this one"
+                << std::endl;
+    return (int)PMX_OK;
+  });
+}
+
+extern "C" int pmx_chi(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision, double* re, double* im) {
+  return run_chi(ctx, P, sw, precision, re, im, false, nullptr);
+}
+
+extern "C" int pmx_chi_device(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision, double* re_dev,
+                              double* im_dev, double* epsm_dev) {
+  return run_chi(ctx, P, sw, precision, re_dev, im_dev, true, epsm_dev);
+}
+
+extern "C" int pmx_chi_epsm(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision, double* re, double* im,
+                            double* epsm) {
+  if (P && P->p.neps > 64) return PMX_ERR_UNSUPPORTED;
+  return run_chi(ctx, P, sw, precision, re, im, false, epsm);
+}
+
+extern "C" void* pmx_ctx_stream(const pmx_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+extern "C" int pmx_ctx_kernel_time(const pmx_ctx* c, const char* family, double* ms, long long* launches) {
+  if (!c || !family) return PMX_ERR_INVALID;
+  auto it = c->ktime.find(family);
+  if (ms) *ms = it == c->ktime.end() ? 0.0 : it->second.first;
+  if (launches) *launches = it == c->ktime.end() ? 0 : it->second.second;
+  return PMX_OK;
+}
+
+extern "C" int pmx_ctx_transfer_bytes(const pmx_ctx* c, long long* h2d_bytes, long long* d2h_bytes) {
+  if (!c) return PMX_ERR_INVALID;
+  if (h2d_bytes) *h2d_bytes = c->h2d;
+  if (d2h_bytes) *d2h_bytes = c->d2h;
+  return PMX_OK;
+}
+
+extern "C" int pmx_ctx_degenerate_cuts(const pmx_ctx* c) { return c ? c->degenerate_cuts : -1; }
+
+extern "C" int pmx_eps_macroscopic(pmx_ctx* ctx, int neps, int nq, int nfreq, const double* chi_re,
+                                   const double* chi_im, double* epsm) {
+  if (neps < 1 || neps > 64 || nq < 0 || nfreq <= 0 || (nq > 0 && (!chi_re || !chi_im || !epsm)))
+    return PMX_ERR_INVALID;
+  return guarded(ctx, [&]() {
+    const size_t vals = (size_t)nq * neps * (neps + 1) / 2 * nfreq;
+    if (vals == 0) return (int)PMX_OK;
+    CK(ctx->chi.ensure(sizeof(double) * 2 * vals));
+    CK(ctx->epsm.ensure(sizeof(double2) * nq * nfreq));
+    CK(cudaMemcpyAsync(ctx->chi.ptr, chi_re, sizeof(double) * vals, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->chi.as<double>() + vals, chi_im, sizeof(double) * vals, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    ctx->h2d += (long long)(2 * sizeof(double) * vals);
+    CK(pmx::dev::launch_epsm(ctx->chi.as<double>(), ctx->chi.as<double>() + vals, neps, nq, nfreq,
+                             ctx->epsm.as<double2>(), ctx->stream));
+    ctx->launches += 1;
+    CK(cudaMemcpyAsync(epsm, ctx->epsm.ptr, sizeof(double2) * nq * nfreq, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->d2h += (long long)(sizeof(double2) * nq * nfreq);
     return (int)PMX_OK;
   });
 }

@@ -124,3 +124,37 @@ def test_chi_mixed_vs_reference(ctx, name, tmp_path):
     scale = max(np.abs(ref_re).max(), np.abs(ref_im).max())
     assert np.max(np.abs(re - ref_re)) <= 1e-4 * scale
     assert np.max(np.abs(im - ref_im)) <= 1e-4 * scale
+
+
+def test_eps_macroscopic_vs_oracle(ctx, tmp_path):
+    """eps_M = 1/[eps^-1]_00 of the LL block (restated macroscopic.m) on the
+    reference's own chi_LL spectrum."""
+    g = load_golden("si_epsLL")
+    args = golden_args(g, tmp_path)
+    p = pm.Problem(args)
+    neps, nf = p.info.neps, p.info.nfreq
+    npairs = neps * (neps + 1) // 2
+    n = g["dat"].size // 2
+    re = g["dat"][:n].reshape(3, 3, 1, npairs, nf)[0, 0]
+    im = g["dat"][n:].reshape(3, 3, 1, npairs, nf)[0, 0]
+    eps = ctx.eps_macroscopic(neps, re, im)
+    ref = O.eps_macroscopic(re[0], im[0], neps)
+    assert np.max(np.abs(eps[0] - ref)) <= 1e-10 * np.max(np.abs(ref))
+    # the fused path (chi + eps_M in one call) agrees with the two-step one
+    cre, cim, eps2 = ctx.chi_epsm(p, pm.SWITCH_EPSLL, pm.PREC_FP64)
+    e3 = ctx.eps_macroscopic(neps, cre.reshape(3, 3, 1, npairs, nf)[0, 0], cim.reshape(3, 3, 1, npairs, nf)[0, 0])
+    assert np.max(np.abs(eps2 - e3)) <= 1e-12 * np.max(np.abs(e3))
+    assert np.max(np.abs(eps2[0] - ref)) <= 1e-7 * np.max(np.abs(ref))
+
+
+def test_degenerate_cut_reported(ctx, tmp_path):
+    """NBAND cutting the Lambda_3 pair of Si (k on Gamma-L) is detected."""
+    from picomax_b200.kgrid import write_kfile
+    kf = os.path.join(str(tmp_path), "k.txt")
+    write_kfile(kf, np.array([[0.25, 0.25, 0.25], [0.1, 0.2, 0.3]]), np.ones(2))
+    args = ("-switch epsLL -crystal zb -a 5.43 -vg 3,4,8,11,-0.21,0,0.04,0.08,-0.21,0,0.04,0.08 -encut 60 "
+            "-nband 16 -nvalence 8 -neps 2 -nfreq 20 -dfreq 0.5 -qvec 0.01,0,0 -kpoint 0").split() + [
+        "-kpointfile", kf]
+    p = pm.Problem(args)
+    ctx.chi(p, pm.SWITCH_EPSLL)
+    assert ctx.degenerate_cuts() >= 1
