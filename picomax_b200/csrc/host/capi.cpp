@@ -540,7 +540,8 @@ extern "C" int pmx_heev_batched(pmx_ctx* ctx, int n, int batch, const double* A,
     for (int i = 0; i < batch; ++i) {
       items[i] = pmx::dev::EigItem{};
       items[i].n = n;
-      items[i].nev = nev;
+      items[i].nev = z ? nev : 0;
+      items[i].nval = nev;
       items[i].want_vec = z ? 1 : 0;
       items[i].h_off = (long long)i * n * n;
       items[i].w_off = (long long)i * nev;
