@@ -110,3 +110,27 @@ def workload(name: str, workdir: str):
                 "-qnum", "30,30,30,30"] + soc
         return argv, 0, 122
     raise KeyError(name)
+
+
+def main(argv=None):
+    """python -m picomax_b200.workloads NAME [extra picomax options]
+
+    Runs the picomax CLI on a named workload (k-point files are written to a
+    temporary directory, outputs too) and prints the CLI's progress output."""
+    import subprocess
+    import sys
+    import tempfile
+
+    from ._capi import CLI_PATH
+    argv = sys.argv[1:] if argv is None else argv
+    if not argv:
+        print(main.__doc__)
+        return 2
+    with tempfile.TemporaryDirectory() as tmp:
+        args, _, _ = workload(argv[0], tmp)
+        r = subprocess.run([CLI_PATH] + args + argv[1:] + ["-wdir", tmp, "-outputfile", argv[0]])
+        return r.returncode
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
