@@ -107,9 +107,9 @@ cudaError_t launch_assemble(const CrystalDev* crystals, const EigItem* items, in
 // --------------------------------------------------------------- eigensolver
 namespace {
 
-constexpr int kHeevThreads = 512;
-constexpr int kMaxWarps = kHeevThreads / 32;
-constexpr int kBisectIters = 200;   // cap; multisection converges in ~20
+constexpr int kHeevThreads = 256;
+constexpr int kWarps = kHeevThreads / 32;
+constexpr int kBisectIters = 200;   // cap; multisection converges in ~15
 constexpr int kInvIters = 3;
 
 __device__ __forceinline__ int sturm_count(const double* d, const double* e2, int n, double x,
@@ -139,7 +139,6 @@ __device__ __forceinline__ double hash_uniform(unsigned long long a, unsigned lo
 // pivoting (the LU has two super-diagonals). u0/u1/u2 are scratch of length n.
 __device__ void tri_solve(const double* d, const double* e, int n, double lam, double tiny,
                           double* x, double* u0, double* u1, double* u2) {
-  // Forward elimination applied to the right-hand side as the LU is formed.
   double a = d[0] - lam;                  // current pivot-row diagonal
   double c = n > 1 ? e[0] : 0.0;          // current pivot-row first super-diagonal
   double c2 = 0.0;                         // current pivot-row second super-diagonal
@@ -158,8 +157,7 @@ __device__ void tri_solve(const double* d, const double* e, int n, double lam, d
       c = en - f * c2;
       c2 = 0.0;
     } else {
-      // swap rows i and i+1
-      const double f = a / b;
+      const double f = a / b;  // swap rows i and i+1
       u0[i] = b;
       u1[i] = dn;
       u2[i] = en;
@@ -173,58 +171,211 @@ __device__ void tri_solve(const double* d, const double* e, int n, double lam, d
   }
   if (a == 0.0 || fabs(a) < tiny) a = a < 0 ? -tiny : tiny;
   u0[n - 1] = a;
-  // back substitution
   x[n - 1] = x[n - 1] / u0[n - 1];
   if (n > 1) x[n - 2] = (x[n - 2] - u1[n - 2] * x[n - 1]) / u0[n - 2];
   for (int i = n - 3; i >= 0; --i) x[i] = (x[i] - u1[i] * x[i + 1] - u2[i] * x[i + 2]) / u0[i];
 }
 
+// Lower triangle of an n x n matrix; col(c)[r - c] = A(r, c) for r >= c.
+struct LowerFull {  // column-major n x n in global memory (upper half unused)
+  double2* A;
+  int n;
+  __device__ __forceinline__ double2* col(int c) const { return A + (size_t)c * n + c; }
+};
+struct LowerPacked {  // packed columns in shared memory
+  double2* A;
+  int n;
+  __device__ __forceinline__ double2* col(int c) const {
+    return A + ((size_t)c * n - (size_t)c * (c - 1) / 2);
+  }
+};
+
 }  // namespace
 
-// Shared-memory layout (double2 units unless noted):
-//   [A: n*n if resident] vprev[n] wprev[n] vcur[n] y[n] tau[n] red2[kMaxWarps]
-//   doubles: d[n] e[n] e2[n] red[kMaxWarps] lam[nev] lo[nev] hi[nev] xs[kHeevThreads]
+// Shared-memory layout (double2 unless noted):
+//   [packed lower A: n(n+1)/2 if resident] vprev[n] wprev[n] vcur[n] dotp[n] tau[n] part[kWarps*n]
+//   doubles: d[n] e[n] e2[n] red[2*kWarps] lam[nev] lo[nev] hi[nev] xs[kHeevThreads]
 //   ints: cnt[kHeevThreads] clus[nev+1] misc[4]
 __host__ __device__ inline size_t heev_smem_bytes(int n, int nev, bool resident) {
   size_t b = 0;
-  if (resident) b += (size_t)n * n * sizeof(double2);
-  b += (size_t)5 * n * sizeof(double2) + kMaxWarps * sizeof(double2);
-  b += (size_t)(3 * n + kMaxWarps + 3 * nev + kHeevThreads) * sizeof(double);
+  if (resident) b += (size_t)n * (n + 1) / 2 * sizeof(double2);
+  b += (size_t)(5 + kWarps) * n * sizeof(double2);
+  b += (size_t)(3 * n + 2 * kWarps + 3 * nev + kHeevThreads) * sizeof(double);
   b += (size_t)(kHeevThreads + nev + 1 + 4) * sizeof(int);
   return b;
 }
 
-template <bool RESIDENT>
-__global__ void __launch_bounds__(kHeevThreads) heev_kernel(const EigItem* __restrict__ items,
-                                                            double2* __restrict__ hbuf,
-                                                            double* __restrict__ wbuf,
-                                                            double2* __restrict__ zbuf,
-                                                            double* __restrict__ scratch,
-                                                            int* __restrict__ info) {
+// Householder tridiagonalisation (zhetd2 convention, lower triangle only).
+// Step j: warp 0 finishes column j (pending rank-2 update of step j-1, then
+// the reflector); all warps then make one pass over the trailing lower
+// triangle that applies the pending update and accumulates y = A v (rows in
+// per-lane registers, column dots by warp reduction) and v^H A v; finally
+// w = tau y - tau^2/2 (v^H A v) v becomes the pending update. Three barriers
+// per step. MAXS = ceil(n / 32) register slots per lane.
+template <int MAXS, class Acc>
+__device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, double2* wprev, double2* vcur,
+                                              double2* dotp, double2* tau, double2* part, double* d, double* e,
+                                              double* red) {
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  bool pending = false;
+  for (int j = 0; j < n - 1; ++j) {
+    // ---- A: column j (warp 0)
+    if (wid == 0) {
+      double2* cj = acc.col(j);
+      double xn = 0.0;
+      for (int r = j + lane; r < n; r += 32) {
+        double2 a = cj[r - j];
+        if (pending) {
+          a = csub(a, cadd(cmul(vprev[r], cconj(wprev[j])), cmul(wprev[r], cconj(vprev[j]))));
+          cj[r - j] = a;
+        }
+        if (r >= j + 2) xn += a.x * a.x + a.y * a.y;
+      }
+      xn = warp_sum(xn);
+      __syncwarp();
+      const double2 ajj = cj[0];
+      const double2 alpha = cj[1];
+      double beta;
+      double2 tj, scal;
+      if (xn == 0.0 && alpha.y == 0.0) {
+        tj = make_double2(0, 0);
+        beta = alpha.x;
+        scal = make_double2(1, 0);
+      } else {
+        beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn), alpha.x);
+        tj = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
+        const double2 den = make_double2(alpha.x - beta, alpha.y);
+        const double dd = den.x * den.x + den.y * den.y;
+        scal = make_double2(den.x / dd, -den.y / dd);
+      }
+      __syncwarp();
+      for (int r = j + 2 + lane; r < n; r += 32) {
+        const double2 a = cmul(cj[r - j], scal);
+        cj[r - j] = a;
+        vcur[r] = a;
+      }
+      if (lane == 0) {
+        d[j] = ajj.x;
+        e[j] = beta;
+        tau[j] = tj;
+        vcur[j + 1] = make_double2(1, 0);
+        cj[1] = make_double2(1, 0);
+      }
+    }
+    __syncthreads();
+    const double2 tj = tau[j];
+    const bool active = tj.x != 0.0 || tj.y != 0.0;
+    // ---- B: fused pass over the trailing lower triangle
+    double2 yreg[MAXS];
+#pragma unroll
+    for (int s = 0; s < MAXS; ++s) yreg[s] = make_double2(0, 0);
+    double vhav = 0.0;
+    if (active || pending) {
+      for (int c = j + 1 + wid; c < n; c += kWarps) {
+        double2* cc = acc.col(c);
+        const double2 vc = vcur[c];
+        const double vc2 = vc.x * vc.x + vc.y * vc.y;
+        const double2 wcc = cconj(wprev[c]), vcc = cconj(vprev[c]);
+        double2 a[MAXS];
+#pragma unroll
+        for (int s = 0; s < MAXS; ++s) {
+          const int r = 32 * s + lane;
+          a[s] = (r >= c && r < n) ? cc[r - c] : make_double2(0, 0);
+        }
+        double2 dot = make_double2(0, 0);
+#pragma unroll
+        for (int s = 0; s < MAXS; ++s) {
+          const int r = 32 * s + lane;
+          if (r >= c && r < n) {
+            double2 v = a[s];
+            if (pending) {
+              v = csub(v, cadd(cmul(vprev[r], wcc), cmul(wprev[r], vcc)));
+              cc[r - c] = v;
+            }
+            if (active) {
+              yreg[s] = cadd(yreg[s], cmul(v, vc));
+              if (r > c) {
+                const double2 vr = vcur[r];
+                dot = cadd(dot, cmulc(v, vr));
+                const double2 t = cmul(cmulc(vr, v), vc);  // conj(v_r) A_rc v_c
+                vhav += 2.0 * t.x;
+              } else {
+                vhav += v.x * vc2;
+              }
+            }
+          }
+        }
+        if (active) {
+          dot = warp_sum2(dot);
+          if (lane == 0) dotp[c] = dot;
+        }
+      }
+    }
+    if (active) {
+#pragma unroll
+      for (int s = 0; s < MAXS; ++s) {
+        const int r = 32 * s + lane;
+        if (r >= j + 1 && r < n) part[wid * n + r] = yreg[s];
+      }
+      vhav = warp_sum(vhav);
+      if (lane == 0) red[wid] = vhav;
+    }
+    __syncthreads();
+    // ---- C: w = tau (A v) - |tau|^2/2 (v^H A v) v becomes the pending update
+    if (active) {
+      double vAv = 0.0;
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) vAv += red[w];
+      const double al = -0.5 * (tj.x * tj.x + tj.y * tj.y) * vAv;
+      for (int r = j + 1 + tid; r < n; r += kHeevThreads) {
+        double2 sum = dotp[r];
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) sum = cadd(sum, part[w * n + r]);
+        const double2 yr = cmul(tj, sum);
+        const double2 vr = vcur[r];
+        wprev[r] = cadd(yr, cscale(vr, al));
+        vprev[r] = vr;
+      }
+    }
+    pending = active;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double2 a = acc.col(n - 1)[0];
+    if (pending && n > 1)
+      a = csub(a, cadd(cmul(vprev[n - 1], cconj(wprev[n - 1])), cmul(wprev[n - 1], cconj(vprev[n - 1]))));
+    d[n - 1] = a.x;
+    if (n == 1) tau[0] = make_double2(0, 0);
+  }
+  __syncthreads();
+}
+
+template <bool RESIDENT, int MAXS>
+__global__ void __launch_bounds__(kHeevThreads, (MAXS <= 9 ? 2 : 1)) heev_kernel(const EigItem* __restrict__ items,
+                                                               double2* __restrict__ hbuf,
+                                                               double* __restrict__ wbuf,
+                                                               double2* __restrict__ zbuf,
+                                                               double* __restrict__ scratch,
+                                                               int* __restrict__ info) {
   const EigItem it = items[blockIdx.x];
   const int n = it.n, nev = it.nval, nvec = it.want_vec ? it.nev : 0;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int nthr = blockDim.x, nw = nthr >> 5;
   extern __shared__ __align__(16) unsigned char smraw[];
   double2* sp = reinterpret_cast<double2*>(smraw);
-  double2* A;
-  if (RESIDENT) {
-    A = sp;
-    sp += (size_t)n * n;
-  } else {
-    A = hbuf + it.h_off;
-  }
+  double2* Apacked = sp;
+  if (RESIDENT) sp += (size_t)n * (n + 1) / 2;
   double2* vprev = sp;
   double2* wprev = vprev + n;
   double2* vcur = wprev + n;
-  double2* y = vcur + n;
-  double2* tau = y + n;
-  double2* red2 = tau + n;
-  double* d = reinterpret_cast<double*>(red2 + kMaxWarps);
+  double2* dotp = vcur + n;
+  double2* tau = dotp + n;
+  double2* part = tau + n;
+  double* d = reinterpret_cast<double*>(part + (size_t)kWarps * n);
   double* e = d + n;
   double* e2 = e + n;
   double* red = e2 + n;
-  double* lam = red + kMaxWarps;
+  double* lam = red + 2 * kWarps;
   double* lo = lam + nev;
   double* hi = lo + nev;
   double* xs = hi + nev;
@@ -232,103 +383,18 @@ __global__ void __launch_bounds__(kHeevThreads) heev_kernel(const EigItem* __res
   int* clus = cnt + kHeevThreads;
   int* misc = clus + nev + 1;
 
+  const double2* src = hbuf + it.h_off;
   if (RESIDENT) {
-    const double2* src = hbuf + it.h_off;
-    for (int i = tid; i < n * n; i += nthr) A[i] = src[i];
+    const LowerPacked pk{Apacked, n};
+    for (int c = wid; c < n; c += nw) {
+      double2* dst = pk.col(c);
+      for (int r = c + lane; r < n; r += 32) dst[r - c] = src[(size_t)c * n + r];
+    }
+    __syncthreads();
+    tridiag_lower<MAXS>(pk, n, vprev, wprev, vcur, dotp, tau, part, d, e, red);
+  } else {
+    tridiag_lower<MAXS>(LowerFull{hbuf + it.h_off, n}, n, vprev, wprev, vcur, dotp, tau, part, d, e, red);
   }
-  __syncthreads();
-
-  // ---------------------------------------------- Householder tridiagonalisation
-  bool pending = false;
-  for (int j = 0; j < n - 1; ++j) {
-    // (1) finish column j: apply the rank-2 update of step j-1.
-    for (int r = j + tid; r < n; r += nthr) {
-      double2 a = A[(long long)j * n + r];
-      if (pending) {
-        a = csub(a, cadd(cmul(vprev[r], cconj(wprev[j])), cmul(wprev[r], cconj(vprev[j]))));
-        A[(long long)j * n + r] = a;
-      }
-    }
-    __syncthreads();
-    // (2) reflector for x = A[j+1:n, j] (zlarfg convention, H = I - tau v v^H,
-    //     H^H x = beta e_1 with beta real)
-    double part = 0.0;
-    for (int r = j + 2 + tid; r < n; r += nthr) {
-      const double2 a = A[(long long)j * n + r];
-      part += a.x * a.x + a.y * a.y;
-    }
-    const double xnorm2 = block_sum(part, red);
-    const double2 alpha = A[(long long)j * n + j + 1];
-    double beta;
-    double2 tj, scal;
-    if (xnorm2 == 0.0 && alpha.y == 0.0) {
-      tj = make_double2(0, 0);
-      beta = alpha.x;
-      scal = make_double2(1, 0);
-    } else {
-      beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2), alpha.x);
-      tj = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
-      // scal = 1 / (alpha - beta)
-      const double2 den = make_double2(alpha.x - beta, alpha.y);
-      const double dd = den.x * den.x + den.y * den.y;
-      scal = make_double2(den.x / dd, -den.y / dd);
-    }
-    for (int r = j + 2 + tid; r < n; r += nthr) {
-      const double2 a = cmul(A[(long long)j * n + r], scal);
-      A[(long long)j * n + r] = a;
-      vcur[r] = a;
-    }
-    if (tid == 0) {
-      d[j] = A[(long long)j * n + j].x;
-      e[j] = beta;
-      tau[j] = tj;
-      vcur[j + 1] = make_double2(1, 0);
-    }
-    __syncthreads();
-    const bool active = tj.x != 0.0 || tj.y != 0.0;
-    // (3) fused pass over the trailing columns: apply update j-1, then
-    //     y_c = tau (A[:,c])^H v  (A Hermitian, so this is tau (A v)_c).
-    for (int c = j + 1 + wid; c < n; c += nw) {
-      double2* col = A + (long long)c * n;
-      double2 acc = make_double2(0, 0);
-      const double2 wc = pending ? cconj(wprev[c]) : make_double2(0, 0);
-      const double2 vc = pending ? cconj(vprev[c]) : make_double2(0, 0);
-      for (int r = j + 1 + lane; r < n; r += 32) {
-        double2 a = col[r];
-        if (pending) {
-          a = csub(a, cadd(cmul(vprev[r], wc), cmul(wprev[r], vc)));
-          col[r] = a;
-        }
-        acc = cadd(acc, cmulc(a, vcur[r]));
-      }
-      acc = warp_sum2(acc);
-      if (lane == 0) y[c] = cmul(tj, acc);
-    }
-    __syncthreads();
-    // (4) w = y - 1/2 tau (y^H v) v becomes the pending update.
-    double2 pp = make_double2(0, 0);
-    if (active)
-      for (int r = j + 1 + tid; r < n; r += nthr) pp = cadd(pp, cmulc(y[r], vcur[r]));
-    const double2 yv = block_sum2(pp, red2);
-    const double2 al = cscale(cmul(tj, yv), -0.5);
-    for (int r = j + 1 + tid; r < n; r += nthr) {
-      vprev[r] = vcur[r];
-      wprev[r] = active ? cadd(y[r], cmul(al, vcur[r])) : make_double2(0, 0);
-    }
-    // v_j(0) = 1 is stored for the back-transform only after every thread
-    // has read alpha = A[j+1, j] above.
-    if (tid == 0) A[(long long)j * n + j + 1] = make_double2(1, 0);
-    pending = active;
-    __syncthreads();
-  }
-  if (tid == 0) {
-    double2 a = A[(long long)(n - 1) * n + n - 1];
-    if (pending && n > 1)
-      a = csub(a, cadd(cmul(vprev[n - 1], cconj(wprev[n - 1])), cmul(wprev[n - 1], cconj(vprev[n - 1]))));
-    d[n - 1] = a.x;
-    if (n == 1) tau[0] = make_double2(0, 0);
-  }
-  __syncthreads();
 
   // ------------------------------------------------------------- eigenvalues
   // Gershgorin interval, pivmin, and negligible off-diagonals set to zero.
@@ -458,7 +524,7 @@ __global__ void __launch_bounds__(kHeevThreads) heev_kernel(const EigItem* __res
     for (int j = n - 2; j >= 0; --j) {
       const double2 tj = tau[j];
       if (tj.x == 0.0 && tj.y == 0.0) continue;
-      const double2* v = A + (long long)j * n;
+      const double2* v = (RESIDENT ? LowerPacked{Apacked, n}.col(j) : LowerFull{hbuf + it.h_off, n}.col(j)) - j;
       double2 s = make_double2(0, 0);
       for (int r = j + 1 + lane; r < n; r += 32) s = cadd(s, cmulc(v[r], z[r]));
       s = cmul(tj, warp_sum2(s));
@@ -470,29 +536,44 @@ __global__ void __launch_bounds__(kHeevThreads) heev_kernel(const EigItem* __res
 }
 
 int heev_smem_max_n() {
-  // largest n whose resident layout fits the 227 KB opt-in limit
+  // largest n whose resident (packed lower) layout fits the 227 KB opt-in limit
   const size_t lim = 227 * 1024;
   int n = 1;
   while (heev_smem_bytes(n + 1, 64, true) <= lim) ++n;
   return n;
 }
 
+namespace {
+template <bool RES, int MAXS>
+cudaError_t heev_launch_t(const EigItem* items, int nitems, size_t smem, double2* hbuf, double* wbuf,
+                          double2* zbuf, double* scratch, int* info, cudaStream_t st) {
+  cudaError_t err = cudaFuncSetAttribute(heev_kernel<RES, MAXS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err != cudaSuccess) return err;
+  heev_kernel<RES, MAXS><<<nitems, kHeevThreads, smem, st>>>(items, hbuf, wbuf, zbuf, scratch, info);
+  return cudaGetLastError();
+}
+}  // namespace
+
 cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev, double2* hbuf,
                         double* wbuf, double2* zbuf, double* scratch, int* info, cudaStream_t st) {
   if (nitems <= 0) return cudaSuccess;
   const bool resident = max_n <= heev_smem_max_n();
   const size_t smem = heev_smem_bytes(max_n, max_nev, resident);
-  cudaError_t err;
-  if (resident) {
-    err = cudaFuncSetAttribute(heev_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (err != cudaSuccess) return err;
-    heev_kernel<true><<<nitems, kHeevThreads, smem, st>>>(items, hbuf, wbuf, zbuf, scratch, info);
-  } else {
-    err = cudaFuncSetAttribute(heev_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (err != cudaSuccess) return err;
-    heev_kernel<false><<<nitems, kHeevThreads, smem, st>>>(items, hbuf, wbuf, zbuf, scratch, info);
-  }
-  return cudaGetLastError();
+  const int slots = (max_n + 31) / 32;
+#define PMX_HEEV(S)                                                                                   \
+  if (slots <= S)                                                                                     \
+    return resident ? heev_launch_t<true, S>(items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st)  \
+                    : heev_launch_t<false, S>(items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st);
+  PMX_HEEV(2)
+  PMX_HEEV(4)
+  PMX_HEEV(6)
+  PMX_HEEV(9)
+  PMX_HEEV(13)
+  PMX_HEEV(19)
+  PMX_HEEV(26)
+  PMX_HEEV(38)
+#undef PMX_HEEV
+  return cudaErrorInvalidValue;  // n > 1216
 }
 
 }  // namespace dev
