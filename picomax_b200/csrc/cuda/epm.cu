@@ -196,10 +196,15 @@ struct LowerPacked {  // packed columns in shared memory
 //   [packed lower A: n(n+1)/2 if resident] vprev[n] wprev[n] vcur[n] dotp[n] tau[n] part[kWarps*n]
 //   doubles: d[n] e[n] e2[n] red[2*kWarps] lam[nev] lo[nev] hi[nev] xs[kHeevThreads]
 //   ints: cnt[kHeevThreads] clus[nev+1] misc[4]
-__host__ __device__ inline size_t heev_smem_bytes(int n, int nev, bool resident) {
+// Depth of the per-warp prefetch ring of the global-memory path for MAXS
+// register slots (0 = direct loads; large n leaves no room for a ring).
+__host__ __device__ constexpr int heev_ring(int maxs) { return maxs <= 9 ? 3 : (maxs <= 13 ? 2 : 0); }
+
+__host__ __device__ inline size_t heev_smem_bytes(int n, int nev, bool resident, int maxs = 0) {
   size_t b = 0;
   if (resident) b += (size_t)n * (n + 1) / 2 * sizeof(double2);
-  b += (size_t)(5 + kWarps) * n * sizeof(double2);
+  if (!resident && maxs > 0) b += (size_t)kWarps * heev_ring(maxs) * 32 * maxs * sizeof(double2);
+  b += (size_t)(6 + kWarps) * n * sizeof(double2);
   b += (size_t)(3 * n + 2 * kWarps + 3 * nev + kHeevThreads) * sizeof(double);
   b += (size_t)(kHeevThreads + nev + 1 + 4) * sizeof(int);
   return b;
@@ -212,29 +217,28 @@ __host__ __device__ inline size_t heev_smem_bytes(int n, int nev, bool resident)
 // per-lane registers, column dots by warp reduction) and v^H A v; finally
 // w = tau y - tau^2/2 (v^H A v) v becomes the pending update. Three barriers
 // per step. MAXS = ceil(n / 32) register slots per lane.
-template <int MAXS, class Acc>
+template <int MAXS, int RING, class Acc>
 __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, double2* wprev, double2* vcur,
-                                              double2* dotp, double2* tau, double2* part, double* d, double* e,
-                                              double* red) {
+                                              double2* dotp, double2* tau, double2* part, double2* cnext,
+                                              double2* wring, double* d, double* e, double* red) {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   bool pending = false;
+  bool staged = false;  // column j is in cnext (rows >= j), as left by the previous fused pass
   for (int j = 0; j < n - 1; ++j) {
-    // ---- A: column j (warp 0)
+    // ---- A: column j (warp 0), from shared memory when staged
     if (wid == 0) {
       double2* cj = acc.col(j);
       double xn = 0.0;
       for (int r = j + lane; r < n; r += 32) {
-        double2 a = cj[r - j];
-        if (pending) {
-          a = csub(a, cadd(cmul(vprev[r], cconj(wprev[j])), cmul(wprev[r], cconj(vprev[j]))));
-          cj[r - j] = a;
-        }
+        double2 a = staged ? cnext[r] : cj[r - j];
+        if (pending) a = csub(a, cadd(cmul(vprev[r], cconj(wprev[j])), cmul(wprev[r], cconj(vprev[j]))));
+        cnext[r] = a;
         if (r >= j + 2) xn += a.x * a.x + a.y * a.y;
       }
       xn = warp_sum(xn);
       __syncwarp();
-      const double2 ajj = cj[0];
-      const double2 alpha = cj[1];
+      const double2 ajj = cnext[j];
+      const double2 alpha = cnext[j + 1];
       double beta;
       double2 tj, scal;
       if (xn == 0.0 && alpha.y == 0.0) {
@@ -249,8 +253,9 @@ __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, do
         scal = make_double2(den.x / dd, -den.y / dd);
       }
       __syncwarp();
+      // the reflector v_j stays in column j for the back-transform
       for (int r = j + 2 + lane; r < n; r += 32) {
-        const double2 a = cmul(cj[r - j], scal);
+        const double2 a = cmul(cnext[r], scal);
         cj[r - j] = a;
         vcur[r] = a;
       }
@@ -271,16 +276,50 @@ __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, do
     for (int s = 0; s < MAXS; ++s) yreg[s] = make_double2(0, 0);
     double vhav = 0.0;
     if (active || pending) {
-      for (int c = j + 1 + wid; c < n; c += kWarps) {
+      // Columns c = c0 + kWarps t of this warp. With RING > 0 every lane
+      // prefetches its own rows of the next RING columns into a per-warp ring
+      // in shared memory (cp.async); each lane reads back only what it copied,
+      // so the per-thread wait_group is the only synchronisation.
+      const int c0 = j + 1 + wid;
+      double2* ring = wring + (size_t)wid * (RING > 0 ? RING : 1) * 32 * MAXS;
+      auto issue = [&](int t) {
+        if (RING > 0) {
+          const int c = c0 + kWarps * t;
+          if (c < n) {
+            const double2* cc = acc.col(c);
+            double2* buf = ring + (t % (RING > 0 ? RING : 1)) * 32 * MAXS;
+#pragma unroll
+            for (int s = 0; s < MAXS; ++s) {
+              const int r = 32 * s + lane;
+              if (r >= c && r < n) cp_async16(buf + 32 * s + lane, cc + (r - c));
+            }
+          }
+          cp_async_commit();
+        }
+      };
+#pragma unroll
+      for (int t = 0; t < RING; ++t) issue(t);
+      for (int t = 0; c0 + kWarps * t < n; ++t) {
+        const int c = c0 + kWarps * t;
         double2* cc = acc.col(c);
         const double2 vc = vcur[c];
         const double vc2 = vc.x * vc.x + vc.y * vc.y;
         const double2 wcc = cconj(wprev[c]), vcc = cconj(vprev[c]);
         double2 a[MAXS];
+        if (RING > 0) {
+          cp_async_wait<(RING > 0 ? RING - 1 : 0)>();
+          const double2* buf = ring + (t % (RING > 0 ? RING : 1)) * 32 * MAXS;
 #pragma unroll
-        for (int s = 0; s < MAXS; ++s) {
-          const int r = 32 * s + lane;
-          a[s] = (r >= c && r < n) ? cc[r - c] : make_double2(0, 0);
+          for (int s = 0; s < MAXS; ++s) {
+            const int r = 32 * s + lane;
+            a[s] = (r >= c && r < n) ? buf[32 * s + lane] : make_double2(0, 0);
+          }
+        } else {
+#pragma unroll
+          for (int s = 0; s < MAXS; ++s) {
+            const int r = 32 * s + lane;
+            a[s] = (r >= c && r < n) ? cc[r - c] : make_double2(0, 0);
+          }
         }
         double2 dot = make_double2(0, 0);
 #pragma unroll
@@ -290,26 +329,33 @@ __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, do
             double2 v = a[s];
             if (pending) {
               v = csub(v, cadd(cmul(vprev[r], wcc), cmul(wprev[r], vcc)));
-              cc[r - c] = v;
+              if (c == j + 1)
+                cnext[r] = v;  // next step's column, kept on chip
+              else
+                cc[r - c] = v;
+            } else if (c == j + 1) {
+              cnext[r] = v;
             }
             if (active) {
               yreg[s] = cadd(yreg[s], cmul(v, vc));
               if (r > c) {
                 const double2 vr = vcur[r];
                 dot = cadd(dot, cmulc(v, vr));
-                const double2 t = cmul(cmulc(vr, v), vc);  // conj(v_r) A_rc v_c
-                vhav += 2.0 * t.x;
+                const double2 tt = cmul(cmulc(vr, v), vc);  // conj(v_r) A_rc v_c
+                vhav += 2.0 * tt.x;
               } else {
                 vhav += v.x * vc2;
               }
             }
           }
         }
+        issue(t + RING);
         if (active) {
           dot = warp_sum2(dot);
           if (lane == 0) dotp[c] = dot;
         }
       }
+      if (RING > 0) cp_async_wait<0>();
     }
     if (active) {
 #pragma unroll
@@ -337,11 +383,12 @@ __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, do
         vprev[r] = vr;
       }
     }
+    staged = active || pending;
     pending = active;
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    double2 a = acc.col(n - 1)[0];
+    double2 a = staged ? cnext[n - 1] : acc.col(n - 1)[0];
     if (pending && n > 1)
       a = csub(a, cadd(cmul(vprev[n - 1], cconj(wprev[n - 1])), cmul(wprev[n - 1], cconj(vprev[n - 1]))));
     d[n - 1] = a.x;
@@ -351,7 +398,7 @@ __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, do
 }
 
 template <bool RESIDENT, int MAXS>
-__global__ void __launch_bounds__(kHeevThreads, (MAXS <= 9 ? 2 : 1)) heev_kernel(const EigItem* __restrict__ items,
+__global__ void __launch_bounds__(kHeevThreads, 1) heev_kernel(const EigItem* __restrict__ items,
                                                                double2* __restrict__ hbuf,
                                                                double* __restrict__ wbuf,
                                                                double2* __restrict__ zbuf,
@@ -371,7 +418,11 @@ __global__ void __launch_bounds__(kHeevThreads, (MAXS <= 9 ? 2 : 1)) heev_kernel
   double2* dotp = vcur + n;
   double2* tau = dotp + n;
   double2* part = tau + n;
-  double* d = reinterpret_cast<double*>(part + (size_t)kWarps * n);
+  double2* cnext = part + (size_t)kWarps * n;
+  double2* wring = cnext + n;  // per-warp prefetch ring (global-memory path)
+  if (!RESIDENT) sp = wring + (size_t)kWarps * heev_ring(MAXS) * 32 * MAXS;
+  else sp = wring;
+  double* d = reinterpret_cast<double*>(sp);
   double* e = d + n;
   double* e2 = e + n;
   double* red = e2 + n;
@@ -391,9 +442,10 @@ __global__ void __launch_bounds__(kHeevThreads, (MAXS <= 9 ? 2 : 1)) heev_kernel
       for (int r = c + lane; r < n; r += 32) dst[r - c] = src[(size_t)c * n + r];
     }
     __syncthreads();
-    tridiag_lower<MAXS>(pk, n, vprev, wprev, vcur, dotp, tau, part, d, e, red);
+    tridiag_lower<MAXS, 0>(pk, n, vprev, wprev, vcur, dotp, tau, part, cnext, wring, d, e, red);
   } else {
-    tridiag_lower<MAXS>(LowerFull{hbuf + it.h_off, n}, n, vprev, wprev, vcur, dotp, tau, part, d, e, red);
+    tridiag_lower<MAXS, heev_ring(MAXS)>(LowerFull{hbuf + it.h_off, n}, n, vprev, wprev, vcur, dotp, tau, part, cnext,
+                                         wring, d, e, red);
   }
 
   // ------------------------------------------------------------- eigenvalues
@@ -560,10 +612,11 @@ cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev
   const bool resident = max_n <= heev_smem_max_n();
   const size_t smem = heev_smem_bytes(max_n, max_nev, resident);
   const int slots = (max_n + 31) / 32;
-#define PMX_HEEV(S)                                                                                   \
-  if (slots <= S)                                                                                     \
-    return resident ? heev_launch_t<true, S>(items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st)  \
-                    : heev_launch_t<false, S>(items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st);
+#define PMX_HEEV(S)                                                                                        \
+  if (slots <= S)                                                                                          \
+    return resident ? heev_launch_t<true, S>(items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st)       \
+                    : heev_launch_t<false, S>(items, nitems, heev_smem_bytes(max_n, max_nev, false, S), hbuf, \
+                                              wbuf, zbuf, scratch, info, st);
   PMX_HEEV(2)
   PMX_HEEV(4)
   PMX_HEEV(6)
