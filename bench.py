@@ -305,6 +305,7 @@ def ours(args, rank, world):
         "gpu_launches": int((l1 - l0) / args.steps),
         "roofline": roof, "clocks": clk.summary(),
         "degenerate_cuts": ctx.degenerate_cuts(),
+        "autotune": ctx.tuning(),
     }
     if rank == 0 and world == 1:
         cb = cpu_baseline_sample(argv, nspec)

@@ -104,6 +104,13 @@ void* pmx_ctx_stream(const pmx_ctx* ctx);
  * created: "assemble", "heev", "overlap", "contract_f64", "contract_mixed",
  * "scale", "kk". */
 int pmx_ctx_kernel_time(const pmx_ctx* ctx, const char* family, double* ms, long long* launches);
+/* Autotuner of the batched eigensolver schedule (on by default): the first
+ * batch of at least 148 matrices of a given size times every schedule once,
+ * keeps the fastest for the rest of the context's life. New in this build. */
+int pmx_ctx_set_autotune(pmx_ctx* ctx, int on);
+/* The autotuner's choices and trial times as JSON text (NUL-terminated,
+ * truncated at len; full length in *needed). */
+int pmx_ctx_tuning(const pmx_ctx* ctx, char* buf, size_t len, size_t* needed);
 /* Bytes copied host->device and device->host by this context so far. */
 int pmx_ctx_transfer_bytes(const pmx_ctx* ctx, long long* h2d_bytes, long long* d2h_bytes);
 /* k and k+q points of the last pmx_chi* call at which the NBAND window cut a

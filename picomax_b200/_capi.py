@@ -36,7 +36,7 @@ EXPORTS = (
     "pmx_ctx_stage_times", "pmx_ctx_kernel_launches", "pmx_hamiltonian", "pmx_heev_batched",
     "pmx_ref_energy", "pmx_band", "pmx_chi", "pmx_kk", "pmx_main", "pmx_ctx_stream",
     "pmx_ctx_transfer_bytes", "pmx_ctx_degenerate_cuts", "pmx_chi_device", "pmx_chi_epsm",
-    "pmx_eps_macroscopic", "pmx_ctx_kernel_time",
+    "pmx_eps_macroscopic", "pmx_ctx_kernel_time", "pmx_ctx_set_autotune", "pmx_ctx_tuning",
 )
 
 
@@ -97,6 +97,8 @@ def load() -> ctypes.CDLL:
         "pmx_chi_epsm": (c_int, [c_void_p, c_void_p, c_int, c_int, dp, dp, dp]),
         "pmx_eps_macroscopic": (c_int, [c_void_p, c_int, c_int, c_int, dp, dp, dp]),
         "pmx_ctx_kernel_time": (c_int, [c_void_p, c_char_p, dp, POINTER(c_longlong)]),
+        "pmx_ctx_set_autotune": (c_int, [c_void_p, c_int]),
+        "pmx_ctx_tuning": (c_int, [c_void_p, c_char_p, c_size_t, POINTER(c_size_t)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -261,6 +263,17 @@ class Context:
         ms, n = c_double(), c_longlong()
         self._lib.pmx_ctx_kernel_time(self.handle, family.encode(), ctypes.byref(ms), ctypes.byref(n))
         return ms.value, n.value
+
+    def set_autotune(self, on: bool):
+        self._lib.pmx_ctx_set_autotune(self.handle, 1 if on else 0)
+
+    def tuning(self) -> dict:
+        import json
+        need = c_size_t()
+        self._lib.pmx_ctx_tuning(self.handle, None, 0, ctypes.byref(need))
+        buf = ctypes.create_string_buffer(need.value)
+        self._lib.pmx_ctx_tuning(self.handle, buf, need.value, ctypes.byref(need))
+        return json.loads(buf.value.decode())
 
     def degenerate_cuts(self) -> int:
         return int(self._lib.pmx_ctx_degenerate_cuts(self.handle))

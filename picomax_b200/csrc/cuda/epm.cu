@@ -196,14 +196,12 @@ struct LowerPacked {  // packed columns in shared memory
 //   [packed lower A: n(n+1)/2 if resident] vprev[n] wprev[n] vcur[n] dotp[n] tau[n] part[kWarps*n]
 //   doubles: d[n] e[n] e2[n] red[2*kWarps] lam[nev] lo[nev] hi[nev] xs[kHeevThreads]
 //   ints: cnt[kHeevThreads] clus[nev+1] misc[4]
-// Depth of the per-warp prefetch ring of the global-memory path for MAXS
-// register slots (0 = direct loads; large n leaves no room for a ring).
-__host__ __device__ constexpr int heev_ring(int maxs) { return maxs <= 9 ? 3 : (maxs <= 13 ? 2 : 0); }
-
-__host__ __device__ inline size_t heev_smem_bytes(int n, int nev, bool resident, int maxs = 0) {
+// ring = depth of the per-warp prefetch ring of the global-memory path
+// (0 = direct loads from L2).
+__host__ __device__ inline size_t heev_smem_bytes(int n, int nev, bool resident, int maxs = 0, int ring = 0) {
   size_t b = 0;
   if (resident) b += (size_t)n * (n + 1) / 2 * sizeof(double2);
-  if (!resident && maxs > 0) b += (size_t)kWarps * heev_ring(maxs) * 32 * maxs * sizeof(double2);
+  if (!resident && maxs > 0) b += (size_t)kWarps * ring * 32 * maxs * sizeof(double2);
   b += (size_t)(6 + kWarps) * n * sizeof(double2);
   b += (size_t)(3 * n + 2 * kWarps + 3 * nev + kHeevThreads) * sizeof(double);
   b += (size_t)(kHeevThreads + nev + 1 + 4) * sizeof(int);
@@ -397,8 +395,8 @@ __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, do
   __syncthreads();
 }
 
-template <bool RESIDENT, int MAXS>
-__global__ void __launch_bounds__(kHeevThreads, 1) heev_kernel(const EigItem* __restrict__ items,
+template <bool RESIDENT, int MAXS, int RING>
+__global__ void __launch_bounds__(kHeevThreads, (RING >= 2 || MAXS > 9) ? 1 : 2) heev_kernel(const EigItem* __restrict__ items,
                                                                double2* __restrict__ hbuf,
                                                                double* __restrict__ wbuf,
                                                                double2* __restrict__ zbuf,
@@ -420,7 +418,7 @@ __global__ void __launch_bounds__(kHeevThreads, 1) heev_kernel(const EigItem* __
   double2* part = tau + n;
   double2* cnext = part + (size_t)kWarps * n;
   double2* wring = cnext + n;  // per-warp prefetch ring (global-memory path)
-  if (!RESIDENT) sp = wring + (size_t)kWarps * heev_ring(MAXS) * 32 * MAXS;
+  if (!RESIDENT) sp = wring + (size_t)kWarps * RING * 32 * MAXS;
   else sp = wring;
   double* d = reinterpret_cast<double*>(sp);
   double* e = d + n;
@@ -444,8 +442,8 @@ __global__ void __launch_bounds__(kHeevThreads, 1) heev_kernel(const EigItem* __
     __syncthreads();
     tridiag_lower<MAXS, 0>(pk, n, vprev, wprev, vcur, dotp, tau, part, cnext, wring, d, e, red);
   } else {
-    tridiag_lower<MAXS, heev_ring(MAXS)>(LowerFull{hbuf + it.h_off, n}, n, vprev, wprev, vcur, dotp, tau, part, cnext,
-                                         wring, d, e, red);
+    tridiag_lower<MAXS, RING>(LowerFull{hbuf + it.h_off, n}, n, vprev, wprev, vcur, dotp, tau, part, cnext, wring,
+                              d, e, red);
   }
 
   // ------------------------------------------------------------- eigenvalues
@@ -596,27 +594,47 @@ int heev_smem_max_n() {
 }
 
 namespace {
-template <bool RES, int MAXS>
+template <bool RES, int MAXS, int RING>
 cudaError_t heev_launch_t(const EigItem* items, int nitems, size_t smem, double2* hbuf, double* wbuf,
                           double2* zbuf, double* scratch, int* info, cudaStream_t st) {
-  cudaError_t err = cudaFuncSetAttribute(heev_kernel<RES, MAXS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t err =
+      cudaFuncSetAttribute(heev_kernel<RES, MAXS, RING>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
-  heev_kernel<RES, MAXS><<<nitems, kHeevThreads, smem, st>>>(items, hbuf, wbuf, zbuf, scratch, info);
+  heev_kernel<RES, MAXS, RING><<<nitems, kHeevThreads, smem, st>>>(items, hbuf, wbuf, zbuf, scratch, info);
   return cudaGetLastError();
 }
 }  // namespace
 
+int heev_variants(int max_n) {
+  const int slots = (max_n + 31) / 32;
+  if (max_n <= heev_smem_max_n()) return 1;  // shared-memory resident: one variant
+  return slots <= 13 ? 3 : 1;
+}
+
 cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev, double2* hbuf,
-                        double* wbuf, double2* zbuf, double* scratch, int* info, cudaStream_t st) {
+                        double* wbuf, double2* zbuf, double* scratch, int* info, cudaStream_t st, int variant) {
   if (nitems <= 0) return cudaSuccess;
   const bool resident = max_n <= heev_smem_max_n();
-  const size_t smem = heev_smem_bytes(max_n, max_nev, resident);
   const int slots = (max_n + 31) / 32;
-#define PMX_HEEV(S)                                                                                        \
-  if (slots <= S)                                                                                          \
-    return resident ? heev_launch_t<true, S>(items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st)       \
-                    : heev_launch_t<false, S>(items, nitems, heev_smem_bytes(max_n, max_nev, false, S), hbuf, \
-                                              wbuf, zbuf, scratch, info, st);
+  // global-memory path variants: 0 = direct L2 loads (2 CTAs/SM), 1 = one-column
+  // prefetch buffer per warp (2 CTAs/SM), 2 = three-column ring (1 CTA/SM)
+  const int ring = resident ? 0 : (variant == 1 ? 1 : (variant == 2 ? 3 : 0));
+#define PMX_HEEV(S)                                                                                          \
+  if (slots <= S) {                                                                                          \
+    if (resident)                                                                                            \
+      return heev_launch_t<true, S, 0>(items, nitems, heev_smem_bytes(max_n, max_nev, true), hbuf, wbuf, zbuf, \
+                                       scratch, info, st);                                                   \
+    if (ring == 3 && S <= 13)                                                                                \
+      return heev_launch_t<false, S, (S <= 13 ? 3 : 0)>(items, nitems,                                        \
+                                                        heev_smem_bytes(max_n, max_nev, false, S, 3), hbuf,   \
+                                                        wbuf, zbuf, scratch, info, st);                      \
+    if (ring == 1 && S <= 13)                                                                                \
+      return heev_launch_t<false, S, (S <= 13 ? 1 : 0)>(items, nitems,                                        \
+                                                        heev_smem_bytes(max_n, max_nev, false, S, 1), hbuf,   \
+                                                        wbuf, zbuf, scratch, info, st);                      \
+    return heev_launch_t<false, S, 0>(items, nitems, heev_smem_bytes(max_n, max_nev, false, S, 0), hbuf, wbuf, \
+                                      zbuf, scratch, info, st);                                              \
+  }
   PMX_HEEV(2)
   PMX_HEEV(4)
   PMX_HEEV(6)

@@ -47,9 +47,13 @@ cudaError_t launch_assemble(const CrystalDev* crystals, const EigItem* items, in
 
 // Eigensolve of every item. Matrices with n <= smem_max_n run with the matrix
 // resident in shared memory. info[i] != 0 flags a failure of item i.
+// variant selects the global-memory path schedule (see heev_variants); the
+// resident path ignores it.
 cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev, double2* hbuf,
-                        double* wbuf, double2* zbuf, double* scratch, int* info, cudaStream_t st);
+                        double* wbuf, double2* zbuf, double* scratch, int* info, cudaStream_t st, int variant = 0);
 int heev_smem_max_n();
+// Number of schedules launch_heev offers for matrices of size max_n.
+int heev_variants(int max_n);
 
 }  // namespace dev
 }  // namespace pmx

@@ -242,6 +242,11 @@ struct pmx_ctx {
   std::map<std::string, std::pair<double, long long>> ktime;
   std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> kpending;
   std::vector<cudaEvent_t> evpool;
+  // autotuner: chosen eigensolver schedule per (n, nval, vectors) and the
+  // device times measured when it was chosen
+  bool autotune = true;
+  std::map<long long, int> heev_choice;
+  std::map<long long, std::vector<float>> heev_trials;
   // named workspaces
   DevBuf crystal, g, hkl, vloc, vso, items, hbuf, wbuf, zk, zq, scratch, info;
   DevBuf loci, kpts, uvec, ssoc, qgn, ncd, nvd, cbase, vbase, cidx, vidx, blkoff, dest;
@@ -413,11 +418,40 @@ void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int 
       CK(pmx::dev::launch_assemble(dc.dev, c->items.as<pmx::dev::EigItem>(), cnt, dc.npw, c->hbuf.as<double2>(),
                                    c->stream));
     }
+    // eigensolver schedule: cached choice, or timed once on the first large
+    // enough chunk (every candidate runs on that chunk; the chosen one runs
+    // last so the results come from it)
+    const long long key = ((long long)n * 1024 + nval) * 2 + (vec ? 1 : 0);
+    int variant = 0;
+    const int nvar = pmx::dev::heev_variants(n);
+    auto it_choice = c->heev_choice.find(key);
+    if (it_choice != c->heev_choice.end()) {
+      variant = it_choice->second;
+    } else if (nvar > 1 && c->autotune && cnt >= 148) {
+      std::vector<float> ms(nvar, 0.f);
+      for (int v = 0; v < nvar; ++v) {
+        CK(cudaEventRecord(c->ev[0], c->stream));
+        CK(pmx::dev::launch_heev(c->items.as<pmx::dev::EigItem>(), cnt, n, nval, c->hbuf.as<double2>(),
+                                 c->wbuf.as<double>(), vec ? zdev : c->hbuf.as<double2>(), c->scratch.as<double>(),
+                                 c->info.as<int>(), c->stream, v));
+        CK(cudaEventRecord(c->ev[1], c->stream));
+        CK(cudaEventSynchronize(c->ev[1]));
+        CK(cudaEventElapsedTime(&ms[v], c->ev[0], c->ev[1]));
+        c->launches += 1;
+        // H is overwritten by the reduction: rebuild it for the next candidate
+        CK(pmx::dev::launch_assemble(dc.dev, c->items.as<pmx::dev::EigItem>(), cnt, dc.npw, c->hbuf.as<double2>(),
+                                     c->stream));
+        c->launches += 1;
+      }
+      variant = (int)(std::min_element(ms.begin(), ms.end()) - ms.begin());
+      c->heev_choice[key] = variant;
+      c->heev_trials[key] = ms;
+    }
     {
       KTime kt(c, "heev");
       CK(pmx::dev::launch_heev(c->items.as<pmx::dev::EigItem>(), cnt, n, nval, c->hbuf.as<double2>(),
                                c->wbuf.as<double>(), vec ? zdev : c->hbuf.as<double2>(), c->scratch.as<double>(),
-                               c->info.as<int>(), c->stream));
+                               c->info.as<int>(), c->stream, variant));
     }
     c->launches += 2;
     CK(cudaMemcpyAsync(info.data(), c->info.ptr, sizeof(int) * cnt, cudaMemcpyDeviceToHost, c->stream));
@@ -985,6 +1019,38 @@ extern "C" int pmx_ctx_transfer_bytes(const pmx_ctx* c, long long* h2d_bytes, lo
 }
 
 extern "C" int pmx_ctx_degenerate_cuts(const pmx_ctx* c) { return c ? c->degenerate_cuts : -1; }
+
+extern "C" int pmx_ctx_set_autotune(pmx_ctx* c, int on) {
+  if (!c) return PMX_ERR_INVALID;
+  c->autotune = on != 0;
+  return PMX_OK;
+}
+
+extern "C" int pmx_ctx_tuning(const pmx_ctx* c, char* buf, size_t len, size_t* needed) {
+  if (!c) return PMX_ERR_INVALID;
+  std::ostringstream os;
+  os << "{\"heev\": [";
+  bool first = true;
+  for (auto& kv : c->heev_choice) {
+    const long long key = kv.first;
+    os << (first ? "" : ", ") << "{\"n\": " << key / 2 / 1024 << ", \"nval\": " << (key / 2) % 1024
+       << ", \"vectors\": " << (key % 2) << ", \"variant\": " << kv.second << ", \"trial_ms\": [";
+    auto t = c->heev_trials.find(key);
+    if (t != c->heev_trials.end())
+      for (size_t i = 0; i < t->second.size(); ++i) os << (i ? ", " : "") << t->second[i];
+    os << "]}";
+    first = false;
+  }
+  os << "]}";
+  const std::string s = os.str();
+  if (needed) *needed = s.size() + 1;
+  if (buf && len > 0) {
+    const size_t n = std::min(len - 1, s.size());
+    std::memcpy(buf, s.data(), n);
+    buf[n] = 0;
+  }
+  return PMX_OK;
+}
 
 extern "C" int pmx_eps_macroscopic(pmx_ctx* ctx, int neps, int nq, int nfreq, const double* chi_re,
                                    const double* chi_im, double* epsm) {

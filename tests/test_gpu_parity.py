@@ -158,3 +158,29 @@ def test_degenerate_cut_reported(ctx, tmp_path):
     p = pm.Problem(args)
     ctx.chi(p, pm.SWITCH_EPSLL)
     assert ctx.degenerate_cuts() >= 1
+
+
+def test_heev_schedules_agree(tmp_path):
+    """Every eigensolver schedule the autotuner can pick gives the same spectrum."""
+    from conftest import gpu_available
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    from picomax_b200.kgrid import write_kfile
+    g = load_golden("gaas_soc_band")
+    args = [str(a) for a in g["argv"]]
+    # 200 k-points so that the autotuner runs (>= 148 matrices in one batch)
+    rng = np.random.default_rng(5)
+    K = rng.uniform(-0.5, 0.5, (200, 3))
+    kf = os.path.join(str(tmp_path), "k.txt")
+    write_kfile(kf, K, np.ones(len(K)))
+    args = [a for a in args if a not in ("band",)]
+    base = args[args.index("-crystal"):]
+    p = pm.Problem(["-switch", "band", "-kpoint", "0", "-kpointfile", kf] + base)
+    c1 = pm.Context(0)
+    e1 = c1.band(p)  # autotuned (trial of every schedule on the first batch)
+    c2 = pm.Context(0)
+    c2.set_autotune(False)
+    e2 = c2.band(p)  # default schedule
+    assert np.max(np.abs(e1 - e2)) < 1e-10
+    c1.close()
+    c2.close()
