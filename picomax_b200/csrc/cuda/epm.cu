@@ -301,7 +301,6 @@ __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, do
         const int c = c0 + kWarps * t;
         double2* cc = acc.col(c);
         const double2 vc = vcur[c];
-        const double vc2 = vc.x * vc.x + vc.y * vc.y;
         const double2 wcc = cconj(wprev[c]), vcc = cconj(vprev[c]);
         double2 a[MAXS];
         if (RING > 0) {
@@ -336,14 +335,7 @@ __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, do
             }
             if (active) {
               yreg[s] = cadd(yreg[s], cmul(v, vc));
-              if (r > c) {
-                const double2 vr = vcur[r];
-                dot = cadd(dot, cmulc(v, vr));
-                const double2 tt = cmul(cmulc(vr, v), vc);  // conj(v_r) A_rc v_c
-                vhav += 2.0 * tt.x;
-              } else {
-                vhav += v.x * vc2;
-              }
+              if (r > c) dot = cadd(dot, cmulc(v, vcur[r]));
             }
           }
         }
@@ -351,17 +343,25 @@ __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, do
         if (active) {
           dot = warp_sum2(dot);
           if (lane == 0) dotp[c] = dot;
+          vhav += cmulc(vc, dot).x;  // conj(v_c) (column part of y_c), same on every lane
         }
       }
       if (RING > 0) cp_async_wait<0>();
     }
     if (active) {
+      // v^H A v = sum_r conj(v_r) y_r with y = sum over warps of the row
+      // partials plus the column dots; this warp's share of both (the column
+      // dot share was added once per column above, identically on all lanes).
+      double vrow = 0.0;
 #pragma unroll
       for (int s = 0; s < MAXS; ++s) {
         const int r = 32 * s + lane;
-        if (r >= j + 1 && r < n) part[wid * n + r] = yreg[s];
+        if (r >= j + 1 && r < n) {
+          part[wid * n + r] = yreg[s];
+          vrow += cmulc(vcur[r], yreg[s]).x;
+        }
       }
-      vhav = warp_sum(vhav);
+      vhav = warp_sum(vrow) + vhav;
       if (lane == 0) red[wid] = vhav;
     }
     __syncthreads();
