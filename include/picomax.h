@@ -104,6 +104,10 @@ void* pmx_ctx_stream(const pmx_ctx* ctx);
  * created: "assemble", "heev", "overlap", "contract_f64", "contract_mixed",
  * "scale", "kk". */
 int pmx_ctx_kernel_time(const pmx_ctx* ctx, const char* family, double* ms, long long* launches);
+/* Precision of the mixed path's FP32 overlap operands in the last pmx_chi*
+ * call: max over all transitions and G of ||M_fp32|^2 - |M|^2| and max |M|^2.
+ * New diagnostic (no reference counterpart). */
+int pmx_ctx_overlap_error(const pmx_ctx* ctx, double* max_abs2_err, double* max_abs2);
 /* Autotuner of the batched eigensolver schedule (on by default): the first
  * batch of at least 148 matrices of a given size times every schedule once,
  * keeps the fastest for the rest of the context's life. New in this build. */

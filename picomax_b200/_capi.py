@@ -37,6 +37,7 @@ EXPORTS = (
     "pmx_ref_energy", "pmx_band", "pmx_chi", "pmx_kk", "pmx_main", "pmx_ctx_stream",
     "pmx_ctx_transfer_bytes", "pmx_ctx_degenerate_cuts", "pmx_chi_device", "pmx_chi_epsm",
     "pmx_eps_macroscopic", "pmx_ctx_kernel_time", "pmx_ctx_set_autotune", "pmx_ctx_tuning",
+    "pmx_ctx_overlap_error",
 )
 
 
@@ -98,6 +99,7 @@ def load() -> ctypes.CDLL:
         "pmx_eps_macroscopic": (c_int, [c_void_p, c_int, c_int, c_int, dp, dp, dp]),
         "pmx_ctx_kernel_time": (c_int, [c_void_p, c_char_p, dp, POINTER(c_longlong)]),
         "pmx_ctx_set_autotune": (c_int, [c_void_p, c_int]),
+        "pmx_ctx_overlap_error": (c_int, [c_void_p, dp, dp]),
         "pmx_ctx_tuning": (c_int, [c_void_p, c_char_p, c_size_t, POINTER(c_size_t)]),
     }
     for name, (res, args) in sig.items():
@@ -263,6 +265,12 @@ class Context:
         ms, n = c_double(), c_longlong()
         self._lib.pmx_ctx_kernel_time(self.handle, family.encode(), ctypes.byref(ms), ctypes.byref(n))
         return ms.value, n.value
+
+    def overlap_error(self):
+        """(max ||M32|^2 - |M|^2|, max |M|^2) of the last mixed-precision chi call."""
+        a, b = c_double(), c_double()
+        self._lib.pmx_ctx_overlap_error(self.handle, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
 
     def set_autotune(self, on: bool):
         self._lib.pmx_ctx_set_autotune(self.handle, 1 if on else 0)

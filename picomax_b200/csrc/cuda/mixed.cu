@@ -42,7 +42,8 @@ constexpr int kPairs = 64;     // pairs per tile (kM / 2)
 constexpr int kN = 256;        // frequencies per tile
 constexpr int kKC = 32;        // transitions per chunk
 constexpr int kThreads = 256;
-constexpr int kPieceChunks = 64;  // chunks per K-split piece (2048 transitions)
+constexpr int kFlushChunks = 64;  // chunks (2048 transitions) per FP32 accumulation before the FP64 flush
+constexpr int kTargetCtas = 4 * 148;  // K-split so that the grid covers the SMs a few times
 constexpr unsigned kWaitLimit = 1u << 26;
 constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s
 
@@ -179,7 +180,7 @@ struct Plan {
   int2* tiles;       // [ntile] (a block, b block)
   float* wgt32;      // [T]
   uint8_t* wbuf;     // [nchunk][32 KB]
-  float* part;       // [nitem][ntile][128][256]
+  double* part;      // [nitem][ntile][128][256] FP64 partial tiles
   int* err;          // error flag
 };
 
@@ -258,8 +259,11 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_kernel(Plan pl, ContractArg
 
   int* s_last = s_abort + 1;  // index (from c_begin) of the last committed chunk, -1 if none
   if (tid == 0) *s_last = -1;
+  double* out = pl.part + ((size_t)item_id * pl.ntile + tile) * (kM * kN);
+  int flushes = 0;
   for (int c = c_begin; c < c_end; ++c) {
     const int n = c - c_begin, s = n & 1;
+    const int g = n % kFlushChunks;  // position inside the current FP32 accumulation group
     uint8_t* st = stage[s];
     // the stage is free once the MMAs of chunk n-2 (same stage) completed
     if (tid == 0 && n >= 2 && !*s_abort && !mbar_wait(&mdone[s], ((n - 2) >> 1) & 1)) {
@@ -337,7 +341,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_kernel(Plan pl, ContractArg
           const uint64_t alo = umma_desc(sa + kABytes + ks * 2 * (kM / 8) * 128, (kM / 8) * 128, 128);
           const uint64_t bhi = umma_desc(sb + ks * 2 * (kN / 8) * 128, (kN / 8) * 128, 128);
           const uint64_t blo = umma_desc(sb + kBBytes + ks * 2 * (kN / 8) * 128, (kN / 8) * 128, 128);
-          const uint32_t acc0 = (n > 0 || ks > 0) ? 1u : 0u;
+          const uint32_t acc0 = (g > 0 || ks > 0) ? 1u : 0u;
           mma_bf16(tmem, ahi, bhi, acc0);
           mma_bf16(tmem, ahi, blo, 1u);
           mma_bf16(tmem, alo, bhi, 1u);
@@ -345,6 +349,38 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_kernel(Plan pl, ContractArg
         mma_commit(&mdone[s]);
         *s_last = n;
       }
+    }
+    // flush the FP32 accumulator into the CTA's FP64 tile at the end of every
+    // group and of the range (the commit of chunk n covers all earlier MMAs)
+    if (g == kFlushChunks - 1 || c == c_end - 1) {
+      if (tid == 0 && !*s_abort && !mbar_wait(&mdone[s], (n >> 1) & 1)) {
+        atomicExch(pl.err, 4);
+        *s_abort = 1;
+      }
+      __syncthreads();
+      tc_fence_after();
+      if (*s_abort) break;
+      if (wid < 4) {
+        const int row = wid * 32 + lane;
+        for (int cb = 0; cb < kN; cb += 8) {
+          uint32_t r[8];
+          const uint32_t taddr = tmem + ((uint32_t)(wid * 32) << 16) + cb;
+          asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                         "=r"(r[7])
+                       : "r"(taddr));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          double* dst = out + (size_t)row * kN + cb;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const double v = (double)__uint_as_float(r[q]);
+            dst[q] = flushes == 0 ? v : dst[q] + v;
+          }
+        }
+      }
+      ++flushes;
+      tc_fence_before();
+      __syncthreads();
     }
   }
   __syncthreads();
@@ -357,41 +393,16 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_kernel(Plan pl, ContractArg
   }
   __syncthreads();
   tc_fence_after();
-  const bool have = nlast >= 0 && !*s_abort;
-  // epilogue: TMEM lane r = row r; warps 0-3 read 32 rows each
-  float* out = pl.part + ((size_t)item_id * pl.ntile + tile) * (kM * kN);
-  if (wid < 4) {
-    const int row = wid * 32 + lane;
-    for (int cb = 0; cb < kN; cb += 32) {
-      uint32_t r[32];
-      const uint32_t taddr = tmem + ((uint32_t)(wid * 32) << 16) + cb;
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
-            "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
-            "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
-            "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-          : "r"(taddr));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      float4* dst = reinterpret_cast<float4*>(out + (size_t)row * kN + cb);
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        float4 v = make_float4(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1]),
-                               __uint_as_float(r[4 * q + 2]), __uint_as_float(r[4 * q + 3]));
-        if (!have) v = make_float4(0.f, 0.f, 0.f, 0.f);
-        dst[q] = v;
-      }
-    }
-  }
+  // an empty range still owns its tile: zero it
+  if (flushes == 0)
+    for (int idx = tid; idx < kM * kN; idx += kThreads) out[idx] = 0.0;
   tc_fence_before();
   __syncthreads();
   if (wid == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kN));
 }
 
-// Sums the FP32 partials of each frequency tile's pieces in FP64, in piece
-// order, and scatters rows to acc[2][9][np][nf] (P1 -> Im, P2 -> Re).
+// Sums the FP64 partial tiles of each frequency tile's pieces in piece order
+// and scatters rows to acc[2][9][np][nf] (P1 -> Im, P2 -> Re).
 __global__ void __launch_bounds__(256) reduce_kernel(Plan pl, ContractArgs a) {
   const int tile = blockIdx.x, ft = blockIdx.y;
   const int2 tb = pl.tiles[tile];
@@ -409,7 +420,7 @@ __global__ void __launch_bounds__(256) reduce_kernel(Plan pl, ContractArgs a) {
     if (n > m) continue;
     double s = 0.0;
     for (int itm = ir.x; itm < ir.y; ++itm)
-      s += (double)pl.part[((size_t)itm * pl.ntile + tile) * (kM * kN) + idx];
+      s += pl.part[((size_t)itm * pl.ntile + tile) * (kM * kN) + idx];
     const size_t o = ((size_t)(i * 3 + j) * a.np + (size_t)m * (m + 1) / 2 + n) * a.nf + f;
     if (row < kPairs)
       a.acc[blk + o] = s;  // Im part
@@ -431,6 +442,18 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 HostPlan make_plan(const ContractArgs& a, const int2* trange_host, int nft) {
   HostPlan h;
+  const int A = 3 * a.neps, nb = (A + 7) / 8;
+  for (int i = 0; i < nb; ++i)
+    for (int j = 0; j < nb; ++j) {
+      const int amax = std::min(8 * i + 7, A - 1), bmin = 8 * j;
+      if (amax / 3 >= bmin / 3) h.tiles.push_back(make_int2(i, j));
+    }
+  long long total = 0;
+  for (int ft = 0; ft < nft; ++ft) total += (trange_host[ft].y - trange_host[ft].x + kKC - 1) / kKC;
+  // pieces: enough CTAs to fill the GPU a few times, each a multiple of the flush group
+  const long long want = std::max<long long>(1, (kTargetCtas + (long long)h.tiles.size() - 1) / h.tiles.size());
+  long long piece = std::max<long long>(kFlushChunks, (total + want - 1) / want);
+  piece = (piece + kFlushChunks - 1) / kFlushChunks * kFlushChunks;
   h.ft_items.resize(nft);
   for (int ft = 0; ft < nft; ++ft) {
     const int tb = trange_host[ft].x, te = trange_host[ft].y;
@@ -442,17 +465,12 @@ HostPlan make_plan(const ContractArgs& a, const int2* trange_host, int nft) {
     }
     const int c1 = (int)h.chunk_ft.size();
     const int i0 = (int)h.items.size();
-    for (int c = c0; c < c1; c += kPieceChunks) h.items.push_back(make_int4(ft, c, std::min(c1, c + kPieceChunks), 0));
+    for (int c = c0; c < c1; c += (int)piece) h.items.push_back(make_int4(ft, c, (int)std::min<long long>(c1, c + piece), 0));
     h.ft_items[ft] = make_int2(i0, (int)h.items.size());
   }
-  const int A = 3 * a.neps, nb = (A + 7) / 8;
-  for (int i = 0; i < nb; ++i)
-    for (int j = 0; j < nb; ++j) {
-      const int amax = std::min(8 * i + 7, A - 1), bmin = 8 * j;
-      if (amax / 3 >= bmin / 3) h.tiles.push_back(make_int2(i, j));
-    }
   return h;
 }
+
 }  // namespace
 
 size_t mixed_workspace_bytes(const ContractArgs& a, long long T) {
@@ -460,9 +478,9 @@ size_t mixed_workspace_bytes(const ContractArgs& a, long long T) {
   const int nft = (a.nf + kN - 1) / kN;
   const long long span = a.window < 0 ? nft : std::min<long long>(nft, (2LL * a.window + kN) / kN + 2);
   const long long nchunk = (T * span + kKC - 1) / kKC + nft + 1;
-  const long long nitem = nchunk / kPieceChunks + nft + 1;
   const int A = 3 * a.neps, nb = (A + 7) / 8;
   const long long ntile = (long long)nb * nb;
+  const long long nitem = kTargetCtas + 2 * nft + 1;  // pieces: want + one remainder per frequency tile
   size_t b = 0;
   b += align256(sizeof(int) * 3 * nchunk);
   b += align256(sizeof(int4) * nitem);
@@ -470,7 +488,7 @@ size_t mixed_workspace_bytes(const ContractArgs& a, long long T) {
   b += align256(sizeof(int2) * ntile);
   b += align256(sizeof(float) * (T + 1));
   b += align256((size_t)kWChunkBytes * nchunk);
-  b += align256(sizeof(float) * (size_t)nitem * ntile * kM * kN);
+  b += align256(sizeof(double) * (size_t)nitem * ntile * kM * kN);
   b += align256(sizeof(int) * 4);
   b += align256(sizeof(float2) * (size_t)(T + 1) * A * a.nch);
   return b;
@@ -479,6 +497,29 @@ size_t mixed_workspace_bytes(const ContractArgs& a, long long T) {
 size_t mixed_smem_bytes(int nch) {
   return (size_t)2 * (2 * kABytes + kWChunkBytes) + (size_t)kKC * 16 * nch * sizeof(float2) + kKC * sizeof(float) +
          4 * sizeof(uint64_t) + 4 * sizeof(int);
+}
+
+// Precision diagnostic of the FP32 overlap copies: max ||M32|^2 - |M|^2| and
+// max |M|^2 over all entries (non-negative doubles compare as integers).
+__global__ void m32_error_kernel(const double2* __restrict__ M, const float2* __restrict__ M32, size_t n,
+                                 unsigned long long* out) {
+  double e = 0.0, mx = 0.0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double2 v = M[i];
+    const float2 w = M32[i];
+    const double a = v.x * v.x + v.y * v.y;
+    const double b = (double)w.x * w.x + (double)w.y * w.y;
+    e = fmax(e, fabs(a - b));
+    mx = fmax(mx, a);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    e = fmax(e, __shfl_xor_sync(0xffffffffu, e, o));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&out[0], (unsigned long long)__double_as_longlong(e));
+    atomicMax(&out[1], (unsigned long long)__double_as_longlong(mx));
+  }
 }
 
 __global__ void m_to_f32_kernel(const double2* __restrict__ M, float2* __restrict__ M32, size_t n,
@@ -534,7 +575,7 @@ cudaError_t launch_contract_mixed(const ContractArgs& a, long long T, void* ws, 
   pl.tiles = reinterpret_cast<int2*>(take(sizeof(int2) * std::max(1, pl.ntile)));
   pl.wgt32 = reinterpret_cast<float*>(take(sizeof(float) * (T + 1)));
   pl.wbuf = take((size_t)kWChunkBytes * std::max(1, pl.nchunk));
-  pl.part = reinterpret_cast<float*>(take(sizeof(float) * (size_t)std::max(1, pl.nitem) * pl.ntile * kM * kN));
+  pl.part = reinterpret_cast<double*>(take(sizeof(double) * (size_t)std::max(1, pl.nitem) * pl.ntile * kM * kN));
   pl.err = reinterpret_cast<int*>(take(sizeof(int) * 4));
   float2* M32 = reinterpret_cast<float2*>(take(sizeof(float2) * (size_t)(T + 1) * A * a.nch));
   if ((size_t)(p - reinterpret_cast<uint8_t*>(ws)) > mixed_workspace_bytes(a, T)) return cudaErrorInvalidValue;
@@ -559,6 +600,13 @@ cudaError_t launch_contract_mixed(const ContractArgs& a, long long T, void* ws, 
   if (T > 0) {
     m_to_f32_kernel<<<1184, 256, 0, st>>>(a.M, M32, (size_t)T * A * a.nch, a.wgt, pl.wgt32, T);
     ++nlaunch;
+    if (a.stats) {
+      e = cudaMemsetAsync(a.stats, 0, 2 * sizeof(double), st);
+      if (e != cudaSuccess) return e;
+      m32_error_kernel<<<592, 256, 0, st>>>(a.M, M32, (size_t)T * A * a.nch,
+                                              reinterpret_cast<unsigned long long*>(a.stats));
+      ++nlaunch;
+    }
   }
   if (pl.nchunk > 0) {
     wgen_kernel<<<pl.nchunk, 256, 0, st>>>(pl, a);

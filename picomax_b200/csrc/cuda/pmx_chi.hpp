@@ -49,6 +49,7 @@ struct ContractArgs {
   double eps, dfreq;
   double* acc;          // [2][9][np][nf] Re then Im
   double* acc_pv;       // principal-value accumulators (epsLL, kk = 0) or null
+  double* stats;        // mixed path only, optional (device, 2 doubles): max ||M32|^2 - |M|^2|, max |M|^2
 };
 
 struct ScaleArgs {

@@ -250,7 +250,8 @@ struct pmx_ctx {
   // named workspaces
   DevBuf crystal, g, hkl, vloc, vso, items, hbuf, wbuf, zk, zq, scratch, info;
   DevBuf loci, kpts, uvec, ssoc, qgn, ncd, nvd, cbase, vbase, cidx, vidx, blkoff, dest;
-  DevBuf M, dE, wgt, f0, trange, acc, accpv, chi, chi2, mixws, epsm;
+  DevBuf M, dE, wgt, f0, trange, acc, accpv, chi, chi2, mixws, epsm, stats;
+  double m2_err = 0.0, m2_max = 0.0;  // |M|^2 error of the mixed path's FP32 overlaps (last call)
   cudaEvent_t ev[2] = {nullptr, nullptr};
 };
 
@@ -772,6 +773,7 @@ static int run_chi(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision, do
     const int nval = std::min(solved_states(p.nband + 1, dc.soc), dc.n);
     const int n = dc.n;
     ctx->degenerate_cuts = 0;
+    ctx->m2_err = ctx->m2_max = 0.0;
     const int nch = (mode == 0 && dc.soc) ? 4 : 1;
     CK(ctx->zk.ensure(std::max<size_t>(sizeof(double2) * (size_t)nk * nev * n, 16)));
     CK(ctx->zq.ensure(std::max<size_t>(sizeof(double2) * (size_t)nk * nev * n, 16)));
@@ -933,9 +935,18 @@ static int run_chi(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision, do
         } else {
           int nl = 0;
           CK(ctx->mixws.ensure(std::max<size_t>(pmx::dev::mixed_workspace_bytes(ca, (long long)T.T), 16)));
-          KTime kt(ctx, "contract_mixed");
-          CK(pmx::dev::launch_contract_mixed(ca, (long long)T.T, ctx->mixws.ptr, nl, st));
+          CK(ctx->stats.ensure(16));
+          ca.stats = ctx->stats.as<double>();
+          {
+            KTime kt(ctx, "contract_mixed");
+            CK(pmx::dev::launch_contract_mixed(ca, (long long)T.T, ctx->mixws.ptr, nl, st));
+          }
           ctx->launches += nl;
+          double sv[2] = {0, 0};
+          CK(cudaMemcpyAsync(sv, ctx->stats.ptr, sizeof(sv), cudaMemcpyDeviceToHost, st));
+          CK(cudaStreamSynchronize(st));
+          ctx->m2_err = std::max(ctx->m2_err, sv[0]);
+          ctx->m2_max = std::max(ctx->m2_max, sv[1]);
         }
       }
       // scaling and Kramers-Kronig
@@ -1019,6 +1030,13 @@ extern "C" int pmx_ctx_transfer_bytes(const pmx_ctx* c, long long* h2d_bytes, lo
 }
 
 extern "C" int pmx_ctx_degenerate_cuts(const pmx_ctx* c) { return c ? c->degenerate_cuts : -1; }
+
+extern "C" int pmx_ctx_overlap_error(const pmx_ctx* c, double* max_abs2_err, double* max_abs2) {
+  if (!c) return PMX_ERR_INVALID;
+  if (max_abs2_err) *max_abs2_err = c->m2_err;
+  if (max_abs2) *max_abs2 = c->m2_max;
+  return PMX_OK;
+}
 
 extern "C" int pmx_ctx_set_autotune(pmx_ctx* c, int on) {
   if (!c) return PMX_ERR_INVALID;

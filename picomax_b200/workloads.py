@@ -72,7 +72,12 @@ def te_form_factors(seed: int = 1968, f: float = 1.33):
 
 
 def workload(name: str, workdir: str):
-    """Returns (argv, nspectra, nsolves) of a named workload; k-files go to workdir."""
+    """Returns (argv, nspectra, nsolves) of a named workload; k-files go to workdir.
+
+    si_band / si_epsLL: config 1 (Si, 121-point path; 8^3 grid, NEPS 15, 1000 w)
+    gaas_epsij[_N]:     config 2 (GaAs + SOC, N^3 grid (16), NEPS 27, 2000 w, Lorentzian)
+    wz_epsLL:           config 3 (wurtzite, N_G 401, 24x24x16 grid, NEPS 59, 2000 w)
+    te_band / te_epsLL: config 5 (trigonal Te + SOC, 2 N_G = 570; 121-point path; 10x10x8 grid)"""
     os.makedirs(workdir, exist_ok=True)
     if name == "si_band":
         argv = ["-switch", "band", "-crystal", "zb", "-a", "5.43", "-vg", SI_VG, "-encut", "110",
@@ -99,16 +104,25 @@ def workload(name: str, workdir: str):
         kf = os.path.join(workdir, "k_wz_24_16.txt")
         nk = make_kfile(kf, "wz", 24, 24, 16, f=1.626)
         argv = ["-switch", "epsLL", "-crystal", "wz", "-a", "3.19", "-f", "1.626", "-u", "0.375",
-                "-vg", wz_form_factors(), "-encut", "200", "-kpoint", "0", "-kpointfile", kf,
+                "-vg", wz_form_factors(), "-encut", "260", "-kpoint", "0", "-kpointfile", kf,
                 "-qvec", "0.01,0,0", "-neps", "59", "-nband", "48", "-nvalence", "16", "-nfreq", "2000",
                 "-dfreq", "0.015", "-delta", "0", "-epsilon", "0.1", "-kk", "1"]
         return argv, 1, 1 + 2 * nk
     if name == "te_band":
         vg, soc = te_form_factors()
         argv = ["-switch", "band", "-crystal", "te", "-a", "4.45", "-f", "1.33", "-u", "0.264", "-vg", vg,
-                "-encut", "60", "-nband", "24", "-nvalence", "18", "-qpath", "G,A,H,K,G",
+                "-encut", "120", "-nband", "24", "-nvalence", "18", "-qpath", "G,A,H,K,G",
                 "-qnum", "30,30,30,30"] + soc
         return argv, 0, 122
+    if name == "te_epsLL":
+        vg, soc = te_form_factors()
+        kf = os.path.join(workdir, "k_te_10_8.txt")
+        nk = make_kfile(kf, "te", 10, 10, 8, f=1.33)
+        argv = ["-switch", "epsLL", "-crystal", "te", "-a", "4.45", "-f", "1.33", "-u", "0.264", "-vg", vg,
+                "-encut", "120", "-kpoint", "0", "-kpointfile", kf, "-qvec", "0.01,0,0", "-neps", "15",
+                "-nband", "24", "-nvalence", "18", "-nfreq", "1000", "-dfreq", "0.01", "-delta", "0",
+                "-epsilon", "0.05", "-kk", "1"] + soc
+        return argv, 1, 1 + 2 * nk
     raise KeyError(name)
 
 
