@@ -605,10 +605,16 @@ cudaError_t heev_launch_t(const EigItem* items, int nitems, size_t smem, double2
 }
 }  // namespace
 
-int heev_variants(int max_n) {
+int heev_variants(int max_n, int max_nev) {
   const int slots = (max_n + 31) / 32;
   if (max_n <= heev_smem_max_n()) return 1;  // shared-memory resident: one variant
-  return slots <= 13 ? 3 : 1;
+  if (slots > 13) return 1;
+  // the prefetch rings only count while their shared memory fits the opt-in limit
+  const int maxs = slots <= 2 ? 2 : slots <= 4 ? 4 : slots <= 6 ? 6 : slots <= 9 ? 9 : 13;
+  const size_t lim = 227 * 1024;
+  if (heev_smem_bytes(max_n, max_nev, false, maxs, 1) > lim) return 1;
+  if (heev_smem_bytes(max_n, max_nev, false, maxs, 3) > lim) return 2;
+  return 3;
 }
 
 cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev, double2* hbuf,

@@ -53,7 +53,7 @@ cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev
                         double* wbuf, double2* zbuf, double* scratch, int* info, cudaStream_t st, int variant = 0);
 int heev_smem_max_n();
 // Number of schedules launch_heev offers for matrices of size max_n.
-int heev_variants(int max_n);
+int heev_variants(int max_n, int max_nev);
 
 }  // namespace dev
 }  // namespace pmx

@@ -424,7 +424,7 @@ void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int 
     // last so the results come from it)
     const long long key = ((long long)n * 1024 + nval) * 2 + (vec ? 1 : 0);
     int variant = 0;
-    const int nvar = pmx::dev::heev_variants(n);
+    const int nvar = pmx::dev::heev_variants(n, nval);
     auto it_choice = c->heev_choice.find(key);
     if (it_choice != c->heev_choice.end()) {
       variant = it_choice->second;
