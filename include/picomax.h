@@ -27,7 +27,8 @@ typedef enum {
   PMX_ERR_NOCONV = 3,      /* eigensolver did not converge (reference: abort() at src/pmx_epm.cpp:233) */
   PMX_ERR_TIMEOUT = 4,     /* a bounded device wait ran out */
   PMX_ERR_NO_DEVICE = 5,   /* no CUDA device: this library has no CPU path */
-  PMX_ERR_UNSUPPORTED = 6  /* input outside what this build implements */
+  PMX_ERR_UNSUPPORTED = 6, /* input outside what this build implements */
+  PMX_ERR_LIMIT = 7        /* size beyond the fixed maximum of pmx_heev_batched_noalloc */
 } pmx_status;
 
 typedef enum { PMX_SWITCH_NONE = 0, PMX_SWITCH_BAND = 1, PMX_SWITCH_EPSIJ = 2, PMX_SWITCH_EPSLL = 3 } pmx_switch;
@@ -135,6 +136,25 @@ int pmx_hamiltonian(pmx_ctx* ctx, const pmx_problem* p, const double* kpts, int 
  * w [batch][nev]; z [batch][nev][n][2] or NULL. Replaces the
  * Eigen::SelfAdjointEigenSolver calls at src/pmx_epm.cpp:232 and :402. */
 int pmx_heev_batched(pmx_ctx* ctx, int n, int batch, const double* A, int nev, double* w, double* z);
+
+/* pmx_heev_batched's eigensolver on caller-owned DEVICE buffers; allocates
+ * nothing (no cudaMalloc/cudaFree, no allocating library routine), for callers
+ * whose device memory is reserved up front by their own pool, or whose
+ * latency path must not synchronise the device as cudaMalloc/cudaFree do.
+ * A [batch][n][n][2] column-major complex (lower triangle read, overwritten),
+ * w [batch][nev], z [batch][nev][n][2] or NULL, info [batch] (0 ok,
+ * 1 no convergence, 2 non-finite input): device pointers of the current
+ * device. Enqueued on `stream` (a cudaStream_t of the current device; NULL:
+ * legacy default stream); returns without waiting for the GPU.
+ * Scratch: one fixed 16 MiB device array inside the library (table of at most
+ * 1024 matrices, then 4 n nev doubles of inverse-iteration vectors per matrix
+ * when z is given). batch > 1024, n > 864, or 32 n nev batch bytes above
+ * 16 MiB - 80 KiB (with z) return PMX_ERR_LIMIT. The first call on a device
+ * looks the array up (set-up, once per device): make that first call before
+ * any stream capture. Every call on a device shares the array and rewrites
+ * what it reads; calls that overlap on the GPU (different streams or threads)
+ * race on it. No counterpart in the reference (added entry point). */
+int pmx_heev_batched_noalloc(void* stream, int n, int batch, double* A, int nev, double* w, double* z, int* info);
 
 /* Energy reference: midpoint of eigenvalues nvalence-1 and nvalence at
  * -refpoint (setRefEnergy, src/pmx_epm.cpp:393-428). */

@@ -24,6 +24,7 @@ PMX_ERR_NOCONV = 3
 PMX_ERR_TIMEOUT = 4
 PMX_ERR_NO_DEVICE = 5
 PMX_ERR_UNSUPPORTED = 6
+PMX_ERR_LIMIT = 7
 
 SWITCH_NONE, SWITCH_BAND, SWITCH_EPSIJ, SWITCH_EPSLL = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
@@ -38,6 +39,7 @@ EXPORTS = (
     "pmx_ctx_transfer_bytes", "pmx_ctx_degenerate_cuts", "pmx_chi_device", "pmx_chi_epsm",
     "pmx_eps_macroscopic", "pmx_ctx_kernel_time", "pmx_ctx_set_autotune", "pmx_ctx_tuning",
     "pmx_ctx_overlap_error",
+    "pmx_heev_batched_noalloc",
 )
 
 
@@ -100,6 +102,7 @@ def load() -> ctypes.CDLL:
         "pmx_ctx_kernel_time": (c_int, [c_void_p, c_char_p, dp, POINTER(c_longlong)]),
         "pmx_ctx_set_autotune": (c_int, [c_void_p, c_int]),
         "pmx_ctx_overlap_error": (c_int, [c_void_p, dp, dp]),
+        "pmx_heev_batched_noalloc": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
         "pmx_ctx_tuning": (c_int, [c_void_p, c_char_p, c_size_t, POINTER(c_size_t)]),
     }
     for name, (res, args) in sig.items():
