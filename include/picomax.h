@@ -195,6 +195,37 @@ int pmx_eps_macroscopic(pmx_ctx* ctx, int neps, int nq, int nfreq, const double*
  * w_f = dfreq f (kramerskronigtransform, src/pmx_chi.cpp:272-309). */
 int pmx_kk(pmx_ctx* ctx, int nrows, int nfreq, double dfreq, double* re, double* im);
 
+/* ---------------------------------------------------------------- adjoint
+ * The reference computes no gradients; these entry points differentiate its
+ * band (src/pmx_epm.cpp:56-253) and chi_LL -> eps_M (src/pmx_chi_copy.cpp:
+ * 320-676, include/matlab_wrapper/+picomax/+eps/macroscopic.m:13-29) stages
+ * with respect to the form factors and SOC parameters, in FP64. */
+
+/* The problem's parameters, in this order: vg[atom][shell] (Ry; the -vg
+ * values after the |G|^2 keys), lambda_S (the -uniform_us_so_val value when
+ * -use_uniform_us_so is given, else one value per -us_so key in ascending key
+ * order), then one lambda_A per -ua_so key (ascending; -ua_so_val_g0 is key 0).
+ * values may be NULL to query *count. */
+int pmx_problem_params(const pmx_problem* p, double* values, int* count);
+/* Replaces the parameters (same order and count) and rebuilds the form-factor
+ * tables; the G/k/q tables are unchanged. */
+int pmx_problem_set_params(pmx_problem* p, const double* values, int count);
+
+/* Vector-Jacobian product of pmx_band: dE [nq][nband] = dL/d eband,
+ * grad [count] = dL/dparams (Hellmann-Feynman, including the reference energy
+ * of setRefEnergy, src/pmx_epm.cpp:393-428). */
+int pmx_band_vjp(pmx_ctx* ctx, const pmx_problem* p, const double* dE, double* grad);
+
+/* Vector-Jacobian product of eps_M (epsLL, the (L, L) block of chi; NEPS <= 64):
+ * deps [nq][nfreq][2] = (dL/dRe eps_M, dL/dIm eps_M), grad [count] = dL/dparams.
+ * chi_re/chi_im: the re/im arrays of a FP64 pmx_chi(PMX_SWITCH_EPSLL) call on
+ * the same parameters (only their leading (L, L) block is read), or NULL to
+ * recompute them. Eigenpairs are recomputed per block of k-points (all
+ * eigenvectors of each H(k), for the eigenvector adjoint); eigenvalue pairs
+ * closer than 1e-8 eV are treated as degenerate and do not mix. */
+int pmx_epsm_vjp(pmx_ctx* ctx, const pmx_problem* p, const double* chi_re, const double* chi_im,
+                 const double* deps, double* grad);
+
 /* ---------------------------------------------------------------- driver */
 
 /* The whole picomax program: the reference main (src/pmx.cpp:43-206) plus

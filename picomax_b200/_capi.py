@@ -40,6 +40,10 @@ EXPORTS = (
     "pmx_eps_macroscopic", "pmx_ctx_kernel_time", "pmx_ctx_set_autotune", "pmx_ctx_tuning",
     "pmx_ctx_overlap_error",
     "pmx_heev_batched_noalloc",
+    "pmx_problem_params",
+    "pmx_problem_set_params",
+    "pmx_band_vjp",
+    "pmx_epsm_vjp",
 )
 
 
@@ -103,6 +107,10 @@ def load() -> ctypes.CDLL:
         "pmx_ctx_set_autotune": (c_int, [c_void_p, c_int]),
         "pmx_ctx_overlap_error": (c_int, [c_void_p, dp, dp]),
         "pmx_heev_batched_noalloc": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+        "pmx_problem_params": (c_int, [c_void_p, dp, ip]),
+        "pmx_problem_set_params": (c_int, [c_void_p, dp, c_int]),
+        "pmx_band_vjp": (c_int, [c_void_p, c_void_p, dp, dp]),
+        "pmx_epsm_vjp": (c_int, [c_void_p, c_void_p, dp, dp, dp, dp]),
         "pmx_ctx_tuning": (c_int, [c_void_p, c_char_p, c_size_t, POINTER(c_size_t)]),
     }
     for name, (res, args) in sig.items():
@@ -174,6 +182,20 @@ class Problem:
         if self.info.nq:
             self._lib.pmx_problem_qpoints(self.handle, _dptr(Q))
         return Q
+
+    def params(self) -> np.ndarray:
+        """Form factors and SOC parameters (Ry) in the order of pmx_problem_params."""
+        n = c_int()
+        self._lib.pmx_problem_params(self.handle, None, ctypes.byref(n))
+        v = np.zeros(n.value, np.float64)
+        self._lib.pmx_problem_params(self.handle, _dptr(v), ctypes.byref(n))
+        return v
+
+    def set_params(self, values):
+        v = np.ascontiguousarray(values, np.float64)
+        st = self._lib.pmx_problem_set_params(self.handle, _dptr(v), len(v))
+        if st != PMX_OK:
+            raise PicomaxError(st, "pmx_problem_set_params: wrong parameter count")
 
     def dump(self) -> str:
         need = c_size_t()
@@ -297,6 +319,28 @@ class Context:
         self._check(self._lib.pmx_chi_epsm(self.handle, prob.handle, switch, precision, _dptr(re), _dptr(im),
                                            _dptr(eps)), "chi_epsm")
         return re, im, eps[..., 0] + 1j * eps[..., 1]
+
+    def band_vjp(self, prob: Problem, dE) -> np.ndarray:
+        """dL/dparams from dL/d eband [nq][nband]."""
+        dE = np.ascontiguousarray(dE, np.float64).reshape(prob.info.nq, prob.info.nband)
+        g = np.zeros(len(prob.params()), np.float64)
+        self._check(self._lib.pmx_band_vjp(self.handle, prob.handle, _dptr(dE), _dptr(g)), "band_vjp")
+        return g
+
+    def epsm_vjp(self, prob: Problem, deps, chi=None) -> np.ndarray:
+        """dL/dparams from dL/d eps_M ([nq][nf] complex: dL/dRe + 1j dL/dIm);
+        chi = (re, im) of a FP64 epsLL chi call on the same parameters, or None."""
+        deps = np.asarray(deps, np.complex128).reshape(prob.info.nq, prob.info.nfreq)
+        d = np.ascontiguousarray(np.stack([deps.real, deps.imag], -1))
+        g = np.zeros(len(prob.params()), np.float64)
+        if chi is None:
+            st = self._lib.pmx_epsm_vjp(self.handle, prob.handle, None, None, _dptr(d), _dptr(g))
+        else:
+            re = np.ascontiguousarray(chi[0], np.float64)
+            im = np.ascontiguousarray(chi[1], np.float64)
+            st = self._lib.pmx_epsm_vjp(self.handle, prob.handle, _dptr(re), _dptr(im), _dptr(d), _dptr(g))
+        self._check(st, "epsm_vjp")
+        return g
 
     def chi_device(self, prob: Problem, switch: int, precision: int, re_ptr: int, im_ptr: int, epsm_ptr: int = 0):
         """pmx_chi_device on caller-owned device buffers (raw pointers, e.g. torch .data_ptr())."""

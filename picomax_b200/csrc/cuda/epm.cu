@@ -477,7 +477,33 @@ __global__ void __launch_bounds__(kHeevThreads, (RING >= 2 || MAXS > 9) ? 1 : 2)
   const int G = nev > 0 ? max(1, nthr / nev) : 1;
   __syncthreads();
   int converged = 0;
-  for (int iter = 0; iter < kBisectIters; ++iter) {
+  if (nev > nthr) {
+    // more eigenvalues than threads: plain bisection, each thread owns the
+    // eigenvalues tid, tid + nthr, ...
+    for (int iter = 0; iter < kBisectIters; ++iter) {
+      int done = 1;
+      for (int k = tid; k < nev; k += nthr) {
+        double l = lo[k], h = hi[k];
+        const double tol = 2.0 * DBL_EPSILON * fmax(fabs(l), fabs(h)) + 4.0 * pivmin;
+        if (h - l > tol) {
+          const double x = l + 0.5 * (h - l);
+          if (sturm_count(d, e2, n, x, pivmin) <= k)
+            l = x;
+          else
+            h = x;
+          lo[k] = l;
+          hi[k] = h;
+          done &= (h - l) <= tol ? 1 : 0;
+        }
+      }
+      done = __syncthreads_and(done);
+      if (done) {
+        converged = 1;
+        break;
+      }
+    }
+  }
+  for (int iter = 0; iter < kBisectIters && !converged && nev <= nthr; ++iter) {
     const int k = tid / G, g = tid % G;
     if (k < nev) {
       const double l = lo[k], h = hi[k];
@@ -585,6 +611,8 @@ __global__ void __launch_bounds__(kHeevThreads, (RING >= 2 || MAXS > 9) ? 1 : 2)
   if (tid == 0) info[blockIdx.x] = 0;
 }
 
+bool heev_resident(int n, int nev) { return heev_smem_bytes(n, nev, true) <= (size_t)227 * 1024; }
+
 int heev_smem_max_n() {
   // largest n whose resident (packed lower) layout fits the 227 KB opt-in limit
   const size_t lim = 227 * 1024;
@@ -607,7 +635,7 @@ cudaError_t heev_launch_t(const EigItem* items, int nitems, size_t smem, double2
 
 int heev_variants(int max_n, int max_nev) {
   const int slots = (max_n + 31) / 32;
-  if (max_n <= heev_smem_max_n()) return 1;  // shared-memory resident: one variant
+  if (max_n <= heev_smem_max_n() && heev_resident(max_n, max_nev)) return 1;  // resident: one variant
   if (slots > 13) return 1;
   // the prefetch rings only count while their shared memory fits the opt-in limit
   const int maxs = slots <= 2 ? 2 : slots <= 4 ? 4 : slots <= 6 ? 6 : slots <= 9 ? 9 : 13;
@@ -620,7 +648,7 @@ int heev_variants(int max_n, int max_nev) {
 cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev, double2* hbuf,
                         double* wbuf, double2* zbuf, double* scratch, int* info, cudaStream_t st, int variant) {
   if (nitems <= 0) return cudaSuccess;
-  const bool resident = max_n <= heev_smem_max_n();
+  const bool resident = max_n <= heev_smem_max_n() && heev_resident(max_n, max_nev);
   const int slots = (max_n + 31) / 32;
   // global-memory path variants: 0 = direct L2 loads (2 CTAs/SM), 1 = one-column
   // prefetch buffer per warp (2 CTAs/SM), 2 = three-column ring (1 CTA/SM)

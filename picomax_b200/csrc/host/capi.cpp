@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../../../include/picomax.h"
+#include "../cuda/pmx_adjoint.hpp"
 #include "../cuda/pmx_chi.hpp"
 #include "../cuda/pmx_device.hpp"
 #include "../cuda/pmx_mixed.hpp"
@@ -251,6 +252,9 @@ struct pmx_ctx {
   DevBuf crystal, g, hkl, vloc, vso, items, hbuf, wbuf, zk, zq, scratch, info;
   DevBuf loci, kpts, uvec, ssoc, qgn, ncd, nvd, cbase, vbase, cidx, vidx, blkoff, dest;
   DevBuf M, dE, wgt, f0, trange, acc, accpv, chi, chi2, mixws, epsm, stats;
+  // adjoint workspaces
+  DevBuf a_chi, a_g, a_gx, a_kk, a_f1, a_f2, a_obar, a_debar, a_mbar, a_zbk, a_zbq, a_lbk, a_lbq;
+  DevBuf a_lamk, a_lamq, a_C, a_X, a_R, a_SV, a_SSO, a_kp, a_linv;
   double m2_err = 0.0, m2_max = 0.0;  // |M|^2 error of the mixed path's FP32 overlaps (last call)
   cudaEvent_t ev[2] = {nullptr, nullptr};
 };
@@ -386,7 +390,7 @@ void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int 
   const int nk = (int)ks.size(), n = dc.n;
   w.assign((size_t)nk * nval, 0.0);
   if (nk == 0) return;
-  if (nval > 512 || nval > n) throw CudaFail("too many eigenvalues requested", PMX_ERR_INVALID);
+  if (nval > n) throw CudaFail("too many eigenvalues requested", PMX_ERR_INVALID);
   const bool vec = zdev != nullptr && nvec > 0;
   const size_t hbytes = (size_t)n * n * sizeof(double2);
   int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)nk, ((size_t)2 << 30) / hbytes));
@@ -562,8 +566,7 @@ extern "C" int pmx_hamiltonian(pmx_ctx* ctx, const pmx_problem* P, const double*
 }
 
 extern "C" int pmx_heev_batched(pmx_ctx* ctx, int n, int batch, const double* A, int nev, double* w, double* z) {
-  if (n <= 0 || batch < 0 || nev <= 0 || nev > n || nev > 512 || (batch > 0 && (!A || !w)))
-    return PMX_ERR_INVALID;
+  if (n <= 0 || batch < 0 || nev <= 0 || nev > n || (batch > 0 && (!A || !w))) return PMX_ERR_INVALID;
   return guarded(ctx, [&]() {
     const size_t hb = sizeof(double2) * (size_t)n * n;
     CK(ctx->hbuf.ensure(std::max<size_t>(hb * batch, 16)));
@@ -652,10 +655,14 @@ struct Transitions {
 // E - E_ref > 0, valence states up from the bottom while E - E_ref <= 0.
 // wk/wq hold nval eigenvalues per k (spatial states without SOC). `cuts`
 // counts k and k+q points where state NBAND-1 and NBAND are degenerate.
+// k0/k1 restrict the list to k-points [k0, k1) (wk/wq and the per-k arrays
+// then count from k0).
 Transitions build_transitions(const Problem& p, int soc, int nval, const std::vector<double>& wk,
-                              const std::vector<double>& wq, double off, bool sort_by_window, int& cuts) {
+                              const std::vector<double>& wq, double off, bool sort_by_window, int& cuts,
+                              int k0 = 0, int k1 = -1) {
   Transitions T;
-  const int nk = p.nk(), NB = p.nband;
+  if (k1 < 0) k1 = p.nk();
+  const int nk = k1 - k0, NB = p.nband;
   T.ncd.resize(nk);
   T.nvd.resize(nk);
   T.cbase.resize(nk);
@@ -671,6 +678,7 @@ Transitions build_transitions(const Problem& p, int soc, int nval, const std::ve
   const double df = p.dfreq, w0 = p.freq.empty() ? 0.0 : p.freq[0];
   const int nh = 2 * p.npw();
   for (int k = 0; k < nk; ++k) {
+    const int kg = k0 + k;  // global k index
     if (NB < nh) {
       const bool cut_k = std::abs(spinor_eig(wk, nval, k, NB, soc) - spinor_eig(wk, nval, k, NB - 1, soc)) < 1e-8;
       const bool cut_q = std::abs(spinor_eig(wq, nval, k, NB, soc) - spinor_eig(wq, nval, k, NB - 1, soc)) < 1e-8;
@@ -715,7 +723,7 @@ Transitions build_transitions(const Problem& p, int soc, int nval, const std::ve
         const double ec = spinor_eig(wk, nval, k, s_c, soc) - off;
         const double ev = spinor_eig(wq, nval, k, s_v, soc) - off;
         const double de = ec - ev;
-        raw.push_back({src, de, p.KW[k] * mult, (int)((de - w0) / df)});
+        raw.push_back({src, de, p.KW[kg] * mult, (int)((de - w0) / df)});
       }
     blk += (long long)cs.size() * vs.size();
   }
@@ -1107,6 +1115,520 @@ extern "C" int pmx_kk(pmx_ctx* ctx, int nrows, int nfreq, double dfreq, double* 
     CK(cudaMemcpyAsync(re, ctx->chi2.ptr, sizeof(double) * blk, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(im, ctx->chi2.as<double>() + blk, sizeof(double) * blk, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    return (int)PMX_OK;
+  });
+}
+
+// ======================================================================= adjoint
+// Parameters of a problem, in this order: vg[atom][shell] (Ry, the -vg
+// values after the g2 keys), then lambda_S (the -uniform_us_so_val value
+// when -use_uniform_us_so is set, else one value per -us_so key, keys
+// ascending), then one lambda_A per -ua_so key (ascending; -ua_so_val_g0 is
+// key 0). H(k) is affine in all of them (src/pmx_epm.cpp:56-203).
+namespace {
+
+bool has_soc_params(const pmx_problem* P) {
+  const pmx::Material& m = P->p.mat;
+  return m.use_uniform_us || !m.Us.empty() || !m.Ua.empty();
+}
+
+std::vector<double> param_vector(const Problem& p) {
+  std::vector<double> v;
+  for (int a = 0; a < p.natom; ++a)
+    for (int s = 0; s < p.mat.NV; ++s) v.push_back(p.mat.vg[a][s]);
+  if (p.mat.use_uniform_us)
+    v.push_back(p.mat.uniform_us);
+  else
+    for (auto& kv : p.mat.Us) v.push_back(kv.second);
+  for (auto& kv : p.mat.Ua) v.push_back(kv.second);
+  return v;
+}
+
+// Index (in ascending key order) of the map entry get_soc_form_factor
+// (src/pmx_epm.cpp:22-50) returns for q2, or -1 when it returns 0.
+int soc_key_index(const std::map<double, double>& m, double q2) {
+  const double tol = 1e-2;
+  if (std::abs(q2) < tol) {
+    int i = 0;
+    for (auto& kv : m) {
+      if (kv.first == 0.0) return i;
+      ++i;
+    }
+    return -1;
+  }
+  int best_i = -1, i = 0;
+  double best = std::numeric_limits<double>::max();
+  for (auto& kv : m) {
+    const double d = std::abs(q2 - kv.first);
+    if (d < best) {
+      best = d;
+      best_i = i;
+    }
+    ++i;
+  }
+  return best < tol ? best_i : -1;
+}
+
+// Parameter gradient from the hkl-difference accumulators: SV[d] = sum over
+// ordered pairs (i != j) with hkl_i - hkl_j = d of the spin trace of
+// conj(dL/dH), SSO[d'] = the same contracted with i (k+G_j)x(k+G_i).sigma,
+// d' = hkl_j - hkl_i. dL/dp = Re sum_d SV[d] dV(d)/dp + Re sum_d SSO[d] dVSO(d)/dp.
+void tables_to_grad(const Problem& p, const std::vector<double2>& SV, const std::vector<double2>& SSO,
+                    bool soc, double* grad) {
+  const int side = 4 * p.imax + 1, off = 2 * p.imax;
+  const pmx::Material& mat = p.mat;
+  const int nvg = p.natom * mat.NV;
+  const int nls = mat.use_uniform_us ? 1 : (int)mat.Us.size();
+  std::vector<double> g(nvg + nls + mat.Ua.size(), 0.0);
+  const Vec3 b1 = p.lat.reciprocal[0], b2 = p.lat.reciprocal[1];
+  const Vec3 b3 = p.lat.dim == 3 ? p.lat.reciprocal[2] : Vec3{0, 0, 0};
+  for (int h = -off; h <= off; ++h)
+    for (int k = -off; k <= off; ++k)
+      for (int l = -off; l <= off; ++l) {
+        if (p.lat.dim == 2 && l != 0) continue;
+        if (!h && !k && !l) continue;
+        const size_t idx = ((size_t)(h + off) * side + (k + off)) * side + (l + off);
+        const Vec3 dG = (double(h) * b1 + double(k) * b2) + double(l) * b3;
+        const double g2 = pmx::sqnorm(dG);
+        const std::complex<double> sv(SV[idx].x, SV[idx].y);
+        if (sv != 0.0 && g2 < mat.g2max) {
+          int shell = -1;
+          for (int s = 0; s < mat.NV; ++s)
+            if (std::abs(mat.g2[s] - g2) < 1e-2) {
+              shell = s;
+              break;
+            }
+          if (shell >= 0 && p.natom > 0)
+            for (int a = 0; a < p.natom; ++a) {
+              const double ph = (-2.0 * pmx::kPi) * pmx::dot(dG, p.lat.atomic[a]);
+              const std::complex<double> c(std::cos(ph), std::sin(ph));
+              g[a * mat.NV + shell] += (sv * c).real() * pmx::kRy2eV / double(p.natom);
+            }
+        }
+        if (!soc) continue;
+        const std::complex<double> so(SSO[idx].x, SSO[idx].y);
+        if (so == 0.0 || p.natom <= 0) continue;
+        double cs = 0, sn = 0;
+        for (const Vec3& t : p.lat.atomic) {
+          cs += std::cos(2.0 * pmx::kPi * pmx::dot(dG, t));
+          sn += std::sin(2.0 * pmx::kPi * pmx::dot(dG, t));
+        }
+        cs /= p.natom;
+        sn /= p.natom;
+        const int ils = mat.use_uniform_us ? 0 : soc_key_index(mat.Us, g2);
+        if (ils >= 0) g[nvg + ils] += (so * (pmx::kRy2eV * cs)).real();
+        const int ila = soc_key_index(mat.Ua, g2);
+        if (ila >= 0) g[nvg + nls + ila] += (so * std::complex<double>(0.0, pmx::kRy2eV * sn)).real();
+      }
+  std::copy(g.begin(), g.end(), grad);
+}
+
+// Accumulates X Z^H of a batch of items into the pair accumulators.
+void hgrad_items(pmx_ctx* c, const DevCrystal& dc, const double2* X, long long xs, const double2* Z, long long zs,
+                 const std::vector<Vec3>& ks, int ns) {
+  const int nb = (int)ks.size();
+  if (nb == 0) return;
+  std::vector<double> kp(3 * (size_t)nb);
+  for (int b = 0; b < nb; ++b)
+    for (int x = 0; x < 3; ++x) kp[3 * b + x] = ks[b][x];
+  h2d(c, c->a_kp, kp.data(), sizeof(double) * kp.size());
+  KTime kt(c, "adj_hgrad");
+  CK(pmx::dev::launch_hgrad(X, xs, Z, zs, c->a_kp.as<double>(), nb, dc.n, dc.npw, dc.soc, ns, c->a_R.as<double2>(),
+                            c->stream));
+  c->launches += 1;
+  // the k table is reused by the next call: keep the launches ordered
+  CK(cudaStreamSynchronize(c->stream));
+}
+
+void adj_begin(pmx_ctx* c, const pmx_problem* P, const DevCrystal& dc) {
+  const size_t pl = (size_t)dc.npw * dc.npw * (dc.soc ? 16 : 1);
+  CK(c->a_R.ensure(sizeof(double2) * std::max<size_t>(pl, 1)));
+  CK(cudaMemsetAsync(c->a_R.ptr, 0, sizeof(double2) * pl, c->stream));
+  const int side = 4 * P->p.imax + 1;
+  const size_t n3 = (size_t)side * side * side;
+  CK(c->a_SV.ensure(sizeof(double2) * n3));
+  CK(c->a_SSO.ensure(sizeof(double2) * n3));
+  CK(cudaMemsetAsync(c->a_SV.ptr, 0, sizeof(double2) * n3, c->stream));
+  CK(cudaMemsetAsync(c->a_SSO.ptr, 0, sizeof(double2) * n3, c->stream));
+}
+
+void adj_finish(pmx_ctx* c, const pmx_problem* P, const DevCrystal& dc, double* grad) {
+  const int side = 4 * P->p.imax + 1;
+  const size_t n3 = (size_t)side * side * side;
+  {
+    KTime kt(c, "adj_hscatter");
+    CK(pmx::dev::launch_hscatter(c->a_R.as<double2>(), dc.npw, dc.soc, c->hkl.as<int>(), c->g.as<double>(),
+                                 P->p.imax, c->a_SV.as<double2>(), c->a_SSO.as<double2>(), c->stream));
+  }
+  c->launches += 1;
+  std::vector<double2> SV(n3), SSO(n3);
+  CK(cudaMemcpyAsync(SV.data(), c->a_SV.ptr, sizeof(double2) * n3, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(SSO.data(), c->a_SSO.ptr, sizeof(double2) * n3, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->d2h += (long long)(2 * sizeof(double2) * n3);
+  tables_to_grad(P->p, SV, SSO, dc.soc != 0, grad);
+}
+
+// Hellmann-Feynman term of the items' eigenvalues: lbar [nb][ns] on the host.
+void hf_items(pmx_ctx* c, const DevCrystal& dc, const double2* Z, long long zs, const std::vector<double>& lbar,
+              const std::vector<Vec3>& ks, int ns) {
+  const int nb = (int)ks.size();
+  if (nb == 0) return;
+  h2d(c, c->a_lbk, lbar.data(), sizeof(double) * lbar.size());
+  CK(c->a_X.ensure(sizeof(double2) * (size_t)nb * ns * dc.n));
+  CK(pmx::dev::launch_hf_x(Z, zs, c->a_lbk.as<double>(), dc.n, ns, nb, c->a_X.as<double2>(), c->stream));
+  c->launches += 1;
+  hgrad_items(c, dc, c->a_X.as<double2>(), (long long)ns * dc.n, Z, zs, ks, ns);
+}
+
+// Gradient of the reference energy (E_{nv-1} + E_nv)/2 scaled by obar.
+void ref_energy_grad(pmx_ctx* c, const pmx_problem* P, const DevCrystal& dc, double obar) {
+  const Problem& p = P->p;
+  const int nh = 2 * p.npw();
+  if (!(p.nvalence > 0 && p.nvalence < nh) || obar == 0.0) return;
+  const int ns = solved_states(p.nvalence + 1, dc.soc);
+  std::vector<double> w;
+  CK(c->zk.ensure(sizeof(double2) * (size_t)ns * dc.n));
+  solve_k(c, dc, {p.refpoint}, ns, ns, c->zk.as<double2>(), w);
+  std::vector<double> lb(ns, 0.0);
+  const int s1 = dc.soc ? p.nvalence - 1 : (p.nvalence - 1) / 2, s2 = dc.soc ? p.nvalence : p.nvalence / 2;
+  lb[s1] += 0.5 * obar;
+  lb[s2] += 0.5 * obar;
+  hf_items(c, dc, c->zk.as<double2>(), (long long)ns * dc.n, lb, {p.refpoint}, ns);
+}
+
+}  // namespace
+
+extern "C" int pmx_problem_params(const pmx_problem* P, double* values, int* count) {
+  if (!P || !count) return PMX_ERR_INVALID;
+  const std::vector<double> v = param_vector(P->p);
+  if (values) std::copy(v.begin(), v.end(), values);
+  *count = (int)v.size();
+  return PMX_OK;
+}
+
+extern "C" int pmx_problem_set_params(pmx_problem* P, const double* values, int count) {
+  if (!P || (!values && count > 0)) return PMX_ERR_INVALID;
+  Problem& p = P->p;
+  if (count != (int)param_vector(p).size()) return PMX_ERR_INVALID;
+  int i = 0;
+  for (int a = 0; a < p.natom; ++a)
+    for (int s = 0; s < p.mat.NV; ++s) p.mat.vg[a][s] = values[i++];
+  if (p.mat.use_uniform_us)
+    p.mat.uniform_us = values[i++];
+  else
+    for (auto& kv : p.mat.Us) kv.second = values[i++];
+  for (auto& kv : p.mat.Ua) kv.second = values[i++];
+  build_tables(*P);
+  return PMX_OK;
+}
+
+extern "C" int pmx_band_vjp(pmx_ctx* ctx, const pmx_problem* P, const double* dE, double* grad) {
+  if (!P || !grad || (!dE && P->p.nq() > 0)) return PMX_ERR_INVALID;
+  return guarded(ctx, [&]() {
+    const Problem& p = P->p;
+    DevCrystal dc = upload_crystal(ctx, P, has_soc_params(P) ? 1 : 0);
+    adj_begin(ctx, P, dc);
+    const int nh = 2 * p.npw(), nq = p.nq();
+    const int nkeep = std::min(p.nband, nh);
+    double osum = 0.0;
+    if (nkeep > 0 && nq > 0) {
+      const int ns = solved_states(nkeep, dc.soc), n = dc.n;
+      const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)nq, ((size_t)1 << 30) / ((size_t)ns * n * 16)));
+      CK(ctx->zq.ensure(sizeof(double2) * (size_t)chunk * ns * n));
+      for (int q0 = 0; q0 < nq; q0 += chunk) {
+        const int cnt = std::min(chunk, nq - q0);
+        std::vector<Vec3> ks(p.lat.Q.begin() + q0, p.lat.Q.begin() + q0 + cnt);
+        std::vector<double> w;
+        solve_k(ctx, dc, ks, ns, ns, ctx->zq.as<double2>(), w);
+        std::vector<double> lb((size_t)cnt * ns, 0.0);
+        for (int q = 0; q < cnt; ++q)
+          for (int s = 0; s < nkeep; ++s) {
+            const double g = dE[(size_t)(q0 + q) * p.nband + s];
+            lb[(size_t)q * ns + (dc.soc ? s : s / 2)] += g;
+            osum += g;
+          }
+        hf_items(ctx, dc, ctx->zq.as<double2>(), (long long)ns * n, lb, ks, ns);
+      }
+    }
+    ref_energy_grad(ctx, P, dc, -osum);
+    adj_finish(ctx, P, dc, grad);
+    return (int)PMX_OK;
+  });
+}
+
+extern "C" int pmx_epsm_vjp(pmx_ctx* ctx, const pmx_problem* P, const double* chi_re, const double* chi_im,
+                            const double* deps, double* grad) {
+  if (!P || !grad || !deps) return PMX_ERR_INVALID;
+  const Problem& p = P->p;
+  if (p.neps < 1 || p.neps > 64) return PMX_ERR_INVALID;
+  std::vector<double> fre, fim;
+  if (!chi_re || !chi_im) {
+    // forward chi_LL (FP64) first
+    const size_t vals = (size_t)9 * p.nq() * (p.neps * (p.neps + 1) / 2) * std::max(p.nfreq, 0);
+    fre.assign(vals, 0.0);
+    fim.assign(vals, 0.0);
+    const int rc = run_chi(ctx, P, PMX_SWITCH_EPSLL, PMX_PREC_FP64, fre.data(), fim.data(), false, nullptr);
+    if (rc != PMX_OK) return rc;
+    chi_re = fre.data();
+    chi_im = fim.data();
+  }
+  return guarded(ctx, [&]() -> int {
+    cudaStream_t st = ctx->stream;
+    for (double& t : ctx->stage_ms) t = 0;
+    const int nk = p.nk(), nq = p.nq(), neps = p.neps, nf = p.nfreq;
+    const int np = neps * (neps + 1) / 2;
+    if (!p.have_freq || nf <= 0 || !(p.dfreq > 0)) throw std::runtime_error("-nfreq and -dfreq are required");
+    if (p.nband <= 0 || p.nband > 2 * p.npw()) throw std::runtime_error("-nband out of range");
+    const size_t llv = (size_t)nq * np * nf;
+    // eps_M -> chi_LL
+    CK(ctx->a_chi.ensure(sizeof(double) * 2 * std::max<size_t>(llv, 1)));
+    CK(cudaMemcpyAsync(ctx->a_chi.ptr, chi_re, sizeof(double) * llv, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->a_chi.as<double>() + llv, chi_im, sizeof(double) * llv, cudaMemcpyHostToDevice, st));
+    ctx->h2d += (long long)(2 * sizeof(double) * llv);
+    h2d(ctx, ctx->a_g, deps, sizeof(double) * 2 * (size_t)nq * nf);
+    CK(ctx->a_gx.ensure(sizeof(double) * 2 * std::max<size_t>(llv, 1)));
+    {
+      KTime kt(ctx, "adj_epsm");
+      CK(pmx::dev::launch_epsm_vjp(ctx->a_chi.as<double>(), ctx->a_chi.as<double>() + llv, ctx->a_g.as<double2>(),
+                                   neps, nq, nf, ctx->a_gx.as<double>(), ctx->a_gx.as<double>() + llv, st));
+    }
+    ctx->launches += 1;
+    DevCrystal dc;
+    double off;
+    {
+      Timer tm(ctx, 0);
+      dc = upload_crystal(ctx, P, has_soc_params(P) ? 1 : 0);
+      off = ref_energy(ctx, P, dc);
+    }
+    adj_begin(ctx, P, dc);
+    const int n = dc.n, nall = n, npw = dc.npw;
+    const int ns = solved_states(p.nband, dc.soc);
+    h2d(ctx, ctx->loci, p.loci.data(), sizeof(int) * p.loci.size());
+    std::vector<int> linv((size_t)neps * npw, -1);
+    for (int m = 0; m < neps; ++m)
+      for (int q = 0; q < npw; ++q) {
+        const int r = p.loci[(size_t)m * npw + q];
+        if (r >= 0) linv[(size_t)m * npw + r] = q;
+      }
+    h2d(ctx, ctx->a_linv, linv.data(), sizeof(int) * linv.size());
+    const double a_cm = p.lat.a * pmx::kAngstrom, bz = p.lat.bz_volume;
+    const double sf_ll = 2.0 * bz * std::pow(pmx::kE, 2) / (pmx::kPi * pmx::kEV * a_cm);
+    const int kb = (int)std::max<size_t>(1, std::min<size_t>((size_t)nk, ((size_t)1 << 30) / ((size_t)n * n * 16)));
+    CK(ctx->zk.ensure(sizeof(double2) * (size_t)kb * nall * n));
+    CK(ctx->zq.ensure(sizeof(double2) * (size_t)kb * nall * n));
+    CK(ctx->a_kk.ensure(sizeof(double) * 2 * (size_t)np * nf));
+    CK(ctx->chi2.ensure(sizeof(double) * 2 * (size_t)np * nf));
+    const double tau = 1e-8;  // eV: eigenvalue pairs closer than this are treated as degenerate
+
+    for (int q = 0; q < nq; ++q) {
+      const Vec3 Q = p.lat.Q[q];
+      // upstream of this q on [2][np][nf]: KK transpose, then the scale factors
+      const size_t rowv = (size_t)np * nf;
+      CK(cudaMemcpyAsync(ctx->chi2.ptr, ctx->a_gx.as<double>() + (size_t)q * rowv, sizeof(double) * rowv,
+                         cudaMemcpyDeviceToDevice, st));
+      CK(cudaMemcpyAsync(ctx->chi2.as<double>() + rowv, ctx->a_gx.as<double>() + llv + (size_t)q * rowv,
+                         sizeof(double) * rowv, cudaMemcpyDeviceToDevice, st));
+      if (p.kk) {
+        KTime kt(ctx, "adj_kk");
+        CK(pmx::dev::launch_kk_t(ctx->chi2.as<double>(), ctx->a_kk.as<double>(), np, nf, p.dfreq, st));
+        ctx->launches += 1;
+      } else {
+        CK(cudaMemcpyAsync(ctx->a_kk.ptr, ctx->chi2.ptr, sizeof(double) * 2 * rowv, cudaMemcpyDeviceToDevice, st));
+      }
+      std::vector<double> f1(np), f2(np);
+      {
+        std::vector<double> qg(neps);
+        for (int m = 0; m < neps; ++m) qg[m] = pmx::norm(Q + p.G[m]);
+        for (int m = 0, pp = 0; m < neps; ++m)
+          for (int nn = 0; nn <= m; ++nn, ++pp) {
+            f1[pp] = pmx::kPi * (sf_ll / (qg[m] * qg[nn]));
+            f2[pp] = 2.0 * (sf_ll / (qg[m] * qg[nn]));
+          }
+      }
+      h2d(ctx, ctx->a_f1, f1.data(), sizeof(double) * np);
+      h2d(ctx, ctx->a_f2, f2.data(), sizeof(double) * np);
+
+      for (int k0 = 0; k0 < nk; k0 += kb) {
+        const int k1 = std::min(nk, k0 + kb), cnt = k1 - k0;
+        std::vector<Vec3> ks(p.K.begin() + k0, p.K.begin() + k1), kqs(cnt);
+        for (int i = 0; i < cnt; ++i) kqs[i] = ks[i] + Q;
+        std::vector<double> wk, wq;
+        {
+          Timer tm(ctx, 0);
+          solve_k(ctx, dc, ks, nall, nall, ctx->zk.as<double2>(), wk);
+          solve_k(ctx, dc, kqs, nall, nall, ctx->zq.as<double2>(), wq);
+        }
+        int cuts = 0;
+        Transitions T = build_transitions(p, dc.soc, nall, wk, wq, off, false, cuts, k0, k1);
+        std::vector<double> kp(3 * (size_t)cnt);
+        for (int i = 0; i < cnt; ++i)
+          for (int x = 0; x < 3; ++x) kp[3 * i + x] = ks[i][x];
+        h2d(ctx, ctx->kpts, kp.data(), sizeof(double) * kp.size());
+        h2d(ctx, ctx->ncd, T.ncd.data(), sizeof(int) * T.ncd.size());
+        h2d(ctx, ctx->nvd, T.nvd.data(), sizeof(int) * T.nvd.size());
+        h2d(ctx, ctx->cbase, T.cbase.data(), sizeof(int) * T.cbase.size());
+        h2d(ctx, ctx->vbase, T.vbase.data(), sizeof(int) * T.vbase.size());
+        h2d(ctx, ctx->cidx, T.cidx.data(), sizeof(int) * T.cidx.size());
+        h2d(ctx, ctx->vidx, T.vidx.data(), sizeof(int) * T.vidx.size());
+        h2d(ctx, ctx->blkoff, T.blkoff.data(), sizeof(long long) * T.blkoff.size());
+        h2d(ctx, ctx->dest, T.dest.data(), sizeof(long long) * T.dest.size());
+        h2d(ctx, ctx->dE, T.dE.data(), sizeof(double) * T.dE.size());
+        h2d(ctx, ctx->wgt, T.wgt.data(), sizeof(double) * T.wgt.size());
+        const int ncd_max = T.ncd.empty() ? 0 : *std::max_element(T.ncd.begin(), T.ncd.end());
+        const int nvd_max = T.nvd.empty() ? 0 : *std::max_element(T.nvd.begin(), T.nvd.end());
+        CK(ctx->a_zbk.ensure(sizeof(double2) * (size_t)cnt * ns * n));
+        CK(ctx->a_zbq.ensure(sizeof(double2) * (size_t)cnt * ns * n));
+        CK(cudaMemsetAsync(ctx->a_zbk.ptr, 0, sizeof(double2) * (size_t)cnt * ns * n, st));
+        CK(cudaMemsetAsync(ctx->a_zbq.ptr, 0, sizeof(double2) * (size_t)cnt * ns * n, st));
+        CK(ctx->a_lbk.ensure(sizeof(double) * (size_t)cnt * ns));
+        CK(ctx->a_lbq.ensure(sizeof(double) * (size_t)cnt * ns));
+        CK(cudaMemsetAsync(ctx->a_lbk.ptr, 0, sizeof(double) * (size_t)cnt * ns, st));
+        CK(cudaMemsetAsync(ctx->a_lbq.ptr, 0, sizeof(double) * (size_t)cnt * ns, st));
+        if (T.T > 0) {
+          const int A = 3 * neps;
+          CK(ctx->M.ensure(sizeof(double2) * (size_t)T.T * A));
+          {
+            Timer tm(ctx, 1);
+            pmx::dev::OverlapArgs oa{};
+            oa.n = n;
+            oa.npw = npw;
+            oa.soc = dc.soc;
+            oa.nev = nall;
+            oa.neps = neps;
+            oa.nch = 1;
+            oa.mode = 1;
+            oa.ncd_max = ncd_max;
+            oa.nvd_max = nvd_max;
+            int cchunk = std::max(1, ncd_max);
+            while (cchunk > 1 && pmx::dev::overlap_smem_bytes(cchunk, nvd_max, n, npw) > 200 * 1024) --cchunk;
+            if (pmx::dev::overlap_smem_bytes(cchunk, nvd_max, n, npw) > 220 * 1024)
+              throw CudaFail("overlap tile does not fit in shared memory", PMX_ERR_UNSUPPORTED);
+            oa.cchunk = cchunk;
+            oa.zk = ctx->zk.as<double2>();
+            oa.zq = ctx->zq.as<double2>();
+            oa.ncd = ctx->ncd.as<int>();
+            oa.nvd = ctx->nvd.as<int>();
+            oa.cbase = ctx->cbase.as<int>();
+            oa.vbase = ctx->vbase.as<int>();
+            oa.cidx = ctx->cidx.as<int>();
+            oa.vidx = ctx->vidx.as<int>();
+            oa.blkoff = ctx->blkoff.as<long long>();
+            oa.dest = ctx->dest.as<long long>();
+            oa.loci = ctx->loci.as<int>();
+            oa.G = ctx->g.as<double>();
+            oa.kpts = ctx->kpts.as<double>();
+            oa.q[0] = Q.x;
+            oa.q[1] = Q.y;
+            oa.q[2] = Q.z;
+            // the L row does not use the polarisation or SOC-current tables
+            oa.uvec = nullptr;
+            oa.ssoc = nullptr;
+            oa.M = ctx->M.as<double2>();
+            CK(ctx->uvec.ensure(sizeof(double2) * 9 * neps));
+            CK(ctx->ssoc.ensure(sizeof(double2) * 3 * neps));
+            CK(cudaMemsetAsync(ctx->uvec.ptr, 0, sizeof(double2) * 9 * neps, st));
+            CK(cudaMemsetAsync(ctx->ssoc.ptr, 0, sizeof(double2) * 3 * neps, st));
+            oa.uvec = ctx->uvec.as<double2>();
+            oa.ssoc = ctx->ssoc.as<double2>();
+            KTime kt(ctx, "overlap");
+            CK(pmx::dev::launch_overlap(oa, cnt, st));
+            ctx->launches += 1;
+          }
+          Timer tm(ctx, 2);
+          CK(ctx->a_obar.ensure(sizeof(double2) * (size_t)T.T * np));
+          CK(ctx->a_debar.ensure(sizeof(double) * (size_t)T.T));
+          CK(cudaMemsetAsync(ctx->a_debar.ptr, 0, sizeof(double) * (size_t)T.T, st));
+          pmx::dev::ContractVjpArgs ca{};
+          ca.M = ctx->M.as<double2>();
+          ca.dE = ctx->dE.as<double>();
+          ca.wgt = ctx->wgt.as<double>();
+          ca.T = (int)T.T;
+          ca.neps = neps;
+          ca.np = np;
+          ca.nf = nf;
+          ca.delta = p.delta;
+          ca.eps = p.epsilon;
+          ca.dfreq = p.dfreq;
+          ca.gre = ctx->a_kk.as<double>();
+          ca.gim = ctx->a_kk.as<double>() + rowv;
+          ca.f1 = ctx->a_f1.as<double>();
+          ca.f2 = p.kk ? nullptr : ctx->a_f2.as<double>();
+          ca.obar = ctx->a_obar.as<double2>();
+          ca.dEbar = ctx->a_debar.as<double>();
+          {
+            KTime kt(ctx, "adj_contract");
+            CK(pmx::dev::launch_contract_vjp(ca, st));
+          }
+          CK(ctx->a_mbar.ensure(sizeof(double2) * (size_t)T.T * neps));
+          {
+            KTime kt(ctx, "adj_mbar");
+            CK(pmx::dev::launch_mbar(ctx->M.as<double2>(), ctx->a_obar.as<double2>(), (int)T.T, neps,
+                                     ctx->a_mbar.as<double2>(), st));
+          }
+          pmx::dev::ZbarArgs za{};
+          za.nk = cnt;
+          za.n = n;
+          za.npw = npw;
+          za.soc = dc.soc;
+          za.nev = nall;
+          za.ns = ns;
+          za.neps = neps;
+          za.ncd_max = ncd_max;
+          za.nvd_max = nvd_max;
+          za.zk = ctx->zk.as<double2>();
+          za.zq = ctx->zq.as<double2>();
+          za.ncd = ctx->ncd.as<int>();
+          za.nvd = ctx->nvd.as<int>();
+          za.cbase = ctx->cbase.as<int>();
+          za.vbase = ctx->vbase.as<int>();
+          za.cidx = ctx->cidx.as<int>();
+          za.vidx = ctx->vidx.as<int>();
+          za.blkoff = ctx->blkoff.as<long long>();
+          za.dest = ctx->dest.as<long long>();
+          za.loci = ctx->loci.as<int>();
+          za.linv = ctx->a_linv.as<int>();
+          za.mbar = ctx->a_mbar.as<double2>();
+          za.dEbar = ctx->a_debar.as<double>();
+          za.zbar_k = ctx->a_zbk.as<double2>();
+          za.zbar_q = ctx->a_zbq.as<double2>();
+          za.lbar_k = ctx->a_lbk.as<double>();
+          za.lbar_q = ctx->a_lbq.as<double>();
+          {
+            KTime kt(ctx, "adj_zbar");
+            CK(pmx::dev::launch_zbar(za, st));
+          }
+          ctx->launches += 3;
+        }
+        // eigenproblem adjoint of both sides, then the pair accumulators
+        Timer tm(ctx, 3);
+        h2d(ctx, ctx->a_lamk, wk.data(), sizeof(double) * wk.size());
+        h2d(ctx, ctx->a_lamq, wq.data(), sizeof(double) * wq.size());
+        const size_t cz = (size_t)cnt * ns * nall;
+        CK(ctx->a_C.ensure(sizeof(double2) * 2 * cz));
+        CK(ctx->a_X.ensure(sizeof(double2) * (size_t)cnt * ns * n));
+        for (int side = 0; side < 2; ++side) {
+          const double2* Z = side == 0 ? ctx->zk.as<double2>() : ctx->zq.as<double2>();
+          const double2* Zb = side == 0 ? ctx->a_zbk.as<double2>() : ctx->a_zbq.as<double2>();
+          const double* lam = side == 0 ? ctx->a_lamk.as<double>() : ctx->a_lamq.as<double>();
+          const double* lb = side == 0 ? ctx->a_lbk.as<double>() : ctx->a_lbq.as<double>();
+          double2* C = ctx->a_C.as<double2>();
+          {
+            KTime kt(ctx, "adj_eig");
+            CK(pmx::dev::launch_zgemm_batched(1, nall, ns, n, Z, n, (long long)nall * n, Zb, n, (long long)ns * n, C,
+                                              nall, (long long)ns * nall, cnt, st));
+            CK(pmx::dev::launch_eig_kmat(C, lam, nall, lb, nall, ns, cnt, tau, st));
+            CK(pmx::dev::launch_zgemm_batched(0, n, ns, nall, Z, n, (long long)nall * n, C + cz, nall,
+                                              (long long)ns * nall, ctx->a_X.as<double2>(), n, (long long)ns * n, cnt,
+                                              st));
+          }
+          ctx->launches += 3;
+          hgrad_items(ctx, dc, ctx->a_X.as<double2>(), (long long)ns * n, Z, (long long)nall * n,
+                      side == 0 ? ks : kqs, ns);
+        }
+      }
+    }
+    adj_finish(ctx, P, dc, grad);
     return (int)PMX_OK;
   });
 }

@@ -83,6 +83,21 @@ def test_heev_vs_numpy(ctx, n, degenerate):
         assert np.max(np.abs(Z[b].conj().T @ Z[b] - np.eye(nev))) < 1e-10
 
 
+@pytest.mark.parametrize("n,nev", [(300, 300), (120, 120), (400, 260)])
+def test_heev_all_eigenpairs(ctx, n, nev):
+    """More eigenvalues than eigensolver threads (plain bisection) and full spectra."""
+    rng = np.random.default_rng(n + nev)
+    A = np.stack([_random_hermitian(rng, n) for _ in range(2)])
+    w, Z = ctx.heev(A, nev)
+    for b in range(2):
+        ref = np.linalg.eigvalsh(A[b])[:nev]
+        scale = np.max(np.abs(ref))
+        assert np.max(np.abs(w[b] - ref)) < 1e-12 * scale * n
+        R = A[b] @ Z[b] - Z[b] * w[b]
+        assert np.max(np.linalg.norm(R, axis=0)) < 1e-10 * scale
+        assert np.max(np.abs(Z[b].conj().T @ Z[b] - np.eye(nev))) < 1e-10
+
+
 def test_kk_vs_oracle(ctx):
     rng = np.random.default_rng(3)
     nf, rows, dw = 300, 7, 0.05
