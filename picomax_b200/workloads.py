@@ -54,21 +54,48 @@ def wz_form_factors(seed: int = 1967, f: float = 1.626):
     return vg
 
 
-def te_form_factors(seed: int = 1968, f: float = 1.33):
-    """8 form factors on the first 8 |G|^2 shells of trigonal Te (same value
-    for the 3 atoms); SOC lambda_S uniform and lambda_A on the listed shells."""
+def te_shells(f: float = 1.33):
+    """The first 8 |G|^2 shells ((2 pi/a)^2) of the trigonal Te lattice."""
     s3 = math.sqrt(3.0)
     b = np.array([[1, -1 / s3, 0], [1, 1 / s3, 0], [0, 0, 1.0 / f]])
     r3 = np.arange(-3, 4)
     hkl = np.array(np.meshgrid(r3, r3, r3, indexing="ij")).reshape(3, -1).T
     g2 = np.unique(np.round(((hkl @ b) ** 2).sum(1), 6))
-    keys = g2[1:9]
+    return g2[1:9]
+
+
+def te_params(seed: int = 1969):
+    """The 10 free parameters of trigonal Te (Ry): 8 form factors (the same
+    for the 3 atoms) ~ U(-0.3, 0.3), lambda_S ~ U(0.002, 0.01) (uniform over
+    |G|^2) and lambda_A ~ U(0, 0.005) (on the first 4 shells). The default
+    seed gives an insulator on the 10x10x8 grid (no state within 0.9 eV of
+    the reference energy), so occupations do not change under small steps."""
     r = np.random.default_rng(seed)
     v = r.uniform(-0.3, 0.3, 8)
-    vg = _fmt(keys) + "," + ",".join([_fmt(v)] * 3)
-    soc = ["-use_uniform_us_so", "-uniform_us_so_val", f"{r.uniform(0.002, 0.01):.6f}",
-           "-ua_so", ",".join(f"{k:.6f}:{x:.6f}" for k, x in zip(keys[:4], r.uniform(0, 0.005, 4)))]
+    return np.concatenate([v, [r.uniform(0.002, 0.01), r.uniform(0.0, 0.005)]])
+
+
+def te_form_factors(seed: int = 1969, f: float = 1.33, theta=None):
+    """-vg and SOC options of trigonal Te for the free parameters theta
+    (te_params(seed) by default)."""
+    keys = te_shells(f)
+    th = te_params(seed) if theta is None else np.asarray(theta, float)
+    vg = _fmt(keys) + "," + ",".join([_fmt(th[:8])] * 3)
+    soc = ["-use_uniform_us_so", "-uniform_us_so_val", f"{th[8]:.6f}",
+           "-ua_so", ",".join(f"{k:.6f}:{th[9]:.6f}" for k in keys[:4])]
     return vg, soc
+
+
+def te_param_map(natom: int = 3, nshell: int = 8, nua: int = 4) -> np.ndarray:
+    """J with full = J @ theta: theta (8 form factors, lambda_S, lambda_A) to
+    the problem's parameter vector (vg[atom][shell], lambda_S, lambda_A per key)."""
+    J = np.zeros((natom * nshell + 1 + nua, nshell + 2))
+    for a in range(natom):
+        for s in range(nshell):
+            J[a * nshell + s, s] = 1.0
+    J[natom * nshell, nshell] = 1.0
+    J[natom * nshell + 1:, nshell + 1] = 1.0
+    return J
 
 
 def workload(name: str, workdir: str):

@@ -95,3 +95,29 @@ def test_epsm_vjp_vs_gpu_finite_differences(ctx, tmp_path):
     prob.set_params(th)
     assert np.max(np.abs(got - fd)) < 1e-6 * np.max(np.abs(fd))
     prob.close()
+
+
+def test_torch_autograd_wrappers(ctx, tmp_path):
+    """picomax_b200.autograd: backward of a loss through band() and eps_m()
+    with a parameter map equals J^T of the C-ABI vector-Jacobian products."""
+    import torch
+    import picomax_b200 as pm
+    from picomax_b200.autograd import band, eps_m
+    args, *_ = grad_case(tmp_path)
+    pe, pb = pm.Problem(args), pm.Problem(_band_args(args))
+    full0 = pe.params()
+    J = np.eye(len(full0))[:, :6] * 0.5  # ties the first 6 parameters, zeroes the rest
+    th = torch.tensor(np.linalg.lstsq(J, full0, rcond=None)[0], dtype=torch.float64, requires_grad=True)
+    E = band(th, pb, ctx, J)
+    eps = eps_m(th, pe, ctx, J)
+    L = (E ** 2).sum() + (eps.imag ** 2).sum()
+    L.backward()
+    full = J @ th.detach().numpy()
+    pb.set_params(full)
+    pe.set_params(full)
+    Eh = ctx.band(pb)
+    _, _, em = ctx.chi_epsm(pe, pm.SWITCH_EPSLL, pm.PREC_FP64)
+    ref = J.T @ (ctx.band_vjp(pb, 2 * Eh) + ctx.epsm_vjp(pe, 2j * em.imag))
+    assert np.max(np.abs(th.grad.numpy() - ref)) < 1e-10 * np.max(np.abs(ref))
+    pe.close()
+    pb.close()
