@@ -148,7 +148,7 @@ int pmx_heev_batched(pmx_ctx* ctx, int n, int batch, const double* A, int nev, d
  * legacy default stream); returns without waiting for the GPU.
  * Scratch: one fixed 16 MiB device array inside the library (table of at most
  * 1024 matrices, then 4 n nev doubles of inverse-iteration vectors per matrix
- * when z is given). batch > 1024, n > 864, or 32 n nev batch bytes above
+ * when z is given). batch > 1024, n > 832, or 32 n nev batch bytes above
  * 16 MiB - 80 KiB (with z) return PMX_ERR_LIMIT. The first call on a device
  * looks the array up (set-up, once per device): make that first call before
  * any stream capture. Every call on a device shares the array and rewrites
@@ -194,6 +194,25 @@ int pmx_eps_macroscopic(pmx_ctx* ctx, int neps, int nq, int nfreq, const double*
 /* Kramers-Kronig transform of nrows spectra in place, re/im [nrows][nfreq],
  * w_f = dfreq f (kramerskronigtransform, src/pmx_chi.cpp:272-309). */
 int pmx_kk(pmx_ctx* ctx, int nrows, int nfreq, double dfreq, double* re, double* im);
+
+/* ---------------------------------------------------------------- batches
+ * Several crystals at once. Every eigensolve stage of all problems (reference
+ * points, path points, the k and k+q grids of each q) runs as one assembly and
+ * one eigensolver launch per matrix-size class (matrices sorted by size),
+ * whatever the mix of N_G and SOC; the chi stages that follow run per problem.
+ * Results are those of the per-problem calls (same kernels; rounding may
+ * differ at the 1e-13 level because the eigensolver schedule can differ).
+ * The reference runs one process per crystal. */
+
+/* pmx_band of problems[0..count): eband[i] as pmx_band's output for problems[i]. */
+int pmx_band_batch(pmx_ctx* ctx, int count, const pmx_problem* const* problems, double* const* eband);
+
+/* pmx_chi (or pmx_chi_epsm when epsm != NULL and epsm[i] != NULL) of
+ * problems[0..count) with one switch and precision; re[i]/im[i] as pmx_chi's
+ * outputs for problems[i]. Problems are grouped so that the eigenvectors of
+ * one group at k and at k+q stay within 2 x 16 GB. */
+int pmx_chi_batch(pmx_ctx* ctx, int count, const pmx_problem* const* problems, int sw, int precision,
+                  double* const* re, double* const* im, double* const* epsm);
 
 /* ---------------------------------------------------------------- adjoint
  * The reference computes no gradients; these entry points differentiate its

@@ -44,6 +44,8 @@ EXPORTS = (
     "pmx_problem_set_params",
     "pmx_band_vjp",
     "pmx_epsm_vjp",
+    "pmx_band_batch",
+    "pmx_chi_batch",
 )
 
 
@@ -111,6 +113,9 @@ def load() -> ctypes.CDLL:
         "pmx_problem_set_params": (c_int, [c_void_p, dp, c_int]),
         "pmx_band_vjp": (c_int, [c_void_p, c_void_p, dp, dp]),
         "pmx_epsm_vjp": (c_int, [c_void_p, c_void_p, dp, dp, dp, dp]),
+        "pmx_band_batch": (c_int, [c_void_p, c_int, POINTER(c_void_p), POINTER(dp)]),
+        "pmx_chi_batch": (c_int, [c_void_p, c_int, POINTER(c_void_p), c_int, c_int, POINTER(dp), POINTER(dp),
+                                  POINTER(dp)]),
         "pmx_ctx_tuning": (c_int, [c_void_p, c_char_p, c_size_t, POINTER(c_size_t)]),
     }
     for name, (res, args) in sig.items():
@@ -319,6 +324,29 @@ class Context:
         self._check(self._lib.pmx_chi_epsm(self.handle, prob.handle, switch, precision, _dptr(re), _dptr(im),
                                            _dptr(eps)), "chi_epsm")
         return re, im, eps[..., 0] + 1j * eps[..., 1]
+
+    def band_batch(self, probs):
+        """pmx_band of several problems in merged launches: list of [nq][nband]."""
+        outs = [np.zeros((p.info.nq, p.info.nband), np.float64) for p in probs]
+        ph = (c_void_p * len(probs))(*[p.handle for p in probs])
+        op = (POINTER(c_double) * len(probs))(*[_dptr(o) for o in outs])
+        self._check(self._lib.pmx_band_batch(self.handle, len(probs), ph, op), "band_batch")
+        return outs
+
+    def chi_batch(self, probs, switch: int, precision: int = PREC_FP64, epsm: bool = False):
+        """pmx_chi(_epsm) of several problems: list of (re, im[, eps_M])."""
+        n = len(probs)
+        res = [np.zeros(p.info.chi_values, np.float64) for p in probs]
+        ims = [np.zeros(p.info.chi_values, np.float64) for p in probs]
+        eps = [np.zeros((p.info.nq, p.info.nfreq, 2), np.float64) for p in probs] if epsm else None
+        ph = (c_void_p * n)(*[p.handle for p in probs])
+        rp = (POINTER(c_double) * n)(*[_dptr(x) for x in res])
+        ip = (POINTER(c_double) * n)(*[_dptr(x) for x in ims])
+        ep = (POINTER(c_double) * n)(*[_dptr(x) for x in eps]) if epsm else None
+        self._check(self._lib.pmx_chi_batch(self.handle, n, ph, switch, precision, rp, ip, ep), "chi_batch")
+        if epsm:
+            return [(r, i, e[..., 0] + 1j * e[..., 1]) for r, i, e in zip(res, ims, eps)]
+        return list(zip(res, ims))
 
     def band_vjp(self, prob: Problem, dE) -> np.ndarray:
         """dL/dparams from dL/d eband [nq][nband]."""

@@ -198,11 +198,15 @@ struct LowerPacked {  // packed columns in shared memory
 //   ints: cnt[kHeevThreads] clus[nev+1] misc[4]
 // ring = depth of the per-warp prefetch ring of the global-memory path
 // (0 = direct loads from L2).
+// With MAXS >= kPartGlobalMaxs (n > 832) the per-warp partial sums part[]
+// live in the item's global scratch instead (see heev_scratch_doubles).
+constexpr int kPartGlobalMaxs = 38;
+
 __host__ __device__ inline size_t heev_smem_bytes(int n, int nev, bool resident, int maxs = 0, int ring = 0) {
   size_t b = 0;
   if (resident) b += (size_t)n * (n + 1) / 2 * sizeof(double2);
   if (!resident && maxs > 0) b += (size_t)kWarps * ring * 32 * maxs * sizeof(double2);
-  b += (size_t)(6 + kWarps) * n * sizeof(double2);
+  b += (size_t)(6 + (maxs >= kPartGlobalMaxs ? 0 : kWarps)) * n * sizeof(double2);
   b += (size_t)(3 * n + 2 * kWarps + 3 * nev + kHeevThreads) * sizeof(double);
   b += (size_t)(kHeevThreads + nev + 1 + 4) * sizeof(int);
   return b;
@@ -415,8 +419,10 @@ __global__ void __launch_bounds__(kHeevThreads, (RING >= 2 || MAXS > 9) ? 1 : 2)
   double2* vcur = wprev + n;
   double2* dotp = vcur + n;
   double2* tau = dotp + n;
-  double2* part = tau + n;
-  double2* cnext = part + (size_t)kWarps * n;
+  constexpr bool kPartG = !RESIDENT && MAXS >= kPartGlobalMaxs;
+  double2* part = kPartG ? reinterpret_cast<double2*>(scratch + it.s_off + (size_t)4 * n * (nvec > 0 ? nvec : 1))
+                         : tau + n;
+  double2* cnext = kPartG ? tau + n : part + (size_t)kWarps * n;
   double2* wring = cnext + n;  // per-warp prefetch ring (global-memory path)
   if (!RESIDENT) sp = wring + (size_t)kWarps * RING * 32 * MAXS;
   else sp = wring;
@@ -609,6 +615,11 @@ __global__ void __launch_bounds__(kHeevThreads, (RING >= 2 || MAXS > 9) ? 1 : 2)
     }
   }
   if (tid == 0) info[blockIdx.x] = 0;
+}
+
+size_t heev_scratch_doubles(int n, int nvec, int max_n) {
+  const int slots = (max_n + 31) / 32;
+  return (size_t)4 * n * (nvec > 0 ? nvec : 1) + (slots > 26 ? (size_t)2 * kWarps * n : 0);
 }
 
 bool heev_resident(int n, int nev) { return heev_smem_bytes(n, nev, true) <= (size_t)227 * 1024; }

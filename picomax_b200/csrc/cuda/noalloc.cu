@@ -29,7 +29,9 @@ constexpr size_t kScratchBytes = size_t(16) << 20;  // the whole array
 constexpr int kMaxItems = 1024;                     // matrices per call
 constexpr size_t kItemBytes = (kMaxItems * sizeof(EigItem) + 255) / 256 * 256;
 constexpr size_t kVecDoubles = (kScratchBytes - kItemBytes) / sizeof(double);
-constexpr int kMaxN = 864;  // the eigensolver's shared-memory layout fits 227 KB up to here (nev <= 512)
+// Above n = 832 the eigensolver keeps per-warp partial sums in global scratch,
+// which this entry point's item layout does not provide.
+constexpr int kMaxN = 832;
 constexpr int kMaxDevices = 64;
 
 // Shared by every call on a device: [item table | inverse-iteration vectors].

@@ -38,7 +38,7 @@ struct EigItem {
   long long h_off;    // double2 offset of the n*n column-major workspace
   long long w_off;    // double offset of nval eigenvalues
   long long z_off;    // double2 offset of nev eigenvectors (column s at z_off + s*n)
-  long long s_off;    // double offset of 4*n*nev inverse-iteration scratch
+  long long s_off;    // double offset of the item's scratch (heev_scratch_doubles)
 };
 
 // Fills H(k) of every item (full Hermitian storage) into hbuf.
@@ -52,6 +52,11 @@ cudaError_t launch_assemble(const CrystalDev* crystals, const EigItem* items, in
 cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev, double2* hbuf,
                         double* wbuf, double2* zbuf, double* scratch, int* info, cudaStream_t st, int variant = 0);
 int heev_smem_max_n();
+// Global scratch (doubles) one item of size n with nvec eigenvectors needs in
+// a launch whose largest matrix is max_n; items must be spaced by at least
+// this much (EigItem::s_off), and the scratch is used with or without vectors
+// when max_n > 832.
+size_t heev_scratch_doubles(int n, int nvec, int max_n);
 // Number of schedules launch_heev offers for matrices of size max_n.
 int heev_variants(int max_n, int max_nev);
 

@@ -255,6 +255,8 @@ struct pmx_ctx {
   // adjoint workspaces
   DevBuf a_chi, a_g, a_gx, a_kk, a_f1, a_f2, a_obar, a_debar, a_mbar, a_zbk, a_zbq, a_lbk, a_lbq;
   DevBuf a_lamk, a_lamq, a_C, a_X, a_R, a_SV, a_SSO, a_kp, a_linv;
+  // several crystals at once (batched entry points)
+  DevBuf b_g, b_hkl, b_vloc, b_vso, b_crystal;
   double m2_err = 0.0, m2_max = 0.0;  // |M|^2 error of the mixed path's FP32 overlaps (last call)
   cudaEvent_t ev[2] = {nullptr, nullptr};
 };
@@ -397,7 +399,9 @@ void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int 
   chunk = std::min(chunk, 4096);
   CK(c->hbuf.ensure(hbytes * chunk));
   CK(c->wbuf.ensure(sizeof(double) * (size_t)nk * nval));
-  CK(c->scratch.ensure(sizeof(double) * 4 * (size_t)n * std::max(nvec, 1) * (vec ? chunk : 1)));
+  const size_t sstride = pmx::dev::heev_scratch_doubles(n, vec ? nvec : 0, n);
+  const bool per_item = vec || n > 832;  // without vectors the scratch holds only the large-n partial sums
+  CK(c->scratch.ensure(sizeof(double) * sstride * (per_item ? chunk : 1)));
   CK(c->info.ensure(sizeof(int) * chunk));
   std::vector<pmx::dev::EigItem> items(chunk);
   std::vector<int> info(chunk);
@@ -415,7 +419,7 @@ void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int 
       it.h_off = (long long)i * n * n;
       it.w_off = (long long)(k0 + i) * nval;
       it.z_off = (long long)(k0 + i) * nvec * n;
-      it.s_off = (long long)i * 4 * n * std::max(nvec, 1);
+      it.s_off = per_item ? (long long)(i * sstride) : 0;
     }
     h2d(c, c->items, items.data(), sizeof(pmx::dev::EigItem) * cnt);
     {
@@ -572,7 +576,8 @@ extern "C" int pmx_heev_batched(pmx_ctx* ctx, int n, int batch, const double* A,
     CK(ctx->hbuf.ensure(std::max<size_t>(hb * batch, 16)));
     CK(ctx->wbuf.ensure(std::max<size_t>(sizeof(double) * (size_t)batch * nev, 16)));
     CK(ctx->zk.ensure(std::max<size_t>(sizeof(double2) * (size_t)batch * nev * n, 16)));
-    CK(ctx->scratch.ensure(std::max<size_t>(sizeof(double) * 4 * (size_t)n * nev * batch, 16)));
+    const size_t sstride = pmx::dev::heev_scratch_doubles(n, z ? nev : 0, n);
+    CK(ctx->scratch.ensure(std::max<size_t>(sizeof(double) * sstride * batch, 16)));
     CK(ctx->info.ensure(std::max<size_t>(sizeof(int) * batch, 16)));
     std::vector<pmx::dev::EigItem> items(batch);
     for (int i = 0; i < batch; ++i) {
@@ -584,7 +589,7 @@ extern "C" int pmx_heev_batched(pmx_ctx* ctx, int n, int batch, const double* A,
       items[i].h_off = (long long)i * n * n;
       items[i].w_off = (long long)i * nev;
       items[i].z_off = (long long)i * nev * n;
-      items[i].s_off = (long long)i * 4 * n * nev;
+      items[i].s_off = (long long)(i * sstride);
     }
     if (batch == 0) return (int)PMX_OK;
     CK(cudaMemcpyAsync(ctx->hbuf.ptr, A, hb * batch, cudaMemcpyHostToDevice, ctx->stream));
@@ -752,6 +757,255 @@ int window_half(const Problem& p) {
 
 }  // namespace
 
+namespace {
+
+// Per-problem constants of the chi stage.
+struct ChiPlan {
+  int mode, nk, nq, neps, nf, np, nev, nval, n, nch, W, FT, nft;
+  size_t blkvals;  // one q, one of Re/Im
+  bool pv;
+  pmx::dev::ScaleArgs sa;
+};
+
+ChiPlan chi_plan(const Problem& p, int sw, const DevCrystal& dc) {
+  if (!p.have_freq || p.nfreq <= 0 || !(p.dfreq > 0))
+    throw std::runtime_error("-nfreq and -dfreq are required for the chi switches");
+  if (p.nband > 2 * p.npw()) throw std::runtime_error("-nband exceeds the Hamiltonian dimension");
+  if (p.nband <= 0) throw std::runtime_error("-nband must be positive");
+  ChiPlan pl;
+  pl.mode = sw == PMX_SWITCH_EPSLL ? 1 : 0;
+  pl.nk = p.nk();
+  pl.nq = p.nq();
+  pl.neps = p.neps;
+  pl.nf = p.nfreq;
+  pl.np = pl.neps * (pl.neps + 1) / 2;
+  pl.blkvals = (size_t)9 * pl.np * pl.nf;
+  pl.nev = solved_states(p.nband, dc.soc);
+  pl.nval = std::min(solved_states(p.nband + 1, dc.soc), dc.n);
+  pl.n = dc.n;
+  pl.nch = (pl.mode == 0 && dc.soc) ? 4 : 1;
+  // scale factors (src/pmx_chi.cpp:341, src/pmx_chi_copy.cpp:351-360)
+  const double a_cm = p.lat.a * pmx::kAngstrom, bz = p.lat.bz_volume;
+  pmx::dev::ScaleArgs& sa = pl.sa;
+  sa = pmx::dev::ScaleArgs{};
+  sa.mode = pl.mode;
+  sa.np = pl.np;
+  sa.nf = pl.nf;
+  sa.dfreq = p.dfreq;
+  sa.sf = 4.0 * bz * std::pow(pmx::kPi, 5) * std::pow(pmx::kHbar, 4) * std::pow(pmx::kE, 2) /
+          (std::pow(pmx::kEV, 3) * std::pow(pmx::kEm, 2) * std::pow(a_cm, 5));
+  sa.sf_ll = 2.0 * bz * std::pow(pmx::kE, 2) / (pmx::kPi * pmx::kEV * a_cm);
+  sa.sf_tt = 32.0 * bz * std::pow(pmx::kPi, 3) * std::pow(pmx::kHbar, 4) * std::pow(pmx::kE, 2) /
+             (std::pow(pmx::kEV, 3) * std::pow(pmx::kEm, 2) * std::pow(a_cm, 5));
+  sa.sf_lt = 8.0 * bz * pmx::kPi * std::pow(pmx::kHbar, 2) * std::pow(pmx::kE, 2) /
+             (std::pow(pmx::kEV, 2) * pmx::kEm * std::pow(a_cm, 3));
+  pl.W = pl.mode == 0 ? window_half(p) : -1;
+  pl.FT = pmx::dev::contract_ftile();
+  pl.nft = (pl.nf + pl.FT - 1) / pl.FT;
+  pl.pv = pl.mode == 1 && p.kk == 0;
+  return pl;
+}
+
+void chi_buffers(pmx_ctx* ctx, const ChiPlan& pl) {
+  CK(ctx->acc.ensure(sizeof(double) * 2 * pl.blkvals));
+  CK(ctx->chi.ensure(sizeof(double) * 2 * pl.blkvals));
+  CK(ctx->chi2.ensure(sizeof(double) * 2 * pl.blkvals));
+  if (pl.pv) CK(ctx->accpv.ensure(sizeof(double) * 2 * pl.blkvals));
+}
+
+// Static tables of one problem's chi stage (loci, k-points).
+void chi_tables(pmx_ctx* ctx, const Problem& p) {
+  h2d(ctx, ctx->loci, p.loci.data(), sizeof(int) * p.loci.size());
+  std::vector<double> kp(3 * (size_t)p.nk());
+  for (int k = 0; k < p.nk(); ++k)
+    for (int x = 0; x < 3; ++x) kp[3 * k + x] = p.K[k][x];
+  h2d(ctx, ctx->kpts, kp.data(), sizeof(double) * kp.size());
+}
+
+// One q of one problem, from the eigenpairs at k (wk, zk) and k+q (wq, zq):
+// transitions, overlaps, contraction, scaling, Kramers-Kronig, copy-out into
+// the .dat layout [i][j][q][m][n][f] of re/im (and eps_M of this q).
+void chi_process_q(pmx_ctx* ctx, const Problem& p, const ChiPlan& pl, const DevCrystal& dc, int q, double off,
+                   const std::vector<double>& wk, const std::vector<double>& wq, const double2* zk,
+                   const double2* zq, int precision, double* re, double* im, bool device_out, double* epsm) {
+  cudaStream_t st = ctx->stream;
+  const int mode = pl.mode, nk = pl.nk, nq = pl.nq, neps = pl.neps, nf = pl.nf, np = pl.np;
+  const int nev = pl.nev, nval = pl.nval, n = pl.n, nch = pl.nch, W = pl.W, FT = pl.FT, nft = pl.nft;
+  const size_t blkvals = pl.blkvals;
+  const bool pv = pl.pv;
+  pmx::dev::ScaleArgs sa = pl.sa;
+  const Vec3 Q = p.lat.Q[q];
+  Transitions T = build_transitions(p, dc.soc, nval, wk, wq, off, mode == 0, ctx->degenerate_cuts);
+  // per-m polarisation and SOC-current tables
+  std::vector<double2> uv((size_t)neps * 9), ss((size_t)neps * 3);
+  std::vector<double> qg(neps);
+  for (int m = 0; m < neps; ++m) {
+    const Vec3 v = Q + p.G[m];
+    qg[m] = pmx::norm(v);
+    double u[3][3][2];
+    pmx::uvec_LT(v, u);
+    std::complex<double> vs[3];
+    soc_current(p, p.G[m], vs);
+    for (int i = 0; i < 3; ++i) {
+      std::complex<double> s(0, 0);
+      for (int x = 0; x < 3; ++x) {
+        uv[((size_t)m * 3 + i) * 3 + x] = make_double2(u[i][x][0], u[i][x][1]);
+        s += std::conj(std::complex<double>(u[i][x][0], u[i][x][1])) * vs[x];
+      }
+      ss[(size_t)m * 3 + i] = make_double2(s.real(), s.imag());
+    }
+  }
+  h2d(ctx, ctx->uvec, uv.data(), sizeof(double2) * uv.size());
+  h2d(ctx, ctx->ssoc, ss.data(), sizeof(double2) * ss.size());
+  h2d(ctx, ctx->qgn, qg.data(), sizeof(double) * qg.size());
+  h2d(ctx, ctx->ncd, T.ncd.data(), sizeof(int) * T.ncd.size());
+  h2d(ctx, ctx->nvd, T.nvd.data(), sizeof(int) * T.nvd.size());
+  h2d(ctx, ctx->cbase, T.cbase.data(), sizeof(int) * T.cbase.size());
+  h2d(ctx, ctx->vbase, T.vbase.data(), sizeof(int) * T.vbase.size());
+  h2d(ctx, ctx->cidx, T.cidx.data(), sizeof(int) * T.cidx.size());
+  h2d(ctx, ctx->vidx, T.vidx.data(), sizeof(int) * T.vidx.size());
+  h2d(ctx, ctx->blkoff, T.blkoff.data(), sizeof(long long) * T.blkoff.size());
+  h2d(ctx, ctx->dest, T.dest.data(), sizeof(long long) * T.dest.size());
+  h2d(ctx, ctx->dE, T.dE.data(), sizeof(double) * T.dE.size());
+  h2d(ctx, ctx->wgt, T.wgt.data(), sizeof(double) * T.wgt.size());
+  h2d(ctx, ctx->f0, T.f0.data(), sizeof(int) * T.f0.size());
+  // frequency-tile transition ranges
+  std::vector<int2> tr(nft);
+  for (int ft = 0; ft < nft; ++ft) {
+    if (W < 0) {
+      tr[ft] = make_int2(0, (int)T.T);
+    } else {
+      const int flo = ft * FT, fhi = std::min(nf, flo + FT) - 1;
+      const auto b = std::lower_bound(T.f0.begin(), T.f0.end(), flo - W);
+      const auto e = std::upper_bound(T.f0.begin(), T.f0.end(), fhi + W);
+      tr[ft] = make_int2((int)(b - T.f0.begin()), (int)(e - T.f0.begin()));
+    }
+  }
+  h2d(ctx, ctx->trange, tr.data(), sizeof(int2) * tr.size());
+  const int A = 3 * neps;
+  CK(ctx->M.ensure(std::max<size_t>(sizeof(double2) * (size_t)T.T * A * nch, 16)));
+  // overlaps
+  if (T.T > 0) {
+    Timer tm(ctx, 1);
+    pmx::dev::OverlapArgs oa{};
+    oa.n = n;
+    oa.npw = dc.npw;
+    oa.soc = dc.soc;
+    oa.nev = nev;
+    oa.neps = neps;
+    oa.nch = nch;
+    oa.mode = mode;
+    oa.ncd_max = *std::max_element(T.ncd.begin(), T.ncd.end());
+    oa.nvd_max = *std::max_element(T.nvd.begin(), T.nvd.end());
+    int cchunk = std::max(1, oa.ncd_max);
+    while (cchunk > 1 && pmx::dev::overlap_smem_bytes(cchunk, oa.nvd_max, n, dc.npw) > 200 * 1024) --cchunk;
+    if (pmx::dev::overlap_smem_bytes(cchunk, oa.nvd_max, n, dc.npw) > 220 * 1024)
+      throw CudaFail("overlap tile does not fit in shared memory", PMX_ERR_UNSUPPORTED);
+    oa.cchunk = cchunk;
+    oa.zk = zk;
+    oa.zq = zq;
+    oa.ncd = ctx->ncd.as<int>();
+    oa.nvd = ctx->nvd.as<int>();
+    oa.cbase = ctx->cbase.as<int>();
+    oa.vbase = ctx->vbase.as<int>();
+    oa.cidx = ctx->cidx.as<int>();
+    oa.vidx = ctx->vidx.as<int>();
+    oa.blkoff = ctx->blkoff.as<long long>();
+    oa.dest = ctx->dest.as<long long>();
+    oa.loci = ctx->loci.as<int>();
+    oa.G = dc.host.G;
+    oa.kpts = ctx->kpts.as<double>();
+    oa.q[0] = Q.x;
+    oa.q[1] = Q.y;
+    oa.q[2] = Q.z;
+    oa.uvec = ctx->uvec.as<double2>();
+    oa.ssoc = ctx->ssoc.as<double2>();
+    oa.M = ctx->M.as<double2>();
+    KTime kt(ctx, "overlap");
+    CK(pmx::dev::launch_overlap(oa, nk, st));
+    ctx->launches += 1;
+  }
+  // contraction
+  {
+    Timer tm(ctx, 2);
+    pmx::dev::ContractArgs ca{};
+    ca.M = ctx->M.as<double2>();
+    ca.dE = ctx->dE.as<double>();
+    ca.wgt = ctx->wgt.as<double>();
+    ca.f0 = ctx->f0.as<int>();
+    ca.trange = ctx->trange.as<int2>();
+    ca.neps = neps;
+    ca.np = np;
+    ca.nf = nf;
+    ca.nch = nch;
+    ca.window = W;
+    ca.delta = p.delta;
+    ca.eps = p.epsilon;
+    ca.dfreq = p.dfreq;
+    ca.acc = ctx->acc.as<double>();
+    ca.acc_pv = pv ? ctx->accpv.as<double>() : nullptr;
+    if (precision == PMX_PREC_FP64 || pv) {
+      KTime kt(ctx, "contract_f64");
+      CK(pmx::dev::launch_contract_f64(ca, st));
+      ctx->launches += 1;
+    } else {
+      int nl = 0;
+      CK(ctx->mixws.ensure(std::max<size_t>(pmx::dev::mixed_workspace_bytes(ca, (long long)T.T), 16)));
+      CK(ctx->stats.ensure(16));
+      ca.stats = ctx->stats.as<double>();
+      {
+        KTime kt(ctx, "contract_mixed");
+        CK(pmx::dev::launch_contract_mixed(ca, (long long)T.T, ctx->mixws.ptr, nl, st));
+      }
+      ctx->launches += nl;
+      double sv[2] = {0, 0};
+      CK(cudaMemcpyAsync(sv, ctx->stats.ptr, sizeof(sv), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      ctx->m2_err = std::max(ctx->m2_err, sv[0]);
+      ctx->m2_max = std::max(ctx->m2_max, sv[1]);
+    }
+  }
+  // scaling and Kramers-Kronig
+  {
+    Timer tm(ctx, 3);
+    sa.qgn = ctx->qgn.as<double>();
+    sa.acc = ctx->acc.as<double>();
+    sa.acc_pv = pv ? ctx->accpv.as<double>() : nullptr;
+    sa.out = ctx->chi.as<double>();
+    {
+      KTime kt(ctx, "scale");
+      CK(pmx::dev::launch_scale(sa, st));
+    }
+    ctx->launches += 1;
+    if (p.kk) {
+      KTime kt(ctx, "kk");
+      CK(pmx::dev::launch_kk(ctx->chi.as<double>(), ctx->chi2.as<double>(), 9 * np, nf, p.dfreq, st));
+      ctx->launches += 1;
+    }
+  }
+  // copy out into [i][j][q][m][n][f]
+  {
+    Timer tm(ctx, 4);
+    const double* res = p.kk ? ctx->chi2.as<double>() : ctx->chi.as<double>();
+    const size_t row = (size_t)np * nf * sizeof(double);
+    const cudaMemcpyKind kind = device_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    CK(cudaMemcpy2DAsync(re + (size_t)q * np * nf, row * nq, res, row, row, 9, kind, st));
+    CK(cudaMemcpy2DAsync(im + (size_t)q * np * nf, row * nq, res + blkvals, row, row, 9, kind, st));
+    if (!device_out) ctx->d2h += (long long)(2 * 9 * row);
+    if (epsm) {
+      // eps_M of this q from the (L, L) block: [i=0][j=0] rows of res
+      CK(ctx->epsm.ensure(sizeof(double2) * nf));
+      CK(pmx::dev::launch_epsm(res, res + blkvals, neps, 1, nf, ctx->epsm.as<double2>(), st));
+      ctx->launches += 1;
+      CK(cudaMemcpyAsync(epsm + (size_t)2 * q * nf, ctx->epsm.ptr, sizeof(double2) * nf,
+                         device_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+      if (!device_out) ctx->d2h += (long long)(sizeof(double2) * nf);
+    }
+  }
+}
+
+}  // namespace
+
 static int run_chi(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision, double* re, double* im,
                    bool device_out, double* epsm) {
   if (!P || (sw != PMX_SWITCH_EPSIJ && sw != PMX_SWITCH_EPSLL)) return PMX_ERR_INVALID;
@@ -760,15 +1014,7 @@ static int run_chi(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision, do
     const Problem& p = P->p;
     cudaStream_t st = ctx->stream;
     for (double& t : ctx->stage_ms) t = 0;
-    if (!p.have_freq || p.nfreq <= 0 || !(p.dfreq > 0))
-      throw std::runtime_error("-nfreq and -dfreq are required for the chi switches");
-    if (p.nband > 2 * p.npw()) throw std::runtime_error("-nband exceeds the Hamiltonian dimension");
-    if (p.nband <= 0) throw std::runtime_error("-nband must be positive");
     if (!re || !im) return (int)PMX_ERR_INVALID;
-    const int mode = sw == PMX_SWITCH_EPSLL ? 1 : 0;
-    const int nk = p.nk(), nq = p.nq(), neps = p.neps, nf = p.nfreq;
-    const int np = neps * (neps + 1) / 2;
-    const size_t blkvals = (size_t)9 * np * nf;  // one q, one of Re/Im
     DevCrystal dc;
     double off;
     std::vector<double> wk;
@@ -777,48 +1023,19 @@ static int run_chi(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision, do
       dc = upload_crystal(ctx, P, 0);
       off = ref_energy(ctx, P, dc);
     }
-    const int nev = solved_states(p.nband, dc.soc);
-    const int nval = std::min(solved_states(p.nband + 1, dc.soc), dc.n);
-    const int n = dc.n;
+    const ChiPlan pl = chi_plan(p, sw, dc);
+    const int nk = pl.nk, nev = pl.nev, nval = pl.nval, n = pl.n;
     ctx->degenerate_cuts = 0;
     ctx->m2_err = ctx->m2_max = 0.0;
-    const int nch = (mode == 0 && dc.soc) ? 4 : 1;
     CK(ctx->zk.ensure(std::max<size_t>(sizeof(double2) * (size_t)nk * nev * n, 16)));
     CK(ctx->zq.ensure(std::max<size_t>(sizeof(double2) * (size_t)nk * nev * n, 16)));
     {
       Timer tm(ctx, 0);
       solve_k(ctx, dc, p.K, nval, nev, ctx->zk.as<double2>(), wk);
     }
-    // static tables of the chi stage
-    h2d(ctx, ctx->loci, p.loci.data(), sizeof(int) * p.loci.size());
-    std::vector<double> kp(3 * (size_t)nk);
-    for (int k = 0; k < nk; ++k)
-      for (int x = 0; x < 3; ++x) kp[3 * k + x] = p.K[k][x];
-    h2d(ctx, ctx->kpts, kp.data(), sizeof(double) * kp.size());
-    // scale factors (src/pmx_chi.cpp:341, src/pmx_chi_copy.cpp:351-360)
-    const double a_cm = p.lat.a * pmx::kAngstrom, bz = p.lat.bz_volume;
-    pmx::dev::ScaleArgs sa{};
-    sa.mode = mode;
-    sa.np = np;
-    sa.nf = nf;
-    sa.dfreq = p.dfreq;
-    sa.sf = 4.0 * bz * std::pow(pmx::kPi, 5) * std::pow(pmx::kHbar, 4) * std::pow(pmx::kE, 2) /
-            (std::pow(pmx::kEV, 3) * std::pow(pmx::kEm, 2) * std::pow(a_cm, 5));
-    sa.sf_ll = 2.0 * bz * std::pow(pmx::kE, 2) / (pmx::kPi * pmx::kEV * a_cm);
-    sa.sf_tt = 32.0 * bz * std::pow(pmx::kPi, 3) * std::pow(pmx::kHbar, 4) * std::pow(pmx::kE, 2) /
-               (std::pow(pmx::kEV, 3) * std::pow(pmx::kEm, 2) * std::pow(a_cm, 5));
-    sa.sf_lt = 8.0 * bz * pmx::kPi * std::pow(pmx::kHbar, 2) * std::pow(pmx::kE, 2) /
-               (std::pow(pmx::kEV, 2) * pmx::kEm * std::pow(a_cm, 3));
-    const int W = mode == 0 ? window_half(p) : -1;
-    const int FT = pmx::dev::contract_ftile();
-    const int nft = (nf + FT - 1) / FT;
-    CK(ctx->acc.ensure(sizeof(double) * 2 * blkvals));
-    CK(ctx->chi.ensure(sizeof(double) * 2 * blkvals));
-    CK(ctx->chi2.ensure(sizeof(double) * 2 * blkvals));
-    const bool pv = mode == 1 && p.kk == 0;
-    if (pv) CK(ctx->accpv.ensure(sizeof(double) * 2 * blkvals));
-
-    for (int q = 0; q < nq; ++q) {
+    chi_tables(ctx, p);
+    chi_buffers(ctx, pl);
+    for (int q = 0; q < pl.nq; ++q) {
       const Vec3 Q = p.lat.Q[q];
       std::vector<Vec3> kq(nk);
       for (int k = 0; k < nk; ++k) kq[k] = p.K[k] + Q;
@@ -827,173 +1044,8 @@ static int run_chi(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision, do
         Timer tm(ctx, 0);
         solve_k(ctx, dc, kq, nval, nev, ctx->zq.as<double2>(), wq);
       }
-      Transitions T = build_transitions(p, dc.soc, nval, wk, wq, off, mode == 0, ctx->degenerate_cuts);
-      // per-m polarisation and SOC-current tables
-      std::vector<double2> uv((size_t)neps * 9), ss((size_t)neps * 3);
-      std::vector<double> qg(neps);
-      for (int m = 0; m < neps; ++m) {
-        const Vec3 v = Q + p.G[m];
-        qg[m] = pmx::norm(v);
-        double u[3][3][2];
-        pmx::uvec_LT(v, u);
-        std::complex<double> vs[3];
-        soc_current(p, p.G[m], vs);
-        for (int i = 0; i < 3; ++i) {
-          std::complex<double> s(0, 0);
-          for (int x = 0; x < 3; ++x) {
-            uv[((size_t)m * 3 + i) * 3 + x] = make_double2(u[i][x][0], u[i][x][1]);
-            s += std::conj(std::complex<double>(u[i][x][0], u[i][x][1])) * vs[x];
-          }
-          ss[(size_t)m * 3 + i] = make_double2(s.real(), s.imag());
-        }
-      }
-      h2d(ctx, ctx->uvec, uv.data(), sizeof(double2) * uv.size());
-      h2d(ctx, ctx->ssoc, ss.data(), sizeof(double2) * ss.size());
-      h2d(ctx, ctx->qgn, qg.data(), sizeof(double) * qg.size());
-      h2d(ctx, ctx->ncd, T.ncd.data(), sizeof(int) * T.ncd.size());
-      h2d(ctx, ctx->nvd, T.nvd.data(), sizeof(int) * T.nvd.size());
-      h2d(ctx, ctx->cbase, T.cbase.data(), sizeof(int) * T.cbase.size());
-      h2d(ctx, ctx->vbase, T.vbase.data(), sizeof(int) * T.vbase.size());
-      h2d(ctx, ctx->cidx, T.cidx.data(), sizeof(int) * T.cidx.size());
-      h2d(ctx, ctx->vidx, T.vidx.data(), sizeof(int) * T.vidx.size());
-      h2d(ctx, ctx->blkoff, T.blkoff.data(), sizeof(long long) * T.blkoff.size());
-      h2d(ctx, ctx->dest, T.dest.data(), sizeof(long long) * T.dest.size());
-      h2d(ctx, ctx->dE, T.dE.data(), sizeof(double) * T.dE.size());
-      h2d(ctx, ctx->wgt, T.wgt.data(), sizeof(double) * T.wgt.size());
-      h2d(ctx, ctx->f0, T.f0.data(), sizeof(int) * T.f0.size());
-      // frequency-tile transition ranges
-      std::vector<int2> tr(nft);
-      for (int ft = 0; ft < nft; ++ft) {
-        if (W < 0) {
-          tr[ft] = make_int2(0, (int)T.T);
-        } else {
-          const int flo = ft * FT, fhi = std::min(nf, flo + FT) - 1;
-          const auto b = std::lower_bound(T.f0.begin(), T.f0.end(), flo - W);
-          const auto e = std::upper_bound(T.f0.begin(), T.f0.end(), fhi + W);
-          tr[ft] = make_int2((int)(b - T.f0.begin()), (int)(e - T.f0.begin()));
-        }
-      }
-      h2d(ctx, ctx->trange, tr.data(), sizeof(int2) * tr.size());
-      const int A = 3 * neps;
-      CK(ctx->M.ensure(std::max<size_t>(sizeof(double2) * (size_t)T.T * A * nch, 16)));
-      // overlaps
-      if (T.T > 0) {
-        Timer tm(ctx, 1);
-        pmx::dev::OverlapArgs oa{};
-        oa.n = n;
-        oa.npw = dc.npw;
-        oa.soc = dc.soc;
-        oa.nev = nev;
-        oa.neps = neps;
-        oa.nch = nch;
-        oa.mode = mode;
-        oa.ncd_max = *std::max_element(T.ncd.begin(), T.ncd.end());
-        oa.nvd_max = *std::max_element(T.nvd.begin(), T.nvd.end());
-        int cchunk = std::max(1, oa.ncd_max);
-        while (cchunk > 1 && pmx::dev::overlap_smem_bytes(cchunk, oa.nvd_max, n, dc.npw) > 200 * 1024) --cchunk;
-        if (pmx::dev::overlap_smem_bytes(cchunk, oa.nvd_max, n, dc.npw) > 220 * 1024)
-          throw CudaFail("overlap tile does not fit in shared memory", PMX_ERR_UNSUPPORTED);
-        oa.cchunk = cchunk;
-        oa.zk = ctx->zk.as<double2>();
-        oa.zq = ctx->zq.as<double2>();
-        oa.ncd = ctx->ncd.as<int>();
-        oa.nvd = ctx->nvd.as<int>();
-        oa.cbase = ctx->cbase.as<int>();
-        oa.vbase = ctx->vbase.as<int>();
-        oa.cidx = ctx->cidx.as<int>();
-        oa.vidx = ctx->vidx.as<int>();
-        oa.blkoff = ctx->blkoff.as<long long>();
-        oa.dest = ctx->dest.as<long long>();
-        oa.loci = ctx->loci.as<int>();
-        oa.G = ctx->g.as<double>();
-        oa.kpts = ctx->kpts.as<double>();
-        oa.q[0] = Q.x;
-        oa.q[1] = Q.y;
-        oa.q[2] = Q.z;
-        oa.uvec = ctx->uvec.as<double2>();
-        oa.ssoc = ctx->ssoc.as<double2>();
-        oa.M = ctx->M.as<double2>();
-        KTime kt(ctx, "overlap");
-        CK(pmx::dev::launch_overlap(oa, nk, st));
-        ctx->launches += 1;
-      }
-      // contraction
-      {
-        Timer tm(ctx, 2);
-        pmx::dev::ContractArgs ca{};
-        ca.M = ctx->M.as<double2>();
-        ca.dE = ctx->dE.as<double>();
-        ca.wgt = ctx->wgt.as<double>();
-        ca.f0 = ctx->f0.as<int>();
-        ca.trange = ctx->trange.as<int2>();
-        ca.neps = neps;
-        ca.np = np;
-        ca.nf = nf;
-        ca.nch = nch;
-        ca.window = W;
-        ca.delta = p.delta;
-        ca.eps = p.epsilon;
-        ca.dfreq = p.dfreq;
-        ca.acc = ctx->acc.as<double>();
-        ca.acc_pv = pv ? ctx->accpv.as<double>() : nullptr;
-        if (precision == PMX_PREC_FP64 || pv) {
-          KTime kt(ctx, "contract_f64");
-          CK(pmx::dev::launch_contract_f64(ca, st));
-          ctx->launches += 1;
-        } else {
-          int nl = 0;
-          CK(ctx->mixws.ensure(std::max<size_t>(pmx::dev::mixed_workspace_bytes(ca, (long long)T.T), 16)));
-          CK(ctx->stats.ensure(16));
-          ca.stats = ctx->stats.as<double>();
-          {
-            KTime kt(ctx, "contract_mixed");
-            CK(pmx::dev::launch_contract_mixed(ca, (long long)T.T, ctx->mixws.ptr, nl, st));
-          }
-          ctx->launches += nl;
-          double sv[2] = {0, 0};
-          CK(cudaMemcpyAsync(sv, ctx->stats.ptr, sizeof(sv), cudaMemcpyDeviceToHost, st));
-          CK(cudaStreamSynchronize(st));
-          ctx->m2_err = std::max(ctx->m2_err, sv[0]);
-          ctx->m2_max = std::max(ctx->m2_max, sv[1]);
-        }
-      }
-      // scaling and Kramers-Kronig
-      {
-        Timer tm(ctx, 3);
-        sa.qgn = ctx->qgn.as<double>();
-        sa.acc = ctx->acc.as<double>();
-        sa.acc_pv = pv ? ctx->accpv.as<double>() : nullptr;
-        sa.out = ctx->chi.as<double>();
-        {
-          KTime kt(ctx, "scale");
-          CK(pmx::dev::launch_scale(sa, st));
-        }
-        ctx->launches += 1;
-        if (p.kk) {
-          KTime kt(ctx, "kk");
-          CK(pmx::dev::launch_kk(ctx->chi.as<double>(), ctx->chi2.as<double>(), 9 * np, nf, p.dfreq, st));
-          ctx->launches += 1;
-        }
-      }
-      // copy out into [i][j][q][m][n][f]
-      {
-        Timer tm(ctx, 4);
-        const double* res = p.kk ? ctx->chi2.as<double>() : ctx->chi.as<double>();
-        const size_t row = (size_t)np * nf * sizeof(double);
-        const cudaMemcpyKind kind = device_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-        CK(cudaMemcpy2DAsync(re + (size_t)q * np * nf, row * nq, res, row, row, 9, kind, st));
-        CK(cudaMemcpy2DAsync(im + (size_t)q * np * nf, row * nq, res + blkvals, row, row, 9, kind, st));
-        if (!device_out) ctx->d2h += (long long)(2 * 9 * row);
-        if (epsm) {
-          // eps_M of this q from the (L, L) block: [i=0][j=0] rows of res
-          CK(ctx->epsm.ensure(sizeof(double2) * nf));
-          CK(pmx::dev::launch_epsm(res, res + blkvals, neps, 1, nf, ctx->epsm.as<double2>(), st));
-          ctx->launches += 1;
-          CK(cudaMemcpyAsync(epsm + (size_t)2 * q * nf, ctx->epsm.ptr, sizeof(double2) * nf,
-                             device_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
-          if (!device_out) ctx->d2h += (long long)(sizeof(double2) * nf);
-        }
-      }
+      chi_process_q(ctx, p, pl, dc, q, off, wk, wq, ctx->zk.as<double2>(), ctx->zq.as<double2>(), precision, re,
+                    im, device_out, epsm);
     }
     CK(cudaStreamSynchronize(st));
     if (ctx->degenerate_cuts > 0)
@@ -1629,6 +1681,332 @@ extern "C" int pmx_epsm_vjp(pmx_ctx* ctx, const pmx_problem* P, const double* ch
       }
     }
     adj_finish(ctx, P, dc, grad);
+    return (int)PMX_OK;
+  });
+}
+
+// ======================================================================= batches
+// Several crystals (problems) in merged launches: every eigensolve stage of all
+// problems runs as one assemble + one eigensolver launch per size class
+// (matrices sorted by dimension, classes = the eigensolver's register-slot
+// templates), instead of one launch sequence per problem.
+namespace {
+
+struct DevCrystalSet {
+  std::vector<DevCrystal> dc;  // dc[i].dev points into the shared device table
+  pmx::dev::CrystalDev* table = nullptr;
+};
+
+DevCrystalSet upload_crystals(pmx_ctx* c, const pmx_problem* const* P, int count) {
+  DevCrystalSet set;
+  std::vector<size_t> og(count + 1, 0), ov(count + 1, 0);
+  for (int i = 0; i < count; ++i) {
+    og[i + 1] = og[i] + 3 * (size_t)P[i]->p.npw();
+    ov[i + 1] = ov[i] + P[i]->vloc.size();
+  }
+  CK(c->b_g.ensure(std::max<size_t>(og[count], 2) * sizeof(double)));
+  CK(c->b_hkl.ensure(std::max<size_t>(og[count], 2) * sizeof(int)));
+  CK(c->b_vloc.ensure(std::max<size_t>(ov[count], 2) * sizeof(double)));
+  CK(c->b_vso.ensure(std::max<size_t>(ov[count], 2) * sizeof(double)));
+  CK(c->b_crystal.ensure(std::max(count, 1) * sizeof(pmx::dev::CrystalDev)));
+  std::vector<double> G(og[count]);
+  std::vector<int> H(og[count]);
+  std::vector<pmx::dev::CrystalDev> tab(count);
+  set.table = c->b_crystal.as<pmx::dev::CrystalDev>();
+  set.dc.resize(count);
+  for (int i = 0; i < count; ++i) {
+    const Problem& p = P[i]->p;
+    for (int g = 0; g < p.npw(); ++g)
+      for (int x = 0; x < 3; ++x) {
+        G[og[i] + 3 * g + x] = p.G[g][x];
+        H[og[i] + 3 * g + x] = p.hkl[g][x];
+      }
+    CK(cudaMemcpyAsync(c->b_vloc.as<double>() + ov[i], P[i]->vloc.data(), sizeof(double) * P[i]->vloc.size(),
+                       cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->b_vso.as<double>() + ov[i], P[i]->vso.data(), sizeof(double) * P[i]->vso.size(),
+                       cudaMemcpyHostToDevice, c->stream));
+    c->h2d += (long long)(2 * sizeof(double) * P[i]->vloc.size());
+    pmx::dev::CrystalDev& cd = tab[i];
+    cd.npw = p.npw();
+    cd.soc = P[i]->soc;
+    cd.imax = p.imax;
+    cd.side = 4 * p.imax + 1;
+    const double sc = 2.0 * pmx::kPi / p.lat.a;
+    cd.kin = pmx::kKCON * (sc * sc);
+    cd.G = c->b_g.as<double>() + og[i];
+    cd.hkl = c->b_hkl.as<int>() + og[i];
+    cd.vloc = reinterpret_cast<const double2*>(c->b_vloc.as<double>() + ov[i]);
+    cd.vso = reinterpret_cast<const double2*>(c->b_vso.as<double>() + ov[i]);
+    DevCrystal& d = set.dc[i];
+    d.host = cd;
+    d.dev = set.table + i;
+    d.soc = cd.soc;
+    d.npw = cd.npw;
+    d.n = cd.soc ? 2 * cd.npw : cd.npw;
+  }
+  if (count > 0) {
+    CK(cudaMemcpyAsync(c->b_g.ptr, G.data(), sizeof(double) * G.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->b_hkl.ptr, H.data(), sizeof(int) * H.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->b_crystal.ptr, tab.data(), sizeof(pmx::dev::CrystalDev) * count, cudaMemcpyHostToDevice,
+                       c->stream));
+    // the host staging vectors die with this function
+    CK(cudaStreamSynchronize(c->stream));
+    c->h2d += (long long)(G.size() * sizeof(double) + H.size() * sizeof(int) + tab.size() * sizeof(tab[0]));
+  }
+  return set;
+}
+
+// One eigenproblem of a merged solve.
+struct SolveReq {
+  int crystal;       // index into the crystal table
+  int n, npw;        // matrix dimension and plane waves of that crystal
+  Vec3 k;
+  int nval, nvec;    // lowest eigenvalues / eigenvectors wanted
+  long long z_off;   // double2 offset of the nvec eigenvectors in zbase
+  double* w;         // host destination of the nval eigenvalues
+};
+
+// Register-slot class of the eigensolver template that runs a matrix of size n.
+int heev_class(int n) {
+  const int slots = (n + 31) / 32;
+  const int cls[] = {2, 4, 6, 9, 13, 19, 26, 38};
+  for (int c : cls)
+    if (slots <= c) return c;
+  return 1 << 20;
+}
+
+void solve_multi(pmx_ctx* c, const pmx::dev::CrystalDev* table, std::vector<SolveReq>& reqs, double2* zbase) {
+  if (reqs.empty()) return;
+  std::vector<int> order(reqs.size());
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return reqs[a].n > reqs[b].n; });
+  const size_t hmax = (size_t)2 << 30;
+  size_t i0 = 0;
+  while (i0 < order.size()) {
+    // one chunk: same size class, bounded workspace
+    const int max_n = reqs[order[i0]].n, cls = heev_class(max_n);
+    size_t i1 = i0, hb = 0;
+    while (i1 < order.size() && i1 - i0 < 4096 && heev_class(reqs[order[i1]].n) == cls) {
+      const size_t b = (size_t)reqs[order[i1]].n * reqs[order[i1]].n * sizeof(double2);
+      if (i1 > i0 && hb + b > hmax) break;
+      hb += b;
+      ++i1;
+    }
+    const int cnt = (int)(i1 - i0);
+    std::vector<pmx::dev::EigItem> items(cnt);
+    long long h = 0, w = 0, sc = 0;
+    int max_nval = 1, max_npw = 1;
+    for (int i = 0; i < cnt; ++i) {
+      const SolveReq& r = reqs[order[i0 + i]];
+      if (r.nval > r.n || r.nvec > r.nval) throw CudaFail("too many eigenvalues requested", PMX_ERR_INVALID);
+      pmx::dev::EigItem& it = items[i];
+      it = pmx::dev::EigItem{};
+      it.crystal = r.crystal;
+      it.n = r.n;
+      it.nev = r.nvec;
+      it.nval = r.nval;
+      it.want_vec = r.nvec > 0 ? 1 : 0;
+      for (int x = 0; x < 3; ++x) it.k[x] = r.k[x];
+      it.h_off = h;
+      it.w_off = w;
+      it.z_off = r.z_off;
+      it.s_off = sc;
+      h += (long long)r.n * r.n;
+      w += r.nval;
+      sc += (long long)pmx::dev::heev_scratch_doubles(r.n, r.nvec, max_n);
+      max_nval = std::max(max_nval, r.nval);
+      max_npw = std::max(max_npw, r.npw);
+    }
+    CK(c->hbuf.ensure(sizeof(double2) * (size_t)h));
+    CK(c->wbuf.ensure(sizeof(double) * (size_t)w));
+    CK(c->scratch.ensure(sizeof(double) * (size_t)sc));
+    CK(c->info.ensure(sizeof(int) * cnt));
+    h2d(c, c->items, items.data(), sizeof(pmx::dev::EigItem) * cnt);
+    {
+      KTime kt(c, "assemble");
+      CK(pmx::dev::launch_assemble(table, c->items.as<pmx::dev::EigItem>(), cnt, max_npw, c->hbuf.as<double2>(),
+                                   c->stream));
+    }
+    {
+      KTime kt(c, "heev");
+      CK(pmx::dev::launch_heev(c->items.as<pmx::dev::EigItem>(), cnt, max_n, max_nval, c->hbuf.as<double2>(),
+                               c->wbuf.as<double>(), zbase ? zbase : c->hbuf.as<double2>(), c->scratch.as<double>(),
+                               c->info.as<int>(), c->stream, 0));
+    }
+    c->launches += 2;
+    std::vector<int> info(cnt);
+    std::vector<double> wv((size_t)w);
+    CK(cudaMemcpyAsync(info.data(), c->info.ptr, sizeof(int) * cnt, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(wv.data(), c->wbuf.ptr, sizeof(double) * wv.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->d2h += (long long)(sizeof(int) * cnt + sizeof(double) * wv.size());
+    for (int i = 0; i < cnt; ++i) {
+      if (info[i] != 0)
+        throw CudaFail("eigensolver failed (status " + std::to_string(info[i]) + ")", PMX_ERR_NOCONV);
+      const SolveReq& r = reqs[order[i0 + i]];
+      std::copy(wv.begin() + items[i].w_off, wv.begin() + items[i].w_off + r.nval, r.w);
+    }
+    i0 = i1;
+  }
+}
+
+// Reference energies of every problem in one merged solve (setRefEnergy,
+// src/pmx_epm.cpp:393-428).
+std::vector<double> ref_energies(pmx_ctx* c, const pmx_problem* const* P, int count, const DevCrystalSet& set) {
+  std::vector<double> off(count, 0.0);
+  std::vector<std::vector<double>> w(count);
+  std::vector<SolveReq> reqs;
+  for (int i = 0; i < count; ++i) {
+    const Problem& p = P[i]->p;
+    const int nh = 2 * p.npw();
+    if (!(p.nvalence > 0 && p.nvalence < nh)) {
+      std::cout << "WARNING::setRefEnergy:: nvalence is out of bounds for eigenvalues. Setting offset to 0."
+                << std::endl;
+      continue;
+    }
+    const DevCrystal& d = set.dc[i];
+    const int nev = solved_states(p.nvalence + 1, d.soc);
+    w[i].assign(nev, 0.0);
+    reqs.push_back({i, d.n, d.npw, p.refpoint, nev, 0, 0, w[i].data()});
+  }
+  solve_multi(c, set.table, reqs, nullptr);
+  for (int i = 0; i < count; ++i) {
+    if (w[i].empty()) continue;
+    const Problem& p = P[i]->p;
+    const int soc = set.dc[i].soc, nev = (int)w[i].size();
+    off[i] = (spinor_eig(w[i], nev, 0, p.nvalence - 1, soc) + spinor_eig(w[i], nev, 0, p.nvalence, soc)) / 2.0;
+  }
+  return off;
+}
+
+}  // namespace
+
+extern "C" int pmx_band_batch(pmx_ctx* ctx, int count, const pmx_problem* const* problems, double* const* eband) {
+  if (count < 0 || (count > 0 && (!problems || !eband))) return PMX_ERR_INVALID;
+  for (int i = 0; i < count; ++i)
+    if (!problems[i] || (!eband[i] && problems[i]->p.nq() > 0)) return PMX_ERR_INVALID;
+  return guarded(ctx, [&]() {
+    for (double& t : ctx->stage_ms) t = 0;
+    Timer tm(ctx, 0);
+    const DevCrystalSet set = upload_crystals(ctx, problems, count);
+    const std::vector<double> off = ref_energies(ctx, problems, count, set);
+    std::vector<std::vector<double>> w(count);
+    std::vector<SolveReq> reqs;
+    for (int i = 0; i < count; ++i) {
+      const Problem& p = problems[i]->p;
+      const DevCrystal& d = set.dc[i];
+      const int nkeep = std::min(p.nband, 2 * p.npw());
+      if (nkeep <= 0) continue;
+      const int nev = solved_states(nkeep, d.soc);
+      w[i].assign((size_t)p.nq() * nev, 0.0);
+      for (int q = 0; q < p.nq(); ++q)
+        reqs.push_back({i, d.n, d.npw, p.lat.Q[q], nev, 0, 0, w[i].data() + (size_t)q * nev});
+    }
+    solve_multi(ctx, set.table, reqs, nullptr);
+    for (int i = 0; i < count; ++i) {
+      const Problem& p = problems[i]->p;
+      const int nh = 2 * p.npw(), nkeep = std::min(p.nband, nh);
+      if (nkeep <= 0) {
+        std::fill(eband[i], eband[i] + (size_t)p.nq() * std::max(p.nband, 0), 0.0);
+        continue;
+      }
+      const int nev = solved_states(nkeep, set.dc[i].soc);
+      for (int q = 0; q < p.nq(); ++q)
+        for (int b = 0; b < p.nband; ++b)
+          eband[i][(size_t)q * p.nband + b] = b < nh ? spinor_eig(w[i], nev, q, b, set.dc[i].soc) - off[i] : 0.0;
+    }
+    return (int)PMX_OK;
+  });
+}
+
+extern "C" int pmx_chi_batch(pmx_ctx* ctx, int count, const pmx_problem* const* problems, int sw, int precision,
+                             double* const* re, double* const* im, double* const* epsm) {
+  if (count < 0 || (count > 0 && (!problems || !re || !im))) return PMX_ERR_INVALID;
+  if (sw != PMX_SWITCH_EPSIJ && sw != PMX_SWITCH_EPSLL) return PMX_ERR_INVALID;
+  if (precision != PMX_PREC_FP64 && precision != PMX_PREC_MIXED) return PMX_ERR_INVALID;
+  for (int i = 0; i < count; ++i)
+    if (!problems[i] || !re[i] || !im[i] || (epsm && epsm[i] && problems[i]->p.neps > 64)) return PMX_ERR_INVALID;
+  return guarded(ctx, [&]() -> int {
+    for (double& t : ctx->stage_ms) t = 0;
+    ctx->degenerate_cuts = 0;
+    ctx->m2_err = ctx->m2_max = 0.0;
+    DevCrystalSet set;
+    std::vector<double> off;
+    {
+      Timer tm(ctx, 0);
+      set = upload_crystals(ctx, problems, count);
+      off = ref_energies(ctx, problems, count, set);
+    }
+    std::vector<ChiPlan> pl;
+    for (int i = 0; i < count; ++i) pl.push_back(chi_plan(problems[i]->p, sw, set.dc[i]));
+    // groups of problems whose eigenvectors at k and at k+q (one q) fit the budget
+    const size_t budget = (size_t)16 << 30;
+    int g0 = 0;
+    while (g0 < count) {
+      int g1 = g0;
+      size_t zb = 0;
+      while (g1 < count) {
+        const size_t b = sizeof(double2) * (size_t)pl[g1].nk * pl[g1].nev * pl[g1].n;
+        if (g1 > g0 && zb + b > budget) break;
+        zb += b;
+        ++g1;
+      }
+      std::vector<long long> zo(g1 - g0 + 1, 0);
+      for (int i = g0; i < g1; ++i)
+        zo[i - g0 + 1] = zo[i - g0] + (long long)pl[i].nk * pl[i].nev * pl[i].n;
+      CK(ctx->zk.ensure(std::max<size_t>(sizeof(double2) * (size_t)zo.back(), 16)));
+      CK(ctx->zq.ensure(std::max<size_t>(sizeof(double2) * (size_t)zo.back(), 16)));
+      // k stage of every problem of the group
+      std::vector<std::vector<double>> wk(count);
+      {
+        Timer tm(ctx, 0);
+        std::vector<SolveReq> reqs;
+        for (int i = g0; i < g1; ++i) {
+          const Problem& p = problems[i]->p;
+          const DevCrystal& d = set.dc[i];
+          wk[i].assign((size_t)pl[i].nk * pl[i].nval, 0.0);
+          for (int k = 0; k < pl[i].nk; ++k)
+            reqs.push_back({i, d.n, d.npw, p.K[k], pl[i].nval, pl[i].nev,
+                            zo[i - g0] + (long long)k * pl[i].nev * pl[i].n, wk[i].data() + (size_t)k * pl[i].nval});
+        }
+        solve_multi(ctx, set.table, reqs, ctx->zk.as<double2>());
+      }
+      int maxq = 0;
+      for (int i = g0; i < g1; ++i) maxq = std::max(maxq, pl[i].nq);
+      for (int q = 0; q < maxq; ++q) {
+        // k+q stage of every problem that has this q, then each problem's chi
+        std::vector<std::vector<double>> wq(count);
+        {
+          Timer tm(ctx, 0);
+          std::vector<SolveReq> reqs;
+          for (int i = g0; i < g1; ++i) {
+            if (q >= pl[i].nq) continue;
+            const Problem& p = problems[i]->p;
+            const DevCrystal& d = set.dc[i];
+            wq[i].assign((size_t)pl[i].nk * pl[i].nval, 0.0);
+            for (int k = 0; k < pl[i].nk; ++k)
+              reqs.push_back({i, d.n, d.npw, p.K[k] + p.lat.Q[q], pl[i].nval, pl[i].nev,
+                              zo[i - g0] + (long long)k * pl[i].nev * pl[i].n,
+                              wq[i].data() + (size_t)k * pl[i].nval});
+          }
+          solve_multi(ctx, set.table, reqs, ctx->zq.as<double2>());
+        }
+        for (int i = g0; i < g1; ++i) {
+          if (q >= pl[i].nq) continue;
+          const Problem& p = problems[i]->p;
+          chi_tables(ctx, p);
+          chi_buffers(ctx, pl[i]);
+          chi_process_q(ctx, p, pl[i], set.dc[i], q, off[i], wk[i], wq[i], ctx->zk.as<double2>() + zo[i - g0],
+                        ctx->zq.as<double2>() + zo[i - g0], precision, re[i], im[i], false,
+                        epsm ? epsm[i] : nullptr);
+        }
+      }
+      g0 = g1;
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->degenerate_cuts > 0)
+      std::cerr << "WARNING: the NBAND window cuts a degenerate set at " << ctx->degenerate_cuts
+                << " k / k+q points of the batch (|E_NBAND - E_NBAND+1| < 1e-8 eV)" << std::endl;
     return (int)PMX_OK;
   });
 }

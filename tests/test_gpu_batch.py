@@ -1,0 +1,54 @@
+"""Merged multi-crystal launches (pmx_band_batch, pmx_chi_batch) against the
+per-problem entry points on crystals of uneven size, with and without SOC."""
+import numpy as np
+import pytest
+
+from conftest import golden_args, load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _band_problems():
+    import picomax_b200 as pm
+    from picomax_b200.workloads import gaas_form_factors, workload, wz_form_factors
+    import tempfile
+    vg, soc = gaas_form_factors()
+    tmp = tempfile.mkdtemp()
+    si, _, _ = workload("si_band", tmp)
+    gaas = ["-switch", "band", "-crystal", "zb", "-a", "5.65", "-vg", vg, "-encut", "80", "-nband", "16",
+            "-nvalence", "8", "-qpath", "G,X,L", "-qnum", "7,5"] + soc
+    wz = ["-switch", "band", "-crystal", "wz", "-a", "3.19", "-f", "1.626", "-u", "0.375", "-vg", wz_form_factors(),
+          "-encut", "150", "-nband", "20", "-nvalence", "16", "-qvec", "0,0,0,0.2,0.1,0,0.3,0,0.2"]
+    return [pm.Problem(a) for a in (si, gaas, wz)]
+
+
+def test_band_batch_matches_single(ctx):
+    probs = _band_problems()
+    assert len({p.info.npw for p in probs}) == 3
+    got = ctx.band_batch(probs)
+    for p, g in zip(probs, got):
+        assert np.max(np.abs(g - ctx.band(p))) < 1e-9
+        p.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_chi_batch_matches_single(ctx, tmp_path, precision):
+    import picomax_b200 as pm
+    names = ["si_epsLL", "gaas_soc_epsij", "wz_epsij_rect"]
+    probs, sws = [], []
+    for nm in names:
+        (tmp_path / nm).mkdir(exist_ok=True)
+        args = golden_args(load_golden(nm), tmp_path / nm)
+        probs.append(pm.Problem(args))
+        sws.append(pm.SWITCH_EPSLL if "epsLL" in args else pm.SWITCH_EPSIJ)
+    for sw in (pm.SWITCH_EPSIJ, pm.SWITCH_EPSLL):
+        sel = [p for p, s in zip(probs, sws) if s == sw]
+        got = ctx.chi_batch(sel, sw, precision)
+        for p, (re, im) in zip(sel, got):
+            r0, i0 = ctx.chi(p, sw, precision)
+            scale = max(np.abs(r0).max(), np.abs(i0).max())
+            tol = 1e-9 if precision == 0 else 1e-5
+            assert np.max(np.abs(re - r0)) < tol * scale
+            assert np.max(np.abs(im - i0)) < tol * scale
+    for p in probs:
+        p.close()

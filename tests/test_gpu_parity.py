@@ -98,6 +98,22 @@ def test_heev_all_eigenpairs(ctx, n, nev):
         assert np.max(np.abs(Z[b].conj().T @ Z[b] - np.eye(nev))) < 1e-10
 
 
+@pytest.mark.parametrize("n,nev,vectors", [(900, 16, True), (1200, 8, True), (1000, 24, False)])
+def test_heev_large_n(ctx, n, nev, vectors):
+    """n > 832: the per-warp partial sums of the reduction live in global scratch."""
+    rng = np.random.default_rng(n)
+    A = np.stack([_random_hermitian(rng, n) for _ in range(2)])
+    w, Z = ctx.heev(A, nev, vectors=vectors)
+    for b in range(2):
+        full = np.linalg.eigvalsh(A[b])
+        scale = np.max(np.abs(full))
+        assert np.max(np.abs(w[b] - full[:nev])) < 1e-12 * scale * n
+        if vectors:
+            R = A[b] @ Z[b] - Z[b] * w[b]
+            assert np.max(np.linalg.norm(R, axis=0)) < 1e-10 * scale
+            assert np.max(np.abs(Z[b].conj().T @ Z[b] - np.eye(nev))) < 1e-10
+
+
 def test_kk_vs_oracle(ctx):
     rng = np.random.default_rng(3)
     nf, rows, dw = 300, 7, 0.05

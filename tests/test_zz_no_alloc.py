@@ -69,8 +69,8 @@ def test_noalloc_rejects_sizes_beyond_limit(ctx):
     from picomax_b200 import _capi
     lib = _capi.load()
     d = ctypes.c_void_p(16)  # never dereferenced: the size checks come first
-    assert lib.pmx_heev_batched_noalloc(None, 865, 1, d, 8, d, d, d) == _capi.PMX_ERR_LIMIT
+    assert lib.pmx_heev_batched_noalloc(None, 833, 1, d, 8, d, d, d) == _capi.PMX_ERR_LIMIT
     assert lib.pmx_heev_batched_noalloc(None, 64, 1025, d, 8, d, None, d) == _capi.PMX_ERR_LIMIT
     # 4 n nev batch doubles of inverse-iteration vectors above the scratch
-    assert lib.pmx_heev_batched_noalloc(None, 864, 1000, d, 512, d, d, d) == _capi.PMX_ERR_LIMIT
+    assert lib.pmx_heev_batched_noalloc(None, 832, 1000, d, 512, d, d, d) == _capi.PMX_ERR_LIMIT
     assert lib.pmx_heev_batched_noalloc(None, 64, 2, d, 65, d, d, d) == _capi.PMX_ERR_INVALID
