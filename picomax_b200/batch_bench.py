@@ -1,0 +1,171 @@
+"""Batch of crystals of uneven size: merged launches against one call per crystal.
+
+python -m picomax_b200.batch_bench [--crystals 64] [--grid 4] [--nq 4] [--nfreq 1000] [--precision mixed]
+
+The crystals are drawn from one seed: structure zb / rs / wz, lattice constant
+~ U(4, 6.5) A, atomic form factors ~ U(-0.3, 0.3) Ry on the first |G|^2 shells,
+spin-orbit coupling on for half of them (lambda_S ~ U(0.002, 0.01) Ry uniform,
+lambda_A ~ U(0, 0.005) Ry on the first shells), a plane-wave count N_G drawn in
+[50, 600] (the cutoff is searched per crystal, so H spans 50-1200 with SOC),
+NEPS drawn from {15, 27, 59} (at most N_G), a Gamma-centred grid^3 k-grid and
+a line of nq q-points with |q| from 0.01 to 0.5 (2 pi/a), nfreq frequencies,
+Gaussian broadening 0.1 eV, Kramers-Kronig on.
+
+Two workloads, each timed both ways with CUDA-synchronising calls:
+  band: the 121-point high-symmetry path of every crystal
+        (pmx_band_batch vs pmx_band per crystal), eigensolve k-points/s;
+  chi:  eps_M spectra of every (crystal, q) (pmx_chi_batch vs pmx_chi per
+        crystal), spectra/s.
+One JSON line per workload goes to stdout.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+from . import _capi as C
+from .kgrid import make_kfile
+
+
+def _fmt(xs):
+    return ",".join(f"{float(x):.6f}" for x in xs)
+
+
+def _shells(crystal: str, f: float, count: int):
+    if crystal in ("zb", "rs"):
+        return np.array([3.0, 4.0, 8.0, 11.0, 12.0, 16.0][:count])
+    s3 = math.sqrt(3.0)
+    b = np.array([[1, -1 / s3, 0], [1, 1 / s3, 0], [0, 0, 1.0 / f]])
+    r3 = np.arange(-3, 4)
+    hkl = np.array(np.meshgrid(r3, r3, r3, indexing="ij")).reshape(3, -1).T
+    return np.unique(np.round(((hkl @ b) ** 2).sum(1), 6))[1:1 + count]
+
+
+def crystal_args(i: int, rng: np.random.Generator):
+    """Structure options (no switch, no cutoff) and the target N_G of crystal i."""
+    kind = ("zb", "rs", "wz")[rng.integers(3)]
+    a = rng.uniform(4.0, 6.5)
+    f, u = 1.626, 0.375
+    natom = 4 if kind == "wz" else 2
+    nsh = 5 if kind == "wz" else 4
+    keys = _shells(kind, f, nsh)
+    v = rng.uniform(-0.3, 0.3, (natom, nsh))
+    args = ["-crystal", kind, "-a", f"{a:.4f}"]
+    if kind == "wz":
+        args += ["-f", str(f), "-u", str(u)]
+    args += ["-vg", _fmt(keys) + "," + ",".join(_fmt(row) for row in v)]
+    soc = i % 2 == 1
+    if soc:
+        args += ["-use_uniform_us_so", "-uniform_us_so_val", f"{rng.uniform(0.002, 0.01):.6f}",
+                 "-ua_so", ",".join(f"{k:.6f}:{x:.6f}" for k, x in zip(keys[:3], rng.uniform(0, 0.005, 3)))]
+    nval, nband = (16, 24) if kind == "wz" else (8, 16)
+    args += ["-nvalence", str(nval), "-nband", str(nband)]
+    return kind, f, args, int(rng.integers(50, 601)), soc
+
+
+def encut_for(args, target: int) -> float:
+    """Largest cutoff (eV, 0.5 eV steps) giving at most `target` plane waves."""
+    lo, hi = 1.0, 4000.0
+
+    def npw(e):
+        p = C.Problem(["-switch", "band", "-qvec", "0,0,0", "-encut", f"{e:.1f}"] + args)
+        n = p.info.npw
+        p.close()
+        return n
+    while hi - lo > 0.5:
+        mid = 0.5 * (lo + hi)
+        if npw(mid) <= target:
+            lo = mid
+        else:
+            hi = mid
+    return lo
+
+
+def build(ncrystal: int, grid: int, nq: int, nfreq: int, workdir: str, seed: int = 4242):
+    rng = np.random.default_rng(seed)
+    band, chi, meta = [], [], []
+    qs = np.linspace(0.01, 0.5, nq) if nq > 1 else np.array([0.01])
+    qvec = ",".join(f"{x:.6f},0,0" for x in qs)
+    for i in range(ncrystal):
+        kind, f, args, target, soc = crystal_args(i, rng)
+        encut = encut_for(args, target)
+        base = args + ["-encut", f"{encut:.1f}"]
+        path = "G,A,H,K,G" if kind == "wz" else "G,X,W,L,G"
+        band.append(C.Problem(["-switch", "band", "-qpath", path, "-qnum", "30,30,30,30"] + base))
+        npw = band[-1].info.npw
+        neps = int(min(rng.choice([15, 27, 59]), npw))
+        kf = os.path.join(workdir, f"k_{i}.txt")
+        make_kfile(kf, "zb" if kind == "rs" else kind, grid, grid, grid, f=f)
+        chi.append(C.Problem(["-switch", "epsLL", "-kpoint", "0", "-kpointfile", kf, "-qvec", qvec, "-neps",
+                              str(neps), "-nfreq", str(nfreq), "-dfreq", f"{25.0 / nfreq:.6f}", "-delta", "0",
+                              "-epsilon", "0.1", "-kk", "1"] + base))
+        meta.append({"kind": kind, "soc": soc, "npw": npw, "nh": 2 * npw if soc else npw, "neps": neps})
+    return band, chi, meta
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--crystals", type=int, default=64)
+    ap.add_argument("--grid", type=int, default=4)
+    ap.add_argument("--nq", type=int, default=4)
+    ap.add_argument("--nfreq", type=int, default=1000)
+    ap.add_argument("--precision", choices=("fp64", "mixed"), default="mixed")
+    ap.add_argument("--repeat", type=int, default=2)
+    a = ap.parse_args(argv)
+    prec = C.PREC_MIXED if a.precision == "mixed" else C.PREC_FP64
+    tmp = tempfile.mkdtemp()
+    t0 = time.perf_counter()
+    band, chi, meta = build(a.crystals, a.grid, a.nq, a.nfreq, tmp)
+    t_setup = time.perf_counter() - t0
+    ctx = C.Context(0)
+    nh = [m["nh"] for m in meta]
+    # warm-up (module loading, autotuning of the per-crystal path)
+    ctx.band_batch(band[:2])
+    for p in band[:2]:
+        ctx.band(p)
+
+    def timed(fn):
+        best = float("inf")
+        out = None
+        for _ in range(a.repeat):
+            t = time.perf_counter()
+            out = fn()
+            best = min(best, time.perf_counter() - t)
+        return best, out
+
+    tb, eb = timed(lambda: ctx.band_batch(band))
+    tl, el = timed(lambda: [ctx.band(p) for p in band])
+    diff = max(float(np.abs(x - y).max()) for x, y in zip(eb, el))
+    nk_band = sum(p.info.nq for p in band) + len(band)
+    print(json.dumps({"workload": "band", "crystals": len(band), "nh_min": min(nh), "nh_max": max(nh),
+                      "solves": nk_band, "batch_s": tb, "per_crystal_s": tl, "batch_kpts_per_s": nk_band / tb,
+                      "per_crystal_kpts_per_s": nk_band / tl, "speedup": tl / tb, "max_abs_diff_eV": diff,
+                      "setup_s": t_setup}), flush=True)
+
+    tb, cb = timed(lambda: ctx.chi_batch(chi, C.SWITCH_EPSLL, prec, epsm=True))
+    tl, cl = timed(lambda: [ctx.chi_epsm(p, C.SWITCH_EPSLL, prec) for p in chi])
+    rel = 0.0
+    for (r0, i0, e0), (r1, i1, e1) in zip(cb, cl):
+        rel = max(rel, float(np.abs(e0 - e1).max() / np.abs(e1).max()))
+    spectra = sum(p.info.nq for p in chi)
+    solves = sum(p.info.nk * (1 + p.info.nq) + 1 for p in chi)
+    print(json.dumps({"workload": "chi_epsLL", "precision": a.precision, "crystals": len(chi), "grid": a.grid,
+                      "nq": a.nq, "nfreq": a.nfreq, "spectra": spectra, "solves": solves, "batch_s": tb,
+                      "per_crystal_s": tl, "batch_spectra_per_s": spectra / tb,
+                      "per_crystal_spectra_per_s": spectra / tl, "speedup": tl / tb,
+                      "max_rel_diff_epsM": rel, "neps": sorted({m["neps"] for m in meta})}), flush=True)
+    for p in band + chi:
+        p.close()
+    ctx.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

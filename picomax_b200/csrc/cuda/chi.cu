@@ -29,27 +29,32 @@ namespace dev {
 __global__ void __launch_bounds__(256) overlap_kernel(OverlapArgs a) {
   const int k = blockIdx.x;
   const int ncd = a.ncd[k], nvd = a.nvd[k];
-  const int c_lo = blockIdx.y * a.cchunk;
+  // blockIdx.y = (conduction chunk) + ncc * (valence chunk)
+  const int ncc = (a.ncd_max + a.cchunk - 1) / a.cchunk;
+  const int c_lo = (blockIdx.y % ncc) * a.cchunk;
   const int c_hi = min(ncd, c_lo + a.cchunk);
-  if (c_lo >= c_hi || nvd <= 0) return;
+  const int v_lo = (blockIdx.y / ncc) * a.vchunk;
+  const int v_hi = min(nvd, v_lo + a.vchunk);
+  if (c_lo >= c_hi || v_lo >= v_hi) return;
+  const int nvl = v_hi - v_lo;
   const int n = a.n, npw = a.npw;
   extern __shared__ __align__(16) unsigned char smraw[];
   double2* sc = reinterpret_cast<double2*>(smraw);          // [cchunk][n]
-  double2* sv = sc + (size_t)a.cchunk * n;                   // [nvd_max][n]
-  double* sg = reinterpret_cast<double*>(sv + (size_t)a.nvd_max * n);  // [npw][3]
+  double2* sv = sc + (size_t)a.cchunk * n;                   // [vchunk][n]
+  double* sg = reinterpret_cast<double*>(sv + (size_t)a.vchunk * n);  // [npw][3]
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
   for (int c = c_lo; c < c_hi; ++c) {
     const double2* src = a.zk + ((size_t)k * a.nev + a.cidx[a.cbase[k] + c]) * n;
     for (int r = tid; r < n; r += blockDim.x) sc[(size_t)(c - c_lo) * n + r] = src[r];
   }
-  for (int v = 0; v < nvd; ++v) {
+  for (int v = v_lo; v < v_hi; ++v) {
     const double2* src = a.zq + ((size_t)k * a.nev + a.vidx[a.vbase[k] + v]) * n;
-    for (int r = tid; r < n; r += blockDim.x) sv[(size_t)v * n + r] = src[r];
+    for (int r = tid; r < n; r += blockDim.x) sv[(size_t)(v - v_lo) * n + r] = src[r];
   }
   for (int r = tid; r < 3 * npw; r += blockDim.x) sg[r] = a.G[r];
   __syncthreads();
   const double kx = a.kpts[3 * k], ky = a.kpts[3 * k + 1], kz = a.kpts[3 * k + 2];
-  const int npair = (c_hi - c_lo) * nvd;
+  const int npair = (c_hi - c_lo) * nvl;
   const int A = 3 * a.neps;
   for (int m = 0; m < a.neps; ++m) {
     const int* loci = a.loci + (size_t)m * npw;
@@ -58,9 +63,9 @@ __global__ void __launch_bounds__(256) overlap_kernel(OverlapArgs a) {
     const double wy = (ky + a.q[1] / 2) + a.G[3 * m + 1] / 2;
     const double wz = (kz + a.q[2] / 2) + a.G[3 * m + 2] / 2;
     for (int pr = wid; pr < npair; pr += nw) {
-      const int cl = pr / nvd, v = pr % nvd;
+      const int cl = pr / nvl, v = v_lo + pr % nvl;
       const double2* cvec = sc + (size_t)cl * n;
-      const double2* vvec = sv + (size_t)v * n;
+      const double2* vvec = sv + (size_t)(v - v_lo) * n;
       // moments: [0..3] spin-summed or up-up, [4..7] down-down, [8] up-down, [9] down-up
       double2 mo[10];
 #pragma unroll
@@ -133,17 +138,27 @@ __global__ void __launch_bounds__(256) overlap_kernel(OverlapArgs a) {
 
 cudaError_t launch_overlap(const OverlapArgs& a, int nk, cudaStream_t st) {
   if (nk <= 0) return cudaSuccess;
-  const size_t smem = ((size_t)a.cchunk * a.n + (size_t)a.nvd_max * a.n) * sizeof(double2) +
-                      (size_t)3 * a.npw * sizeof(double);
+  if (a.cchunk < 1 || a.vchunk < 1) return cudaErrorInvalidValue;
+  const size_t smem = overlap_smem_bytes(a.cchunk, a.vchunk, a.n, a.npw);
   cudaError_t err = cudaFuncSetAttribute(overlap_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
-  dim3 grid(nk, (a.ncd_max + a.cchunk - 1) / a.cchunk);
+  const int ncc = (a.ncd_max + a.cchunk - 1) / a.cchunk, nvc = (a.nvd_max + a.vchunk - 1) / a.vchunk;
+  dim3 grid(nk, ncc * nvc);
   overlap_kernel<<<grid, 256, smem, st>>>(a);
   return cudaGetLastError();
 }
 
-size_t overlap_smem_bytes(int cchunk, int nvd_max, int n, int npw) {
-  return ((size_t)cchunk * n + (size_t)nvd_max * n) * sizeof(double2) + (size_t)3 * npw * sizeof(double);
+size_t overlap_smem_bytes(int cchunk, int vchunk, int n, int npw) {
+  return ((size_t)cchunk * n + (size_t)vchunk * n) * sizeof(double2) + (size_t)3 * npw * sizeof(double);
+}
+
+bool overlap_tiles(int ncd_max, int nvd_max, int n, int npw, int& cchunk, int& vchunk) {
+  const size_t lim = 200 * 1024;
+  vchunk = std::max(1, nvd_max);
+  cchunk = std::max(1, ncd_max);
+  while (cchunk > 1 && overlap_smem_bytes(cchunk, vchunk, n, npw) > lim) --cchunk;
+  while (vchunk > 1 && overlap_smem_bytes(cchunk, vchunk, n, npw) > lim) --vchunk;
+  return overlap_smem_bytes(cchunk, vchunk, n, npw) <= lim;
 }
 
 // ------------------------------------------------------------ broadening

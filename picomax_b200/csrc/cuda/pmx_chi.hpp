@@ -17,6 +17,7 @@ struct OverlapArgs {
   int nch;          // 1 or 4 output channels
   int mode;         // 0 epsij, 1 epsLL
   int cchunk;       // conduction states per CTA
+  int vchunk;       // valence states per CTA
   int ncd_max, nvd_max;
   const double2* zk;      // [nk][nev][n] eigenvectors at k
   const double2* zq;      // [nk][nev][n] eigenvectors at k+q
@@ -65,7 +66,10 @@ struct ScaleArgs {
 };
 
 cudaError_t launch_overlap(const OverlapArgs& a, int nk, cudaStream_t st);
-size_t overlap_smem_bytes(int cchunk, int nvd_max, int n, int npw);
+size_t overlap_smem_bytes(int cchunk, int vchunk, int n, int npw);
+// Largest conduction / valence chunks whose staged eigenvectors fit 200 KB of
+// shared memory; false when even one of each does not fit.
+bool overlap_tiles(int ncd_max, int nvd_max, int n, int npw, int& cchunk, int& vchunk);
 cudaError_t launch_contract_f64(const ContractArgs& a, cudaStream_t st);
 int contract_ftile();
 cudaError_t launch_scale(const ScaleArgs& s, cudaStream_t st);

@@ -897,11 +897,8 @@ void chi_process_q(pmx_ctx* ctx, const Problem& p, const ChiPlan& pl, const DevC
     oa.mode = mode;
     oa.ncd_max = *std::max_element(T.ncd.begin(), T.ncd.end());
     oa.nvd_max = *std::max_element(T.nvd.begin(), T.nvd.end());
-    int cchunk = std::max(1, oa.ncd_max);
-    while (cchunk > 1 && pmx::dev::overlap_smem_bytes(cchunk, oa.nvd_max, n, dc.npw) > 200 * 1024) --cchunk;
-    if (pmx::dev::overlap_smem_bytes(cchunk, oa.nvd_max, n, dc.npw) > 220 * 1024)
+    if (!pmx::dev::overlap_tiles(oa.ncd_max, oa.nvd_max, n, dc.npw, oa.cchunk, oa.vchunk))
       throw CudaFail("overlap tile does not fit in shared memory", PMX_ERR_UNSUPPORTED);
-    oa.cchunk = cchunk;
     oa.zk = zk;
     oa.zq = zq;
     oa.ncd = ctx->ncd.as<int>();
@@ -1552,11 +1549,8 @@ extern "C" int pmx_epsm_vjp(pmx_ctx* ctx, const pmx_problem* P, const double* ch
             oa.mode = 1;
             oa.ncd_max = ncd_max;
             oa.nvd_max = nvd_max;
-            int cchunk = std::max(1, ncd_max);
-            while (cchunk > 1 && pmx::dev::overlap_smem_bytes(cchunk, nvd_max, n, npw) > 200 * 1024) --cchunk;
-            if (pmx::dev::overlap_smem_bytes(cchunk, nvd_max, n, npw) > 220 * 1024)
+            if (!pmx::dev::overlap_tiles(ncd_max, nvd_max, n, npw, oa.cchunk, oa.vchunk))
               throw CudaFail("overlap tile does not fit in shared memory", PMX_ERR_UNSUPPORTED);
-            oa.cchunk = cchunk;
             oa.zk = ctx->zk.as<double2>();
             oa.zq = ctx->zq.as<double2>();
             oa.ncd = ctx->ncd.as<int>();
