@@ -17,6 +17,7 @@
 // the tridiagonal eigenvectors, then the back-transform by the stored
 // reflectors. Only the eigenpairs the caller needs are formed.
 #include <cfloat>
+#include <algorithm>
 #include <cmath>
 
 #include "pmx_common.cuh"
@@ -306,6 +307,8 @@ __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, do
         double2* cc = acc.col(c);
         const double2 vc = vcur[c];
         const double2 wcc = cconj(wprev[c]), vcc = cconj(vprev[c]);
+        // slots wholly above the diagonal (rows < c) or below the matrix are
+        // skipped with warp-uniform branches, not predicated
         double2 a[MAXS];
         if (RING > 0) {
           cp_async_wait<(RING > 0 ? RING - 1 : 0)>();
@@ -313,18 +316,21 @@ __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, do
 #pragma unroll
           for (int s = 0; s < MAXS; ++s) {
             const int r = 32 * s + lane;
-            a[s] = (r >= c && r < n) ? buf[32 * s + lane] : make_double2(0, 0);
+            a[s] = make_double2(0, 0);
+            if (32 * s + 31 >= c && 32 * s < n && r >= c && r < n) a[s] = buf[32 * s + lane];
           }
         } else {
 #pragma unroll
           for (int s = 0; s < MAXS; ++s) {
             const int r = 32 * s + lane;
-            a[s] = (r >= c && r < n) ? cc[r - c] : make_double2(0, 0);
+            a[s] = make_double2(0, 0);
+            if (32 * s + 31 >= c && 32 * s < n && r >= c && r < n) a[s] = cc[r - c];
           }
         }
         double2 dot = make_double2(0, 0);
 #pragma unroll
         for (int s = 0; s < MAXS; ++s) {
+          if (32 * s + 31 < c || 32 * s >= n) continue;  // warp-uniform
           const int r = 32 * s + lane;
           if (r >= c && r < n) {
             double2 v = a[s];
@@ -399,8 +405,10 @@ __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, do
   __syncthreads();
 }
 
-template <bool RESIDENT, int MAXS, int RING>
-__global__ void __launch_bounds__(kHeevThreads, (RING >= 2 || MAXS > 9) ? 1 : 2) heev_kernel(const EigItem* __restrict__ items,
+// OCC > 0 overrides the minimum number of resident CTAs per SM the register
+// allocation is sized for.
+template <bool RESIDENT, int MAXS, int RING, int OCC = 0>
+__global__ void __launch_bounds__(kHeevThreads, OCC > 0 ? OCC : ((RING >= 2 || MAXS > 9) ? 1 : 2)) heev_kernel(const EigItem* __restrict__ items,
                                                                double2* __restrict__ hbuf,
                                                                double* __restrict__ wbuf,
                                                                double2* __restrict__ zbuf,
@@ -633,13 +641,13 @@ int heev_smem_max_n() {
 }
 
 namespace {
-template <bool RES, int MAXS, int RING>
+template <bool RES, int MAXS, int RING, int OCC = 0>
 cudaError_t heev_launch_t(const EigItem* items, int nitems, size_t smem, double2* hbuf, double* wbuf,
                           double2* zbuf, double* scratch, int* info, cudaStream_t st) {
-  cudaError_t err =
-      cudaFuncSetAttribute(heev_kernel<RES, MAXS, RING>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t err = cudaFuncSetAttribute(heev_kernel<RES, MAXS, RING, OCC>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
-  heev_kernel<RES, MAXS, RING><<<nitems, kHeevThreads, smem, st>>>(items, hbuf, wbuf, zbuf, scratch, info);
+  heev_kernel<RES, MAXS, RING, OCC><<<nitems, kHeevThreads, smem, st>>>(items, hbuf, wbuf, zbuf, scratch, info);
   return cudaGetLastError();
 }
 }  // namespace
@@ -647,13 +655,13 @@ cudaError_t heev_launch_t(const EigItem* items, int nitems, size_t smem, double2
 int heev_variants(int max_n, int max_nev) {
   const int slots = (max_n + 31) / 32;
   if (max_n <= heev_smem_max_n() && heev_resident(max_n, max_nev)) return 1;  // resident: one variant
-  if (slots > 13) return 1;
+  if (slots > 13) return 1;  // one CTA per SM already
   // the prefetch rings only count while their shared memory fits the opt-in limit
   const int maxs = slots <= 2 ? 2 : slots <= 4 ? 4 : slots <= 6 ? 6 : slots <= 9 ? 9 : 13;
   const size_t lim = 227 * 1024;
-  if (heev_smem_bytes(max_n, max_nev, false, maxs, 1) > lim) return 1;
-  if (heev_smem_bytes(max_n, max_nev, false, maxs, 3) > lim) return 2;
-  return 3;
+  if (heev_smem_bytes(max_n, max_nev, false, maxs, 1) > lim) return 2;
+  if (heev_smem_bytes(max_n, max_nev, false, maxs, 3) > lim) return 3;
+  return 4;
 }
 
 cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev, double2* hbuf,
@@ -661,9 +669,11 @@ cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev
   if (nitems <= 0) return cudaSuccess;
   const bool resident = max_n <= heev_smem_max_n() && heev_resident(max_n, max_nev);
   const int slots = (max_n + 31) / 32;
-  // global-memory path variants: 0 = direct L2 loads (2 CTAs/SM), 1 = one-column
-  // prefetch buffer per warp (2 CTAs/SM), 2 = three-column ring (1 CTA/SM)
-  const int ring = resident ? 0 : (variant == 1 ? 1 : (variant == 2 ? 3 : 0));
+  // global-memory path variants: 0 = direct L2 loads (2 CTAs/SM); 1 = the same
+  // with registers capped for 3 CTAs/SM (more warps in flight; n <= 288);
+  // 2 = one-column prefetch buffer per warp; 3 = three-column ring (1 CTA/SM)
+  const int ring = resident ? 0 : (variant == 2 ? 1 : (variant == 3 ? 3 : 0));
+  const bool occ3 = !resident && variant == 1;
 #define PMX_HEEV(S)                                                                                          \
   if (slots <= S) {                                                                                          \
     if (resident)                                                                                            \
@@ -677,6 +687,10 @@ cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev
       return heev_launch_t<false, S, (S <= 13 ? 1 : 0)>(items, nitems,                                        \
                                                         heev_smem_bytes(max_n, max_nev, false, S, 1), hbuf,   \
                                                         wbuf, zbuf, scratch, info, st);                      \
+    if (occ3 && S <= 9)                                                                                      \
+      return heev_launch_t<false, S, 0, (S <= 9 ? 3 : 0)>(items, nitems,                                      \
+                                                          heev_smem_bytes(max_n, max_nev, false, S, 0), hbuf, \
+                                                          wbuf, zbuf, scratch, info, st);                    \
     return heev_launch_t<false, S, 0>(items, nitems, heev_smem_bytes(max_n, max_nev, false, S, 0), hbuf, wbuf, \
                                       zbuf, scratch, info, st);                                              \
   }
