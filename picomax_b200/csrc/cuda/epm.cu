@@ -405,10 +405,8 @@ __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, do
   __syncthreads();
 }
 
-// OCC > 0 overrides the minimum number of resident CTAs per SM the register
-// allocation is sized for.
-template <bool RESIDENT, int MAXS, int RING, int OCC = 0>
-__global__ void __launch_bounds__(kHeevThreads, OCC > 0 ? OCC : ((RING >= 2 || MAXS > 9) ? 1 : 2)) heev_kernel(const EigItem* __restrict__ items,
+template <bool RESIDENT, int MAXS, int RING>
+__global__ void __launch_bounds__(kHeevThreads, (RING >= 2 || MAXS > 9) ? 1 : 2) heev_kernel(const EigItem* __restrict__ items,
                                                                double2* __restrict__ hbuf,
                                                                double* __restrict__ wbuf,
                                                                double2* __restrict__ zbuf,
@@ -641,13 +639,13 @@ int heev_smem_max_n() {
 }
 
 namespace {
-template <bool RES, int MAXS, int RING, int OCC = 0>
+template <bool RES, int MAXS, int RING>
 cudaError_t heev_launch_t(const EigItem* items, int nitems, size_t smem, double2* hbuf, double* wbuf,
                           double2* zbuf, double* scratch, int* info, cudaStream_t st) {
-  cudaError_t err = cudaFuncSetAttribute(heev_kernel<RES, MAXS, RING, OCC>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t err =
+      cudaFuncSetAttribute(heev_kernel<RES, MAXS, RING>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
-  heev_kernel<RES, MAXS, RING, OCC><<<nitems, kHeevThreads, smem, st>>>(items, hbuf, wbuf, zbuf, scratch, info);
+  heev_kernel<RES, MAXS, RING><<<nitems, kHeevThreads, smem, st>>>(items, hbuf, wbuf, zbuf, scratch, info);
   return cudaGetLastError();
 }
 }  // namespace
@@ -659,9 +657,9 @@ int heev_variants(int max_n, int max_nev) {
   // the prefetch rings only count while their shared memory fits the opt-in limit
   const int maxs = slots <= 2 ? 2 : slots <= 4 ? 4 : slots <= 6 ? 6 : slots <= 9 ? 9 : 13;
   const size_t lim = 227 * 1024;
-  if (heev_smem_bytes(max_n, max_nev, false, maxs, 1) > lim) return 2;
-  if (heev_smem_bytes(max_n, max_nev, false, maxs, 3) > lim) return 3;
-  return 4;
+  if (heev_smem_bytes(max_n, max_nev, false, maxs, 1) > lim) return 1;
+  if (heev_smem_bytes(max_n, max_nev, false, maxs, 3) > lim) return 2;
+  return 3;
 }
 
 cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev, double2* hbuf,
@@ -669,11 +667,14 @@ cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev
   if (nitems <= 0) return cudaSuccess;
   const bool resident = max_n <= heev_smem_max_n() && heev_resident(max_n, max_nev);
   const int slots = (max_n + 31) / 32;
-  // global-memory path variants: 0 = direct L2 loads (2 CTAs/SM); 1 = the same
-  // with registers capped for 3 CTAs/SM (more warps in flight; n <= 288);
-  // 2 = one-column prefetch buffer per warp; 3 = three-column ring (1 CTA/SM)
-  const int ring = resident ? 0 : (variant == 2 ? 1 : (variant == 3 ? 3 : 0));
-  const bool occ3 = !resident && variant == 1;
+  // global-memory path variants: 0 = direct L2 loads (2 CTAs/SM), 1 = one-column
+  // prefetch buffer per warp (2 CTAs/SM), 2 = three-column ring (1 CTA/SM).
+  // Measured on n = 274 (B200): 82 / 95 / 108 ms per 1787 matrices; a
+  // one-CTA-per-SM padding of schedule 0 (L2-resident trailing blocks), a
+  // register cap for 3 CTAs/SM and a two-columns-per-iteration pass were
+  // slower still (120 / 106 / 97 ms): the pass is bound by dependent FP64
+  // chains and load latency at 16 warps per SM.
+  const int ring = resident ? 0 : (variant == 1 ? 1 : (variant == 2 ? 3 : 0));
 #define PMX_HEEV(S)                                                                                          \
   if (slots <= S) {                                                                                          \
     if (resident)                                                                                            \
@@ -687,10 +688,6 @@ cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev
       return heev_launch_t<false, S, (S <= 13 ? 1 : 0)>(items, nitems,                                        \
                                                         heev_smem_bytes(max_n, max_nev, false, S, 1), hbuf,   \
                                                         wbuf, zbuf, scratch, info, st);                      \
-    if (occ3 && S <= 9)                                                                                      \
-      return heev_launch_t<false, S, 0, (S <= 9 ? 3 : 0)>(items, nitems,                                      \
-                                                          heev_smem_bytes(max_n, max_nev, false, S, 0), hbuf, \
-                                                          wbuf, zbuf, scratch, info, st);                    \
     return heev_launch_t<false, S, 0>(items, nitems, heev_smem_bytes(max_n, max_nev, false, S, 0), hbuf, wbuf, \
                                       zbuf, scratch, info, st);                                              \
   }
