@@ -123,6 +123,11 @@ int pmx_ctx_transfer_bytes(const pmx_ctx* ctx, long long* h2d_bytes, long long* 
  * result depends on its eigensolver's basis inside the set; a warning is
  * printed on stderr. No reference counterpart (new diagnostic). */
 int pmx_ctx_degenerate_cuts(const pmx_ctx* ctx);
+/* k and k+q points of the last pmx_chi* call with a state of the NBAND window
+ * within 1e-8 eV of the reference energy (metals): the occupation test
+ * E - E_ref > 0 of src/pmx_chi.cpp:391-397 is then decided by rounding, for the
+ * reference as for this library; a warning is printed. No reference counterpart. */
+int pmx_ctx_occupation_ties(const pmx_ctx* ctx);
 
 /* ---------------------------------------------------------------- stage 1 */
 

@@ -46,6 +46,7 @@ EXPORTS = (
     "pmx_epsm_vjp",
     "pmx_band_batch",
     "pmx_chi_batch",
+    "pmx_ctx_occupation_ties",
 )
 
 
@@ -102,6 +103,7 @@ def load() -> ctypes.CDLL:
         "pmx_ctx_stream": (c_void_p, [c_void_p]),
         "pmx_ctx_transfer_bytes": (c_int, [c_void_p, POINTER(c_longlong), POINTER(c_longlong)]),
         "pmx_ctx_degenerate_cuts": (c_int, [c_void_p]),
+        "pmx_ctx_occupation_ties": (c_int, [c_void_p]),
         "pmx_chi_device": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p]),
         "pmx_chi_epsm": (c_int, [c_void_p, c_void_p, c_int, c_int, dp, dp, dp]),
         "pmx_eps_macroscopic": (c_int, [c_void_p, c_int, c_int, c_int, dp, dp, dp]),
@@ -315,6 +317,9 @@ class Context:
 
     def degenerate_cuts(self) -> int:
         return int(self._lib.pmx_ctx_degenerate_cuts(self.handle))
+
+    def occupation_ties(self) -> int:
+        return int(self._lib.pmx_ctx_occupation_ties(self.handle))
 
     def chi_epsm(self, prob: Problem, switch: int, precision: int = PREC_FP64):
         n = prob.info.chi_values

@@ -239,6 +239,7 @@ struct pmx_ctx {
   long long launches = 0;
   long long h2d = 0, d2h = 0;  // bytes copied by the library since creation
   int degenerate_cuts = 0;     // k-points of the last chi call whose NBAND window cut a degenerate set
+  int occupation_ties = 0;     // k-points of the last chi call with a window state within 1e-8 eV of E_ref
   // per kernel family: device time (CUDA events around the launches) and launches
   std::map<std::string, std::pair<double, long long>> ktime;
   std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> kpending;
@@ -664,7 +665,7 @@ struct Transitions {
 // then count from k0).
 Transitions build_transitions(const Problem& p, int soc, int nval, const std::vector<double>& wk,
                               const std::vector<double>& wq, double off, bool sort_by_window, int& cuts,
-                              int k0 = 0, int k1 = -1) {
+                              int k0 = 0, int k1 = -1, int* ties = nullptr) {
   Transitions T;
   if (k1 < 0) k1 = p.nk();
   const int nk = k1 - k0, NB = p.nband;
@@ -688,6 +689,15 @@ Transitions build_transitions(const Problem& p, int soc, int nval, const std::ve
       const bool cut_k = std::abs(spinor_eig(wk, nval, k, NB, soc) - spinor_eig(wk, nval, k, NB - 1, soc)) < 1e-8;
       const bool cut_q = std::abs(spinor_eig(wq, nval, k, NB, soc) - spinor_eig(wq, nval, k, NB - 1, soc)) < 1e-8;
       cuts += (int)cut_k + (int)cut_q;
+    }
+    if (ties) {
+      // a state of the window within 1e-8 eV of E_ref: its occupation is decided by rounding
+      bool tk = false, tq = false;
+      for (int s = 0; s < NB && s < nh; ++s) {
+        tk |= std::abs(spinor_eig(wk, nval, k, s, soc) - off) < 1e-8;
+        tq |= std::abs(spinor_eig(wq, nval, k, s, soc) - off) < 1e-8;
+      }
+      *ties += (int)tk + (int)tq;
     }
     int nc = 0, nv = 0;
     while (nc < NB && spinor_eig(wk, nval, k, NB - 1 - nc, soc) - off > 0) ++nc;
@@ -835,7 +845,8 @@ void chi_process_q(pmx_ctx* ctx, const Problem& p, const ChiPlan& pl, const DevC
   const bool pv = pl.pv;
   pmx::dev::ScaleArgs sa = pl.sa;
   const Vec3 Q = p.lat.Q[q];
-  Transitions T = build_transitions(p, dc.soc, nval, wk, wq, off, mode == 0, ctx->degenerate_cuts);
+  Transitions T = build_transitions(p, dc.soc, nval, wk, wq, off, mode == 0, ctx->degenerate_cuts, 0, -1,
+                                    &ctx->occupation_ties);
   // per-m polarisation and SOC-current tables
   std::vector<double2> uv((size_t)neps * 9), ss((size_t)neps * 3);
   std::vector<double> qg(neps);
@@ -1023,6 +1034,7 @@ static int run_chi(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision, do
     const ChiPlan pl = chi_plan(p, sw, dc);
     const int nk = pl.nk, nev = pl.nev, nval = pl.nval, n = pl.n;
     ctx->degenerate_cuts = 0;
+    ctx->occupation_ties = 0;
     ctx->m2_err = ctx->m2_max = 0.0;
     CK(ctx->zk.ensure(std::max<size_t>(sizeof(double2) * (size_t)nk * nev * n, 16)));
     CK(ctx->zq.ensure(std::max<size_t>(sizeof(double2) * (size_t)nk * nev * n, 16)));
@@ -1049,6 +1061,11 @@ static int run_chi(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision, do
       std::cerr << "WARNING: -nband " << p.nband << " cuts a degenerate set at " << ctx->degenerate_cuts
                 << " k / k+q points (|E_NBAND - E_NBAND+1| < 1e-8 eV); chi then depends on the eigenvector "
                    "basis inside that set, for the reference's eigensolver as for this one"
+                << std::endl;
+    if (ctx->occupation_ties > 0)
+      std::cerr << "WARNING: " << ctx->occupation_ties
+                << " k / k+q points have a state within 1e-8 eV of the reference energy; their occupation "
+                   "(E - E_ref > 0 or <= 0) and so chi are decided by rounding"
                 << std::endl;
     return (int)PMX_OK;
   });
@@ -1085,6 +1102,8 @@ extern "C" int pmx_ctx_transfer_bytes(const pmx_ctx* c, long long* h2d_bytes, lo
   if (d2h_bytes) *d2h_bytes = c->d2h;
   return PMX_OK;
 }
+
+extern "C" int pmx_ctx_occupation_ties(const pmx_ctx* c) { return c ? c->occupation_ties : -1; }
 
 extern "C" int pmx_ctx_degenerate_cuts(const pmx_ctx* c) { return c ? c->degenerate_cuts : -1; }
 
@@ -1923,6 +1942,7 @@ extern "C" int pmx_chi_batch(pmx_ctx* ctx, int count, const pmx_problem* const* 
   return guarded(ctx, [&]() -> int {
     for (double& t : ctx->stage_ms) t = 0;
     ctx->degenerate_cuts = 0;
+    ctx->occupation_ties = 0;
     ctx->m2_err = ctx->m2_max = 0.0;
     DevCrystalSet set;
     std::vector<double> off;
@@ -2001,6 +2021,10 @@ extern "C" int pmx_chi_batch(pmx_ctx* ctx, int count, const pmx_problem* const* 
     if (ctx->degenerate_cuts > 0)
       std::cerr << "WARNING: the NBAND window cuts a degenerate set at " << ctx->degenerate_cuts
                 << " k / k+q points of the batch (|E_NBAND - E_NBAND+1| < 1e-8 eV)" << std::endl;
+    if (ctx->occupation_ties > 0)
+      std::cerr << "WARNING: " << ctx->occupation_ties
+                << " k / k+q points of the batch have a state within 1e-8 eV of the reference energy; "
+                   "their occupation is decided by rounding" << std::endl;
     return (int)PMX_OK;
   });
 }
