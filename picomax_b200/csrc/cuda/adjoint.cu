@@ -10,8 +10,11 @@
 
 #include <algorithm>
 
+#include <cfloat>
+
 #include "pmx_adjoint.hpp"
 #include "pmx_common.cuh"
+#include "pmx_tri.cuh"
 
 namespace pmx {
 namespace dev {
@@ -541,6 +544,137 @@ cudaError_t launch_hf_x(const double2* Z, long long zs, const double* lbar, int 
   const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
   hf_x_kernel<<<blocks, 256, 0, st>>>(Z, zs, lbar, n, ns, batch, X);
   return cudaGetLastError();
+}
+
+// ------------------------------------------------------------- resolvent
+// Complement part of the eigenvector adjoint without the complement's
+// eigenvectors: Y_k += P (lam_k - H)^-1 P zbar_k, P = 1 - Z_S Z_S^H, with
+// (lam - H)^-1 = Q (lam - T)^-1 Q^H from the reduction H = Q T Q^H. One warp
+// per right-hand side, rows in registers (MAXS slots of 32); the tridiagonal
+// solve runs on lane 0. (lam_k - T) is singular along the eigenvectors of S;
+// the right-hand side has no component there and the final projection removes
+// what rounding puts there.
+template <int MAXS>
+__global__ void __launch_bounds__(256) resolvent_kernel(ResolventArgs a) {
+  const int b = blockIdx.x, n = a.n;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const double2* H = a.H + (size_t)b * n * n;
+  const double* d = a.tri + (size_t)b * 4 * n;
+  const double* e = d + n;
+  const double2* tau = reinterpret_cast<const double2*>(d + 2 * n);
+  const double2* Z = a.Z + (size_t)b * a.zs;
+  __shared__ double s_tiny;
+  if (threadIdx.x == 0) {
+    double tn = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double el = i > 0 ? fabs(e[i - 1]) : 0.0, er = i < n - 1 ? fabs(e[i]) : 0.0;
+      tn = fmax(tn, fabs(d[i]) + el + er);
+    }
+    s_tiny = DBL_EPSILON * fmax(tn, DBL_MIN);
+  }
+  __syncthreads();
+  const double tiny = s_tiny;
+  double* u0 = a.work + ((size_t)b * nw + wid) * 5 * n;
+  double* u1 = u0 + n;
+  double* u2 = u1 + n;
+  double* xr = u2 + n;
+  double* xi = xr + n;
+  auto project = [&](double2* y) {
+    for (int m = 0; m < a.nsx; ++m) {
+      const double2* zm = Z + (size_t)m * n;
+      double2 dot = make_double2(0, 0);
+#pragma unroll
+      for (int s = 0; s < MAXS; ++s) {
+        const int r = 32 * s + lane;
+        if (r < n) dot = cadd(dot, cmulc(zm[r], y[s]));
+      }
+      dot = warp_sum2(dot);
+#pragma unroll
+      for (int s = 0; s < MAXS; ++s) {
+        const int r = 32 * s + lane;
+        if (r < n) y[s] = csub(y[s], cmul(zm[r], dot));
+      }
+    }
+  };
+  // apply H_j (conj = false) or H_j^H (conj = true): y -= t v (v^H y)
+  auto reflect = [&](double2* y, int j, bool conj) {
+    double2 t = tau[j];
+    if (t.x == 0.0 && t.y == 0.0) return;
+    if (conj) t.y = -t.y;
+    const double2* v = H + (size_t)j * n;
+    double2 dot = make_double2(0, 0);
+#pragma unroll
+    for (int s = 0; s < MAXS; ++s) {
+      if (32 * s + 31 <= j || 32 * s >= n) continue;  // warp-uniform
+      const int r = 32 * s + lane;
+      if (r > j && r < n) dot = cadd(dot, cmulc(v[r], y[s]));
+    }
+    const double2 sc = cmul(t, warp_sum2(dot));
+#pragma unroll
+    for (int s = 0; s < MAXS; ++s) {
+      if (32 * s + 31 <= j || 32 * s >= n) continue;
+      const int r = 32 * s + lane;
+      if (r > j && r < n) y[s] = csub(y[s], cmul(v[r], sc));
+    }
+  };
+  for (int k = wid; k < a.ns; k += nw) {
+    const double lk = a.lam[(size_t)b * a.lam_stride + k];
+    const double2* zb = a.zbar + ((size_t)b * a.ns + k) * n;
+    double2 y[MAXS];
+#pragma unroll
+    for (int s = 0; s < MAXS; ++s) {
+      const int r = 32 * s + lane;
+      y[s] = r < n ? zb[r] : make_double2(0, 0);
+    }
+    project(y);
+    for (int j = 0; j < n - 1; ++j) reflect(y, j, true);
+#pragma unroll
+    for (int s = 0; s < MAXS; ++s) {
+      const int r = 32 * s + lane;
+      if (r < n) {
+        xr[r] = y[s].x;
+        xi[r] = y[s].y;
+      }
+    }
+    __syncwarp();
+    if (lane == 0) {
+      tri_solve(d, e, n, lk, tiny, xr, u0, u1, u2);
+      tri_solve(d, e, n, lk, tiny, xi, u0, u1, u2);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int s = 0; s < MAXS; ++s) {
+      const int r = 32 * s + lane;
+      y[s] = r < n ? make_double2(-xr[r], -xi[r]) : make_double2(0, 0);
+    }
+    __syncwarp();
+    for (int j = n - 2; j >= 0; --j) reflect(y, j, false);
+    project(y);
+    double2* out = a.Y + ((size_t)b * a.ns + k) * n;
+#pragma unroll
+    for (int s = 0; s < MAXS; ++s) {
+      const int r = 32 * s + lane;
+      if (r < n) out[r] = cadd(out[r], y[s]);
+    }
+  }
+}
+
+cudaError_t launch_resolvent(const ResolventArgs& a, cudaStream_t st) {
+  if (a.nitems <= 0 || a.ns <= 0) return cudaSuccess;
+  const int slots = (a.n + 31) / 32;
+#define PMX_RES(S)                                                  \
+  if (slots <= S) {                                                 \
+    resolvent_kernel<S><<<a.nitems, 256, 0, st>>>(a);               \
+    return cudaGetLastError();                                      \
+  }
+  PMX_RES(4)
+  PMX_RES(9)
+  PMX_RES(13)
+  PMX_RES(19)
+  PMX_RES(26)
+  PMX_RES(38)
+#undef PMX_RES
+  return cudaErrorInvalidValue;
 }
 
 // ------------------------------------------------------- pair accumulators

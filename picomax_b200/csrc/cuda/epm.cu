@@ -22,6 +22,7 @@
 
 #include "pmx_common.cuh"
 #include "pmx_device.hpp"
+#include "pmx_tri.cuh"
 
 namespace pmx {
 namespace dev {
@@ -134,47 +135,6 @@ __device__ __forceinline__ double hash_uniform(unsigned long long a, unsigned lo
   x *= 0x94D049BB133111EBull;
   x ^= x >> 31;
   return ((double)(x >> 11) * (1.0 / 9007199254740992.0)) * 2.0 - 1.0;  // (-1, 1)
-}
-
-// Solves (T - lam I) x = b in place by Gaussian elimination with partial
-// pivoting (the LU has two super-diagonals). u0/u1/u2 are scratch of length n.
-__device__ void tri_solve(const double* d, const double* e, int n, double lam, double tiny,
-                          double* x, double* u0, double* u1, double* u2) {
-  double a = d[0] - lam;                  // current pivot-row diagonal
-  double c = n > 1 ? e[0] : 0.0;          // current pivot-row first super-diagonal
-  double c2 = 0.0;                         // current pivot-row second super-diagonal
-  for (int i = 0; i < n - 1; ++i) {
-    const double b = e[i];                // sub-diagonal below the pivot
-    const double dn = d[i + 1] - lam;     // next row diagonal
-    const double en = i + 1 < n - 1 ? e[i + 1] : 0.0;  // next row super-diagonal
-    if (fabs(a) >= fabs(b)) {
-      if (a == 0.0) a = tiny;
-      const double f = b / a;
-      u0[i] = a;
-      u1[i] = c;
-      u2[i] = c2;
-      x[i + 1] -= f * x[i];
-      a = dn - f * c;
-      c = en - f * c2;
-      c2 = 0.0;
-    } else {
-      const double f = a / b;  // swap rows i and i+1
-      u0[i] = b;
-      u1[i] = dn;
-      u2[i] = en;
-      const double xi = x[i];
-      x[i] = x[i + 1];
-      x[i + 1] = xi - f * x[i];
-      a = c - f * dn;
-      c = c2 - f * en;
-      c2 = 0.0;
-    }
-  }
-  if (a == 0.0 || fabs(a) < tiny) a = a < 0 ? -tiny : tiny;
-  u0[n - 1] = a;
-  x[n - 1] = x[n - 1] / u0[n - 1];
-  if (n > 1) x[n - 2] = (x[n - 2] - u1[n - 2] * x[n - 1]) / u0[n - 2];
-  for (int i = n - 3; i >= 0; --i) x[i] = (x[i] - u1[i] * x[i + 1] - u2[i] * x[i + 2]) / u0[i];
 }
 
 // Lower triangle of an n x n matrix; col(c)[r - c] = A(r, c) for r >= c.
@@ -411,7 +371,8 @@ __global__ void __launch_bounds__(kHeevThreads, (RING >= 2 || MAXS > 9) ? 1 : 2)
                                                                double* __restrict__ wbuf,
                                                                double2* __restrict__ zbuf,
                                                                double* __restrict__ scratch,
-                                                               int* __restrict__ info) {
+                                                               int* __restrict__ info,
+                                                               double* __restrict__ tri_out) {
   const EigItem it = items[blockIdx.x];
   const int n = it.n, nev = it.nval, nvec = it.want_vec ? it.nev : 0;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -556,6 +517,26 @@ __global__ void __launch_bounds__(kHeevThreads, (RING >= 2 || MAXS > 9) ? 1 : 2)
   }
   finite = __syncthreads_and(finite);
   const int status = !finite ? 2 : (!converged ? 1 : 0);
+  if (tri_out) {
+    // H = Q T Q^H for the adjoint: T (d, e after deflation), the reflector
+    // scalars tau, and (resident path) the reflectors back into hbuf
+    double* t = tri_out + (size_t)blockIdx.x * 4 * n;
+    for (int i = tid; i < n; i += nthr) {
+      t[i] = d[i];
+      t[n + i] = i < n - 1 ? e[i] : 0.0;
+      t[2 * n + 2 * i] = tau[i].x;
+      t[2 * n + 2 * i + 1] = i < n - 1 ? tau[i].y : 0.0;
+      if (i == n - 1) t[2 * n + 2 * i] = 0.0;
+    }
+    if (RESIDENT) {
+      const LowerPacked pk{Apacked, n};
+      double2* dst = hbuf + it.h_off;
+      for (int c = wid; c < n; c += nw) {
+        const double2* col = pk.col(c);
+        for (int r = c + lane; r < n; r += 32) dst[(size_t)c * n + r] = col[r - c];
+      }
+    }
+  }
   if (!it.want_vec || status != 0) {
     if (tid == 0) info[blockIdx.x] = status;
     return;
@@ -641,11 +622,11 @@ int heev_smem_max_n() {
 namespace {
 template <bool RES, int MAXS, int RING>
 cudaError_t heev_launch_t(const EigItem* items, int nitems, size_t smem, double2* hbuf, double* wbuf,
-                          double2* zbuf, double* scratch, int* info, cudaStream_t st) {
+                          double2* zbuf, double* scratch, int* info, cudaStream_t st, double* tri) {
   cudaError_t err =
       cudaFuncSetAttribute(heev_kernel<RES, MAXS, RING>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
-  heev_kernel<RES, MAXS, RING><<<nitems, kHeevThreads, smem, st>>>(items, hbuf, wbuf, zbuf, scratch, info);
+  heev_kernel<RES, MAXS, RING><<<nitems, kHeevThreads, smem, st>>>(items, hbuf, wbuf, zbuf, scratch, info, tri);
   return cudaGetLastError();
 }
 }  // namespace
@@ -663,7 +644,8 @@ int heev_variants(int max_n, int max_nev) {
 }
 
 cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev, double2* hbuf,
-                        double* wbuf, double2* zbuf, double* scratch, int* info, cudaStream_t st, int variant) {
+                        double* wbuf, double2* zbuf, double* scratch, int* info, cudaStream_t st, int variant,
+                        double* tri) {
   if (nitems <= 0) return cudaSuccess;
   const bool resident = max_n <= heev_smem_max_n() && heev_resident(max_n, max_nev);
   const int slots = (max_n + 31) / 32;
@@ -679,17 +661,17 @@ cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev
   if (slots <= S) {                                                                                          \
     if (resident)                                                                                            \
       return heev_launch_t<true, S, 0>(items, nitems, heev_smem_bytes(max_n, max_nev, true), hbuf, wbuf, zbuf, \
-                                       scratch, info, st);                                                   \
+                                       scratch, info, st, tri);                                                   \
     if (ring == 3 && S <= 13)                                                                                \
       return heev_launch_t<false, S, (S <= 13 ? 3 : 0)>(items, nitems,                                        \
                                                         heev_smem_bytes(max_n, max_nev, false, S, 3), hbuf,   \
-                                                        wbuf, zbuf, scratch, info, st);                      \
+                                                        wbuf, zbuf, scratch, info, st, tri);                      \
     if (ring == 1 && S <= 13)                                                                                \
       return heev_launch_t<false, S, (S <= 13 ? 1 : 0)>(items, nitems,                                        \
                                                         heev_smem_bytes(max_n, max_nev, false, S, 1), hbuf,   \
-                                                        wbuf, zbuf, scratch, info, st);                      \
+                                                        wbuf, zbuf, scratch, info, st, tri);                      \
     return heev_launch_t<false, S, 0>(items, nitems, heev_smem_bytes(max_n, max_nev, false, S, 0), hbuf, wbuf, \
-                                      zbuf, scratch, info, st);                                              \
+                                      zbuf, scratch, info, st, tri);                                              \
   }
   PMX_HEEV(2)
   PMX_HEEV(4)

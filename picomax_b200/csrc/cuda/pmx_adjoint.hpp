@@ -80,6 +80,23 @@ cudaError_t launch_zgemm_batched(int conj_a, int M, int N, int K, const double2*
 cudaError_t launch_eig_kmat(double2* C, const double* lam, int lam_stride, const double* lbar, int nall, int ns,
                             int batch, double tau, cudaStream_t st);
 
+struct ResolventArgs {
+  int n;                // matrix dimension (<= 1216)
+  int ns;               // right-hand sides per item (states with a gradient)
+  int nsx;              // eigenvectors projected out (a prefix of the spectrum, nsx >= ns)
+  int nitems;
+  const double2* H;     // [item][n][n] reflectors left by launch_heev(tri)
+  const double* tri;    // [item][4 n] d, e, tau of launch_heev(tri)
+  const double* lam;    // eigenvalues, item b at lam + b lam_stride
+  int lam_stride;
+  const double2* Z;     // eigenvectors, item b at Z + b zs, column m at m n (m < nsx)
+  long long zs;
+  const double2* zbar;  // [item][ns][n]
+  double2* Y;           // [item][ns][n], accumulated: Y += P (lam_k - H)^-1 P zbar_k
+  double* work;         // [item][8][5 n] doubles
+};
+cudaError_t launch_resolvent(const ResolventArgs& a, cudaStream_t st);
+
 // X = diag(lbar) Z (Hellmann-Feynman only): X [batch][ns][n], Z stride zs.
 cudaError_t launch_hf_x(const double2* Z, long long zs, const double* lbar, int n, int ns, int batch, double2* X,
                         cudaStream_t st);

@@ -49,8 +49,12 @@ cudaError_t launch_assemble(const CrystalDev* crystals, const EigItem* items, in
 // resident in shared memory. info[i] != 0 flags a failure of item i.
 // variant selects the global-memory path schedule (see heev_variants); the
 // resident path ignores it.
+// tri (optional, [nitems][4 n]): per item d[n], e[n] (e[n-1] = 0) and the
+// reflector scalars tau[n] (complex) of H = Q T Q^H; with it, the reflectors
+// are left in hbuf (column j, rows > j, v[j+1] = 1) on every path.
 cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev, double2* hbuf,
-                        double* wbuf, double2* zbuf, double* scratch, int* info, cudaStream_t st, int variant = 0);
+                        double* wbuf, double2* zbuf, double* scratch, int* info, cudaStream_t st, int variant = 0,
+                        double* tri = nullptr);
 int heev_smem_max_n();
 // Global scratch (doubles) one item of size n with nvec eigenvectors needs in
 // a launch whose largest matrix is max_n; items must be spaced by at least

@@ -255,7 +255,7 @@ struct pmx_ctx {
   DevBuf M, dE, wgt, f0, trange, acc, accpv, chi, chi2, mixws, epsm, stats;
   // adjoint workspaces
   DevBuf a_chi, a_g, a_gx, a_kk, a_f1, a_f2, a_obar, a_debar, a_mbar, a_zbk, a_zbq, a_lbk, a_lbq;
-  DevBuf a_lamk, a_lamq, a_C, a_X, a_R, a_SV, a_SSO, a_kp, a_linv;
+  DevBuf a_lamk, a_lamq, a_C, a_X, a_R, a_SV, a_SSO, a_kp, a_linv, a_hk, a_trik, a_triq, a_work;
   // several crystals at once (batched entry points)
   DevBuf b_g, b_hkl, b_vloc, b_vso, b_crystal;
   double m2_err = 0.0, m2_max = 0.0;  // |M|^2 error of the mixed path's FP32 overlaps (last call)
@@ -388,8 +388,11 @@ DevCrystal upload_crystal(pmx_ctx* c, const pmx_problem* P, int force_spinor) {
 // Assembles and diagonalises H(k) for every k; the lowest nval eigenvalues
 // go to w (host, [nk][nval]); with zdev the lowest nvec eigenvectors go to
 // zdev ([nk][nvec][n]).
+// With tri (device, [nk][4 n]) the tridiagonal form of every H(k) is exported
+// and the reflectors of the last chunk stay in c->hbuf (ks must then fit one
+// chunk: nk <= 2 GB / (16 n^2)).
 void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int nval, int nvec, double2* zdev,
-             std::vector<double>& w) {
+             std::vector<double>& w, double* tri = nullptr) {
   const int nk = (int)ks.size(), n = dc.n;
   w.assign((size_t)nk * nval, 0.0);
   if (nk == 0) return;
@@ -461,7 +464,7 @@ void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int 
       KTime kt(c, "heev");
       CK(pmx::dev::launch_heev(c->items.as<pmx::dev::EigItem>(), cnt, n, nval, c->hbuf.as<double2>(),
                                c->wbuf.as<double>(), vec ? zdev : c->hbuf.as<double2>(), c->scratch.as<double>(),
-                               c->info.as<int>(), c->stream, variant));
+                               c->info.as<int>(), c->stream, variant, tri ? tri + (size_t)k0 * 4 * n : nullptr));
     }
     c->launches += 2;
     CK(cudaMemcpyAsync(info.data(), c->info.ptr, sizeof(int) * cnt, cudaMemcpyDeviceToHost, c->stream));
@@ -1482,9 +1485,13 @@ extern "C" int pmx_epsm_vjp(pmx_ctx* ctx, const pmx_problem* P, const double* ch
     h2d(ctx, ctx->a_linv, linv.data(), sizeof(int) * linv.size());
     const double a_cm = p.lat.a * pmx::kAngstrom, bz = p.lat.bz_volume;
     const double sf_ll = 2.0 * bz * std::pow(pmx::kE, 2) / (pmx::kPi * pmx::kEV * a_cm);
-    const int kb = (int)std::max<size_t>(1, std::min<size_t>((size_t)nk, ((size_t)1 << 30) / ((size_t)n * n * 16)));
-    CK(ctx->zk.ensure(sizeof(double2) * (size_t)kb * nall * n));
-    CK(ctx->zq.ensure(sizeof(double2) * (size_t)kb * nall * n));
+    // The eigenvector adjoint needs the first nsx eigenpairs (a prefix of the
+    // spectrum containing every state with a gradient, closed under
+    // degeneracy) and the reduction H = Q T Q^H of each H(k) for the resolvent
+    // of the rest; a block's reflectors must fit one eigensolver chunk.
+    int nsx = std::min(n, ns + 8);
+    const int kb = (int)std::max<size_t>(1, std::min<size_t>((size_t)nk, ((size_t)2 << 30) / ((size_t)n * n * 16)));
+    (void)nall;
     CK(ctx->a_kk.ensure(sizeof(double) * 2 * (size_t)np * nf));
     CK(ctx->chi2.ensure(sizeof(double) * 2 * (size_t)np * nf));
     const double tau = 1e-8;  // eV: eigenvalue pairs closer than this are treated as degenerate
@@ -1522,13 +1529,33 @@ extern "C" int pmx_epsm_vjp(pmx_ctx* ctx, const pmx_problem* P, const double* ch
         std::vector<Vec3> ks(p.K.begin() + k0, p.K.begin() + k1), kqs(cnt);
         for (int i = 0; i < cnt; ++i) kqs[i] = ks[i] + Q;
         std::vector<double> wk, wq;
-        {
-          Timer tm(ctx, 0);
-          solve_k(ctx, dc, ks, nall, nall, ctx->zk.as<double2>(), wk);
-          solve_k(ctx, dc, kqs, nall, nall, ctx->zq.as<double2>(), wq);
+        int nvs = 0, nvl = 0;
+        for (;;) {
+          nvs = nsx;
+          nvl = std::min(n, nsx + 1);
+          CK(ctx->zk.ensure(sizeof(double2) * (size_t)cnt * nvs * n));
+          CK(ctx->zq.ensure(sizeof(double2) * (size_t)cnt * nvs * n));
+          CK(ctx->a_trik.ensure(sizeof(double) * 4 * (size_t)cnt * n));
+          CK(ctx->a_triq.ensure(sizeof(double) * 4 * (size_t)cnt * n));
+          {
+            Timer tm(ctx, 0);
+            solve_k(ctx, dc, ks, nvl, nvs, ctx->zk.as<double2>(), wk, ctx->a_trik.as<double>());
+            // keep the reflectors of the k side while the k+q side is reduced
+            std::swap(ctx->hbuf.ptr, ctx->a_hk.ptr);
+            std::swap(ctx->hbuf.bytes, ctx->a_hk.bytes);
+            solve_k(ctx, dc, kqs, nvl, nvs, ctx->zq.as<double2>(), wq, ctx->a_triq.as<double>());
+          }
+          // the projected prefix must not split a degenerate set
+          bool split = false;
+          if (nsx < n)
+            for (int i = 0; i < cnt && !split; ++i)
+              split = wk[(size_t)i * nvl + nsx] - wk[(size_t)i * nvl + nsx - 1] < tau ||
+                      wq[(size_t)i * nvl + nsx] - wq[(size_t)i * nvl + nsx - 1] < tau;
+          if (!split) break;
+          nsx = std::min(n, nsx + 8);
         }
         int cuts = 0;
-        Transitions T = build_transitions(p, dc.soc, nall, wk, wq, off, false, cuts, k0, k1);
+        Transitions T = build_transitions(p, dc.soc, nvl, wk, wq, off, false, cuts, k0, k1);
         std::vector<double> kp(3 * (size_t)cnt);
         for (int i = 0; i < cnt; ++i)
           for (int x = 0; x < 3; ++x) kp[3 * i + x] = ks[i][x];
@@ -1562,7 +1589,7 @@ extern "C" int pmx_epsm_vjp(pmx_ctx* ctx, const pmx_problem* P, const double* ch
             oa.n = n;
             oa.npw = npw;
             oa.soc = dc.soc;
-            oa.nev = nall;
+            oa.nev = nvs;
             oa.neps = neps;
             oa.nch = 1;
             oa.mode = 1;
@@ -1636,7 +1663,7 @@ extern "C" int pmx_epsm_vjp(pmx_ctx* ctx, const pmx_problem* P, const double* ch
           za.n = n;
           za.npw = npw;
           za.soc = dc.soc;
-          za.nev = nall;
+          za.nev = nvs;
           za.ns = ns;
           za.neps = neps;
           za.ncd_max = ncd_max;
@@ -1669,9 +1696,10 @@ extern "C" int pmx_epsm_vjp(pmx_ctx* ctx, const pmx_problem* P, const double* ch
         Timer tm(ctx, 3);
         h2d(ctx, ctx->a_lamk, wk.data(), sizeof(double) * wk.size());
         h2d(ctx, ctx->a_lamq, wq.data(), sizeof(double) * wq.size());
-        const size_t cz = (size_t)cnt * ns * nall;
+        const size_t cz = (size_t)cnt * ns * nsx;
         CK(ctx->a_C.ensure(sizeof(double2) * 2 * cz));
         CK(ctx->a_X.ensure(sizeof(double2) * (size_t)cnt * ns * n));
+        CK(ctx->a_work.ensure(sizeof(double) * (size_t)cnt * 8 * 5 * n));
         for (int side = 0; side < 2; ++side) {
           const double2* Z = side == 0 ? ctx->zk.as<double2>() : ctx->zq.as<double2>();
           const double2* Zb = side == 0 ? ctx->a_zbk.as<double2>() : ctx->a_zbq.as<double2>();
@@ -1680,15 +1708,35 @@ extern "C" int pmx_epsm_vjp(pmx_ctx* ctx, const pmx_problem* P, const double* ch
           double2* C = ctx->a_C.as<double2>();
           {
             KTime kt(ctx, "adj_eig");
-            CK(pmx::dev::launch_zgemm_batched(1, nall, ns, n, Z, n, (long long)nall * n, Zb, n, (long long)ns * n, C,
-                                              nall, (long long)ns * nall, cnt, st));
-            CK(pmx::dev::launch_eig_kmat(C, lam, nall, lb, nall, ns, cnt, tau, st));
-            CK(pmx::dev::launch_zgemm_batched(0, n, ns, nall, Z, n, (long long)nall * n, C + cz, nall,
-                                              (long long)ns * nall, ctx->a_X.as<double2>(), n, (long long)ns * n, cnt,
+            // X = Z_S' K (prefix part) ...
+            CK(pmx::dev::launch_zgemm_batched(1, nsx, ns, n, Z, n, (long long)nvs * n, Zb, n, (long long)ns * n, C,
+                                              nsx, (long long)ns * nsx, cnt, st));
+            CK(pmx::dev::launch_eig_kmat(C, lam, nvl, lb, nsx, ns, cnt, tau, st));
+            CK(pmx::dev::launch_zgemm_batched(0, n, ns, nsx, Z, n, (long long)nvs * n, C + cz, nsx,
+                                              (long long)ns * nsx, ctx->a_X.as<double2>(), n, (long long)ns * n, cnt,
                                               st));
           }
-          ctx->launches += 3;
-          hgrad_items(ctx, dc, ctx->a_X.as<double2>(), (long long)ns * n, Z, (long long)nall * n,
+          {
+            // ... + P (lam_k - H)^-1 P zbar_k for the rest of the spectrum
+            KTime kt(ctx, "adj_resolvent");
+            pmx::dev::ResolventArgs ra{};
+            ra.n = n;
+            ra.ns = ns;
+            ra.nsx = nsx;
+            ra.nitems = cnt;
+            ra.H = side == 0 ? ctx->a_hk.as<double2>() : ctx->hbuf.as<double2>();
+            ra.tri = side == 0 ? ctx->a_trik.as<double>() : ctx->a_triq.as<double>();
+            ra.lam = lam;
+            ra.lam_stride = nvl;
+            ra.Z = Z;
+            ra.zs = (long long)nvs * n;
+            ra.zbar = Zb;
+            ra.Y = ctx->a_X.as<double2>();
+            ra.work = ctx->a_work.as<double>();
+            CK(pmx::dev::launch_resolvent(ra, st));
+          }
+          ctx->launches += 4;
+          hgrad_items(ctx, dc, ctx->a_X.as<double2>(), (long long)ns * n, Z, (long long)nvs * n,
                       side == 0 ? ks : kqs, ns);
         }
       }
