@@ -31,7 +31,7 @@ from .autograd import band, eps_m
 from .workloads import te_param_map, te_params, workload
 
 FAMILIES = ("assemble", "heev", "overlap", "contract_f64", "scale", "kk", "adj_epsm", "adj_kk", "adj_contract",
-            "adj_mbar", "adj_zbar", "adj_eig", "adj_hgrad", "adj_hscatter")
+            "adj_mbar", "adj_zbar", "adj_eig", "adj_resolvent", "adj_hgrad", "adj_hscatter")
 
 
 def perturbed(theta0: np.ndarray, seed: int = 1970) -> np.ndarray:
