@@ -31,7 +31,13 @@ typedef enum {
   PMX_ERR_LIMIT = 7        /* size beyond the fixed maximum of pmx_heev_batched_noalloc */
 } pmx_status;
 
-typedef enum { PMX_SWITCH_NONE = 0, PMX_SWITCH_BAND = 1, PMX_SWITCH_EPSIJ = 2, PMX_SWITCH_EPSLL = 3 } pmx_switch;
+typedef enum {
+  PMX_SWITCH_NONE = 0,
+  PMX_SWITCH_BAND = 1,
+  PMX_SWITCH_EPSIJ = 2,
+  PMX_SWITCH_EPSLL = 3,
+  PMX_SWITCH_EPSXYZ = 4
+} pmx_switch;
 typedef enum { PMX_PREC_FP64 = 0, PMX_PREC_MIXED = 1 } pmx_precision;
 
 typedef struct pmx_problem pmx_problem; /* parsed picomax invocation (host) */
@@ -171,8 +177,10 @@ int pmx_band(pmx_ctx* ctx, const pmx_problem* p, double* eband);
 
 /* ---------------------------------------------------------------- stage 2 */
 
-/* Susceptibility of -switch epsij (chi_tensor, src/pmx_chi.cpp:319-713) or
- * epsLL (chi_LL, src/pmx_chi_copy.cpp:320-676), including the Kramers-Kronig
+/* Susceptibility of -switch epsij (chi_tensor, src/pmx_chi.cpp:319-713),
+ * epsLL (chi_LL, src/pmx_chi_copy.cpp:320-676) or epsxyz (chi_xyz,
+ * src/pmx_chi_copy.cpp:1070-1303, dispatched at src_bkp/pmx.cpp:226-241;
+ * spinor eigenvectors always, as the reference), including the Kramers-Kronig
  * step when -kk 1. re/im each hold info.chi_values doubles in .dat order
  * [i][j][q][m][n<=m][f]. precision: PMX_PREC_FP64 or PMX_PREC_MIXED. */
 int pmx_chi(pmx_ctx* ctx, const pmx_problem* p, int sw, int precision, double* re, double* im);

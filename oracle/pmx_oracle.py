@@ -359,6 +359,90 @@ def chi(cr: Crystal, mat: Material, G, hkl, K, KW, Q, *, mode: str, neps: int, n
     return RE, IM
 
 
+def chi_xyz(cr: Crystal, mat: Material, G, hkl, K, KW, Q, *, neps: int, nband: int, nvalence: int, nfreq: int,
+            dfreq: float, epsilon: float, delta: int, kk: int, refpoint=(0, 0, 0)):
+    """chi_xyz (src/pmx_chi_copy.cpp:1070-1303, switch epsxyz): Cartesian
+    current-current tensor. Valence states at k (counted up while E - E_ref
+    <= 0), conduction states at k+q (counted down from the top of the NBAND
+    window while E - E_ref > 0); the overlap multiplies the first NPW
+    components of the spinor eigenvectors (the reference's
+    eigenvectors().col(v)(p), p < NPW) with the orbital current
+    e_i . (G_p + k + q/2 + G_m/2); SCALEFACTOR of the TT block, PV term
+    1 / dE / (dE^2 - w^2) when kk = 0. Because component p is paired with plane
+    wave loci[m][p], the result depends on the full G order: G must be the
+    reference's (pmx_problem_gvectors), not gvectors() of this module.
+    Returns (re, im) [3, 3, NQ, npairs, NFREQ]."""
+    G = np.asarray(G, float)
+    npw = len(G)
+    L = loci_table(np.asarray(hkl), neps)
+    off = ref_energy(cr, mat, G, nvalence, refpoint)
+    freq = dfreq * np.arange(nfreq)
+    npairs = neps * (neps + 1) // 2
+    RE = np.zeros((3, 3, len(Q), npairs, nfreq))
+    IM = np.zeros_like(RE)
+    acm = cr.a * ANG
+    SF = 32.0 * cr.bz_volume * PI ** 3 * HBAR ** 4 * E ** 2 / (EV ** 3 * EM ** 2 * acm ** 5)
+    kst = []
+    for k in K:
+        w, v = _eig_k(cr, mat, G, k)
+        ev = []
+        for vv in range(nband):
+            e = w[vv] - off
+            if e > 0:
+                break
+            ev.append(e)
+        kst.append((np.array(ev), v[:npw, :len(ev)]))
+    for iq, q in enumerate(Q):
+        q = np.asarray(q, float)
+        trans = []  # (kw, dE, oint[3][neps])
+        for ik, k in enumerate(K):
+            w, v = _eig_k(cr, mat, G, np.asarray(k) + q)
+            ec = []
+            for c in range(nband):
+                e = w[nband - 1 - c] - off
+                if e <= 0:
+                    break
+                ec.append(e)
+            cq = v[:npw, [nband - 1 - c for c in range(len(ec))]]
+            evk, ck = kst[ik]
+            for vv in range(len(evk)):
+                for c in range(len(ec)):
+                    O = np.zeros((3, neps), complex)
+                    for m in range(neps):
+                        act = np.nonzero(L[m] >= 0)[0]
+                        orbv = G[act] + np.asarray(k) + q / 2 + G[m] / 2
+                        prod = np.conj(ck[act, vv]) * cq[L[m, act], c]
+                        for i in range(3):
+                            O[i, m] = np.sum(prod * orbv[:, i])
+                    trans.append((KW[ik], ec[c] - evk[vv], O))
+        for i in range(3):
+            for j in range(3):
+                pidx = 0
+                for m in range(neps):
+                    for n in range(m + 1):
+                        s_im = np.zeros(nfreq)
+                        s_re = np.zeros(nfreq)
+                        p_re = np.zeros(nfreq)
+                        p_im = np.zeros(nfreq)
+                        for kw, de, O in trans:
+                            o = O[i, m] * np.conj(O[j, n])
+                            d = delta_fn(delta, epsilon, de - freq)
+                            s_im += kw * o.real * d
+                            s_re -= kw * o.imag * d
+                            if kk == 0:
+                                g = 1.0 / de / (de * de - freq * freq)
+                                p_re += kw * o.real * g
+                                p_im += kw * o.imag * g
+                        inv = np.zeros(nfreq)
+                        inv[1:] = 1.0 / freq[1:] ** 2
+                        IM[i, j, iq, pidx] = SF * (PI * s_im * inv + 2.0 * p_im)
+                        RE[i, j, iq, pidx] = SF * (PI * s_re * inv + 2.0 * p_re)
+                        pidx += 1
+        if kk:
+            RE[:, :, iq], IM[:, :, iq] = kk_transform(RE[:, :, iq], IM[:, :, iq], freq, dfreq)
+    return RE, IM
+
+
 def eps_macroscopic(chi_ll_re: np.ndarray, chi_ll_im: np.ndarray, neps: int) -> np.ndarray:
     """eps_M(w) = 1 / [eps^-1]_00 with eps_mn = delta_mn + chi^LL_mn, Hermitian
     fill of the stored n <= m half (include/matlab_wrapper/+picomax/+eps/

@@ -6,7 +6,7 @@ The compute path is the in-tree shared library ``lib/libpicomax_b200.so``
 the torch autograd wrapper. There is no CPU implementation of the GPU stages.
 """
 from ._capi import (  # noqa: F401
-    PREC_FP64, PREC_MIXED, SWITCH_BAND, SWITCH_EPSIJ, SWITCH_EPSLL, CLI_PATH, LIB_PATH, Context,
+    PREC_FP64, PREC_MIXED, SWITCH_BAND, SWITCH_EPSIJ, SWITCH_EPSLL, SWITCH_EPSXYZ, CLI_PATH, LIB_PATH, Context,
     PicomaxError, Problem, load, run_main)
 from .kgrid import gamma_grid, make_kfile, write_kfile  # noqa: F401
 from . import dat  # noqa: F401

@@ -26,7 +26,7 @@ PMX_ERR_NO_DEVICE = 5
 PMX_ERR_UNSUPPORTED = 6
 PMX_ERR_LIMIT = 7
 
-SWITCH_NONE, SWITCH_BAND, SWITCH_EPSIJ, SWITCH_EPSLL = 0, 1, 2, 3
+SWITCH_NONE, SWITCH_BAND, SWITCH_EPSIJ, SWITCH_EPSLL, SWITCH_EPSXYZ = 0, 1, 2, 3, 4
 PREC_FP64, PREC_MIXED = 0, 1
 
 # Every entry point declared in include/picomax.h.

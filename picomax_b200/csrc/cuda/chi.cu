@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(kCThreads) contract_f64_kernel(ContractArgs a)
   for (int u = 0; u < 9; ++u) {
     const int pp = pg * 9 + u;
     const int i = (pp / kAB) % 3, j = (pp % kAB) % 3;
-    pclass[u] = (i == 0 && j == 0) ? 1 : ((i == 0 || j == 0) ? 2 : 3);
+    pclass[u] = a.pvclass ? a.pvclass : ((i == 0 && j == 0) ? 1 : ((i == 0 || j == 0) ? 2 : 3));
   }
   for (int t0 = tr.x; t0 < tr.y; t0 += kTK) {
     const int nt = min(kTK, tr.y - t0);
@@ -421,6 +421,8 @@ __global__ void scale_kernel(ScaleArgs s) {
       double f1;
       if (f == 0) {
         f1 = 0.0;
+      } else if (s.mode == 2) {  // epsxyz: every block scales as TT (src/pmx_chi_copy.cpp:1093, :1272-1281)
+        f1 = s.sf_tt / (w * w);
       } else if (i == 0 && j == 0) {
         f1 = s.sf_ll / (qm * qn);
       } else if (i == 0) {
@@ -433,7 +435,9 @@ __global__ void scale_kernel(ScaleArgs s) {
       double out = 3.14159265358979323846 * (v * f1);
       if (s.acc_pv) {
         double f2;
-        if (i == 0 && j == 0)
+        if (s.mode == 2)
+          f2 = s.sf_tt;
+        else if (i == 0 && j == 0)
           f2 = s.sf_ll / (qm * qn);
         else if (i == 0)
           f2 = s.sf_lt / qm;

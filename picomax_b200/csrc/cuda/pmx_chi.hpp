@@ -51,10 +51,11 @@ struct ContractArgs {
   double* acc;          // [2][9][np][nf] Re then Im
   double* acc_pv;       // principal-value accumulators (epsLL, kk = 0) or null
   double* stats;        // mixed path only, optional (device, 2 doubles): max ||M32|^2 - |M|^2|, max |M|^2
+  int pvclass;          // principal-value function: 0 by (i, j) block (epsLL), 3 = 1/dE/(dE^2-w^2) for all (epsxyz)
 };
 
 struct ScaleArgs {
-  int mode;             // 0 epsij, 1 epsLL
+  int mode;             // 0 epsij, 1 epsLL, 2 epsxyz
   int np, nf;
   double dfreq;
   double sf;            // epsij SCALEFACTOR

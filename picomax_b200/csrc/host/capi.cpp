@@ -668,7 +668,7 @@ struct Transitions {
 // then count from k0).
 Transitions build_transitions(const Problem& p, int soc, int nval, const std::vector<double>& wk,
                               const std::vector<double>& wq, double off, bool sort_by_window, int& cuts,
-                              int k0 = 0, int k1 = -1, int* ties = nullptr) {
+                              int k0 = 0, int k1 = -1, int* ties = nullptr, bool xyz = false) {
   Transitions T;
   if (k1 < 0) k1 = p.nk();
   const int nk = k1 - k0, NB = p.nband;
@@ -703,6 +703,29 @@ Transitions build_transitions(const Problem& p, int soc, int nval, const std::ve
       *ties += (int)tk + (int)tq;
     }
     int nc = 0, nv = 0;
+    if (xyz) {
+      // chi_xyz (src/pmx_chi_copy.cpp:1128-1140, :1178-1186): the conjugated
+      // (first) set is the valence at k, counted up while E - E_ref <= 0; the
+      // second set the conduction at k+q, counted down from the top while > 0.
+      // Spinor states only.
+      std::vector<int> fs, ss;
+      while (nc < NB && spinor_eig(wk, nval, k, nc, soc) - off <= 0) fs.push_back(nc++);
+      while (nv < NB && spinor_eig(wq, nval, k, NB - 1 - nv, soc) - off > 0) ss.push_back(NB - 1 - nv++);
+      T.ncd[k] = (int)fs.size();
+      T.nvd[k] = (int)ss.size();
+      T.cbase[k] = (int)T.cidx.size();
+      T.vbase[k] = (int)T.vidx.size();
+      T.cidx.insert(T.cidx.end(), fs.begin(), fs.end());
+      T.vidx.insert(T.vidx.end(), ss.begin(), ss.end());
+      T.blkoff[k] = blk;
+      for (size_t a = 0; a < fs.size(); ++a)
+        for (size_t b = 0; b < ss.size(); ++b) {
+          const double de = (spinor_eig(wq, nval, k, ss[b], soc) - off) - (spinor_eig(wk, nval, k, fs[a], soc) - off);
+          raw.push_back({blk + (long long)(a * ss.size() + b), de, p.KW[kg], (int)((de - w0) / df)});
+        }
+      blk += (long long)fs.size() * ss.size();
+      continue;
+    }
     while (nc < NB && spinor_eig(wk, nval, k, NB - 1 - nc, soc) - off > 0) ++nc;
     while (nv < NB && spinor_eig(wq, nval, k, nv, soc) - off <= 0) ++nv;
     // distinct solved states
@@ -786,7 +809,8 @@ ChiPlan chi_plan(const Problem& p, int sw, const DevCrystal& dc) {
   if (p.nband > 2 * p.npw()) throw std::runtime_error("-nband exceeds the Hamiltonian dimension");
   if (p.nband <= 0) throw std::runtime_error("-nband must be positive");
   ChiPlan pl;
-  pl.mode = sw == PMX_SWITCH_EPSLL ? 1 : 0;
+  pl.mode = sw == PMX_SWITCH_EPSLL ? 1 : (sw == PMX_SWITCH_EPSXYZ ? 2 : 0);
+  if (pl.mode == 2 && !dc.soc) throw std::runtime_error("epsxyz needs the spinor eigenproblem");
   pl.nk = p.nk();
   pl.nq = p.nq();
   pl.neps = p.neps;
@@ -815,7 +839,7 @@ ChiPlan chi_plan(const Problem& p, int sw, const DevCrystal& dc) {
   pl.W = pl.mode == 0 ? window_half(p) : -1;
   pl.FT = pmx::dev::contract_ftile();
   pl.nft = (pl.nf + pl.FT - 1) / pl.FT;
-  pl.pv = pl.mode == 1 && p.kk == 0;
+  pl.pv = pl.mode >= 1 && p.kk == 0;
   return pl;
 }
 
@@ -849,7 +873,7 @@ void chi_process_q(pmx_ctx* ctx, const Problem& p, const ChiPlan& pl, const DevC
   pmx::dev::ScaleArgs sa = pl.sa;
   const Vec3 Q = p.lat.Q[q];
   Transitions T = build_transitions(p, dc.soc, nval, wk, wq, off, mode == 0, ctx->degenerate_cuts, 0, -1,
-                                    &ctx->occupation_ties);
+                                    &ctx->occupation_ties, mode == 2);
   // per-m polarisation and SOC-current tables
   std::vector<double2> uv((size_t)neps * 9), ss((size_t)neps * 3);
   std::vector<double> qg(neps);
@@ -867,6 +891,13 @@ void chi_process_q(pmx_ctx* ctx, const Problem& p, const ChiPlan& pl, const DevC
         s += std::conj(std::complex<double>(u[i][x][0], u[i][x][1])) * vs[x];
       }
       ss[(size_t)m * 3 + i] = make_double2(s.real(), s.imag());
+    }
+    if (mode == 2) {
+      // epsxyz: Cartesian unit vectors, no SOC current (src/pmx_chi_copy.cpp:1203-1222)
+      for (int i = 0; i < 3; ++i) {
+        for (int x = 0; x < 3; ++x) uv[((size_t)m * 3 + i) * 3 + x] = make_double2(i == x ? 1.0 : 0.0, 0.0);
+        ss[(size_t)m * 3 + i] = make_double2(0, 0);
+      }
     }
   }
   h2d(ctx, ctx->uvec, uv.data(), sizeof(double2) * uv.size());
@@ -904,11 +935,14 @@ void chi_process_q(pmx_ctx* ctx, const Problem& p, const ChiPlan& pl, const DevC
     pmx::dev::OverlapArgs oa{};
     oa.n = n;
     oa.npw = dc.npw;
-    oa.soc = dc.soc;
+    // epsxyz pairs eigenvector component p (not plane wave p) with loci[m][p]
+    // over the first N_G components (src/pmx_chi_copy.cpp:1143, :1188, :1216):
+    // the unresolved (soc = 0) gather on the spinor vectors does exactly that
+    oa.soc = mode == 2 ? 0 : dc.soc;
     oa.nev = nev;
     oa.neps = neps;
     oa.nch = nch;
-    oa.mode = mode;
+    oa.mode = mode == 2 ? 0 : mode;  // epsxyz: orbital current along x, y, z
     oa.ncd_max = *std::max_element(T.ncd.begin(), T.ncd.end());
     oa.nvd_max = *std::max_element(T.nvd.begin(), T.nvd.end());
     if (!pmx::dev::overlap_tiles(oa.ncd_max, oa.nvd_max, n, dc.npw, oa.cchunk, oa.vchunk))
@@ -955,6 +989,7 @@ void chi_process_q(pmx_ctx* ctx, const Problem& p, const ChiPlan& pl, const DevC
     ca.dfreq = p.dfreq;
     ca.acc = ctx->acc.as<double>();
     ca.acc_pv = pv ? ctx->accpv.as<double>() : nullptr;
+    ca.pvclass = mode == 2 ? 3 : 0;
     if (precision == PMX_PREC_FP64 || pv) {
       KTime kt(ctx, "contract_f64");
       CK(pmx::dev::launch_contract_f64(ca, st));
@@ -1019,8 +1054,9 @@ void chi_process_q(pmx_ctx* ctx, const Problem& p, const ChiPlan& pl, const DevC
 
 static int run_chi(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision, double* re, double* im,
                    bool device_out, double* epsm) {
-  if (!P || (sw != PMX_SWITCH_EPSIJ && sw != PMX_SWITCH_EPSLL)) return PMX_ERR_INVALID;
+  if (!P || (sw != PMX_SWITCH_EPSIJ && sw != PMX_SWITCH_EPSLL && sw != PMX_SWITCH_EPSXYZ)) return PMX_ERR_INVALID;
   if (precision != PMX_PREC_FP64 && precision != PMX_PREC_MIXED) return PMX_ERR_INVALID;
+  if (epsm && sw == PMX_SWITCH_EPSXYZ) return PMX_ERR_INVALID;  // eps_M is defined on the (L, L) block
   return guarded(ctx, [&]() -> int {
     const Problem& p = P->p;
     cudaStream_t st = ctx->stream;
@@ -1031,7 +1067,7 @@ static int run_chi(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision, do
     std::vector<double> wk;
     {
       Timer tm(ctx, 0);
-      dc = upload_crystal(ctx, P, 0);
+      dc = upload_crystal(ctx, P, sw == PMX_SWITCH_EPSXYZ ? 1 : 0);
       off = ref_energy(ctx, P, dc);
     }
     const ChiPlan pl = chi_plan(p, sw, dc);
@@ -1758,7 +1794,7 @@ struct DevCrystalSet {
   pmx::dev::CrystalDev* table = nullptr;
 };
 
-DevCrystalSet upload_crystals(pmx_ctx* c, const pmx_problem* const* P, int count) {
+DevCrystalSet upload_crystals(pmx_ctx* c, const pmx_problem* const* P, int count, int force_spinor = 0) {
   DevCrystalSet set;
   std::vector<size_t> og(count + 1, 0), ov(count + 1, 0);
   for (int i = 0; i < count; ++i) {
@@ -1789,7 +1825,7 @@ DevCrystalSet upload_crystals(pmx_ctx* c, const pmx_problem* const* P, int count
     c->h2d += (long long)(2 * sizeof(double) * P[i]->vloc.size());
     pmx::dev::CrystalDev& cd = tab[i];
     cd.npw = p.npw();
-    cd.soc = P[i]->soc;
+    cd.soc = (P[i]->soc || force_spinor) ? 1 : 0;
     cd.imax = p.imax;
     cd.side = 4 * p.imax + 1;
     const double sc = 2.0 * pmx::kPi / p.lat.a;
@@ -1983,8 +2019,9 @@ extern "C" int pmx_band_batch(pmx_ctx* ctx, int count, const pmx_problem* const*
 extern "C" int pmx_chi_batch(pmx_ctx* ctx, int count, const pmx_problem* const* problems, int sw, int precision,
                              double* const* re, double* const* im, double* const* epsm) {
   if (count < 0 || (count > 0 && (!problems || !re || !im))) return PMX_ERR_INVALID;
-  if (sw != PMX_SWITCH_EPSIJ && sw != PMX_SWITCH_EPSLL) return PMX_ERR_INVALID;
+  if (sw != PMX_SWITCH_EPSIJ && sw != PMX_SWITCH_EPSLL && sw != PMX_SWITCH_EPSXYZ) return PMX_ERR_INVALID;
   if (precision != PMX_PREC_FP64 && precision != PMX_PREC_MIXED) return PMX_ERR_INVALID;
+  if (epsm && sw == PMX_SWITCH_EPSXYZ) return PMX_ERR_INVALID;
   for (int i = 0; i < count; ++i)
     if (!problems[i] || !re[i] || !im[i] || (epsm && epsm[i] && problems[i]->p.neps > 64)) return PMX_ERR_INVALID;
   return guarded(ctx, [&]() -> int {
@@ -1996,7 +2033,7 @@ extern "C" int pmx_chi_batch(pmx_ctx* ctx, int count, const pmx_problem* const* 
     std::vector<double> off;
     {
       Timer tm(ctx, 0);
-      set = upload_crystals(ctx, problems, count);
+      set = upload_crystals(ctx, problems, count, sw == PMX_SWITCH_EPSXYZ ? 1 : 0);
       off = ref_energies(ctx, problems, count, set);
     }
     std::vector<ChiPlan> pl;

@@ -709,6 +709,7 @@ void build_problem(int argc, const char* const* argv, Problem& p) {
     if (p.switch_name == "band") p.sw = Switch::Band;
     else if (p.switch_name == "epsij") p.sw = Switch::Epsij;
     else if (p.switch_name == "epsLL") p.sw = Switch::EpsLL;
+    else if (p.switch_name == "epsxyz") p.sw = Switch::EpsXyz;
   }
   generate_gvectors(p);
   generate_loci(p);
@@ -764,7 +765,7 @@ void print_doc() {
             << "-wdir : working directory {pwd}\n"
             << "-logfile : print output to a logfile {0}\n\n"
             << "-switch : calculation switch\n"
-            << "    band, epsij, epsLL\n\n"
+            << "    band, epsij, epsLL, epsxyz\n\n"
             << "-crystal : crystal structure\n"
             << "    zb, wz, rs, te, hex\n"
             << "-dim : crystal dimension {3}\n"

@@ -86,7 +86,7 @@ struct Material {
   double uniform_us = 0;
 };
 
-enum class Switch { None, Band, Epsij, EpsLL };
+enum class Switch { None, Band, Epsij, EpsLL, EpsXyz };
 
 // One parsed picomax invocation (src/pmx_io.cpp:108-503).
 struct Problem {

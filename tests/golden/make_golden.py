@@ -35,6 +35,11 @@ GAAS_VG = ",".join(["3", "4", "8", "11"] + [f"{x:.6f}" for x in _vs + _va] + [f"
 WZ_VG = ("0.378233,1.333333,1.512930,1.711566," + ",".join(["-0.119900,0.224132,-0.296841,0.192737"] * 4))
 GAAS_SOC = ["-use_uniform_us_so", "-uniform_us_so_val", "0.004", "-ua_so", "3:0.002,4:0.0015,8:0.001,11:0.0005"]
 
+# generic k-points for epsxyz: away from the time-reversal-invariant momenta,
+# where every level is a Kramers pair and chi_xyz (which mixes the first N_G
+# spinor components) depends on the eigensolver's basis inside the pair
+K_GENERIC = [[0.11, 0.23, 0.05], [0.31, -0.17, 0.09], [-0.07, 0.19, -0.26], [0.41, 0.08, 0.21]]
+
 CASES = {
     # name: (binary, argv, kgrid or None)
     "si_band": ("picomax_ref", ["-switch", "band", "-crystal", "zb", "-a", "5.43", "-vg", SI_VG, "-encut", "110",
@@ -58,6 +63,14 @@ CASES = {
                                              "-encut", "80", "-nband", "16", "-nvalence", "8", "-neps", "4",
                                              "-nfreq", "120", "-dfreq", "0.125", "-delta", "2", "-epsilon", "0.3",
                                              "-kk", "0", "-qvec", "0.02,0.01,0"] + GAAS_SOC, ("zb", 2, 2, 2)),
+    "gaas_soc_epsxyz": ("picomax_ref_ll", ["-switch", "epsxyz", "-crystal", "zb", "-a", "5.65", "-vg", GAAS_VG,
+                                           "-encut", "80", "-nband", "16", "-nvalence", "8", "-neps", "4",
+                                           "-nfreq", "120", "-dfreq", "0.125", "-delta", "0", "-epsilon", "0.1",
+                                           "-kk", "1", "-qvec", "0.01,0,0"] + GAAS_SOC, ("list", K_GENERIC)),
+    "gaas_soc_epsxyz_pv": ("picomax_ref_ll", ["-switch", "epsxyz", "-crystal", "zb", "-a", "5.65", "-vg", GAAS_VG,
+                                              "-encut", "80", "-nband", "16", "-nvalence", "8", "-neps", "3",
+                                              "-nfreq", "100", "-dfreq", "0.125", "-delta", "1", "-epsilon", "0.05",
+                                              "-kk", "0", "-qvec", "0.02,0.01,0"] + GAAS_SOC, ("list", K_GENERIC)),
     "wz_epsij_rect": ("picomax_ref_guard", ["-switch", "epsij", "-crystal", "wz", "-a", "3.19", "-f", "1.626", "-u",
                                             "0.375", "-vg", WZ_VG, "-encut", "50", "-nband", "24", "-nvalence", "8",
                                             "-neps", "3", "-nfreq", "100", "-dfreq", "0.15", "-delta", "3",
@@ -69,7 +82,13 @@ CASES = {
 def run_case(name, binary, argv, grid, tmp):
     args = list(argv)
     K = None
-    if grid is not None:
+    if grid is not None and grid[0] == "list":
+        K = np.asarray(grid[1], float)
+        W = np.ones(len(K))
+        kf = os.path.join(tmp, f"{name}_k.txt")
+        write_kfile(kf, K, W)
+        args += ["-kpoint", "0", "-kpointfile", kf]
+    elif grid is not None:
         crystal, n1, n2, n3 = grid
         K, W = gamma_grid(crystal, n1, n2, n3)
         kf = os.path.join(tmp, f"{name}_k.txt")
@@ -89,8 +108,9 @@ def run_case(name, binary, argv, grid, tmp):
         out["gpt"] = np.fromfile(gpt, np.float64)
     if K is not None:
         out["kpts"] = K
-        out["kgrid"] = np.array(grid[1:], np.int64)
-        out["kcrystal"] = grid[0]
+        if grid[0] != "list":
+            out["kgrid"] = np.array(grid[1:], np.int64)
+            out["kcrystal"] = grid[0]
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
     print(f"{name}: {out['dat'].size} values, {dt:.2f} s")
 

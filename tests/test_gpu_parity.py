@@ -18,7 +18,8 @@ import pmx_oracle as O
 
 pytestmark = pytest.mark.gpu
 
-CHI_CASES = ["si_epsij", "gaas_soc_epsij", "si_epsLL", "gaas_soc_epsLL_pv", "wz_epsij_rect"]
+CHI_CASES = ["si_epsij", "gaas_soc_epsij", "si_epsLL", "gaas_soc_epsLL_pv", "wz_epsij_rect", "gaas_soc_epsxyz",
+             "gaas_soc_epsxyz_pv"]
 
 
 @pytest.mark.parametrize("name", ["si_band", "gaas_soc_band"])
@@ -29,12 +30,17 @@ def test_band_vs_reference(ctx, name, tmp_path):
     assert np.max(np.abs(eb.ravel() - g["dat"])) < 1e-9
 
 
+def _switch(args):
+    name = args[args.index("-switch") + 1]
+    return {"epsij": pm.SWITCH_EPSIJ, "epsLL": pm.SWITCH_EPSLL, "epsxyz": pm.SWITCH_EPSXYZ}[name]
+
+
 @pytest.mark.parametrize("name", CHI_CASES)
 def test_chi_fp64_vs_reference(ctx, name, tmp_path):
     g = load_golden(name)
     args = golden_args(g, tmp_path)
     p = pm.Problem(args)
-    sw = pm.SWITCH_EPSLL if "epsLL" in args else pm.SWITCH_EPSIJ
+    sw = _switch(args)
     re, im = ctx.chi(p, sw, pm.PREC_FP64)
     n = re.size
     ref_re, ref_im = g["dat"][:n], g["dat"][n:]
@@ -125,7 +131,7 @@ def test_kk_vs_oracle(ctx):
     assert np.max(np.abs(i1 - i0)) < 1e-10 * np.max(np.abs(i0))
 
 
-@pytest.mark.parametrize("name", ["si_band", "si_epsLL", "gaas_soc_epsij"])
+@pytest.mark.parametrize("name", ["si_band", "si_epsLL", "gaas_soc_epsij", "gaas_soc_epsxyz"])
 def test_cli_files_vs_reference(name, tmp_path):
     """The picomax executable writes byte-compatible .dat/.gpt files."""
     g = load_golden(name)
@@ -148,7 +154,7 @@ def test_chi_mixed_vs_reference(ctx, name, tmp_path):
     g = load_golden(name)
     args = golden_args(g, tmp_path)
     p = pm.Problem(args)
-    sw = pm.SWITCH_EPSLL if "epsLL" in args else pm.SWITCH_EPSIJ
+    sw = _switch(args)
     re, im = ctx.chi(p, sw, pm.PREC_MIXED)
     n = re.size
     ref_re, ref_im = g["dat"][:n], g["dat"][n:]

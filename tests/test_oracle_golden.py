@@ -52,3 +52,26 @@ def test_oracle_chi(name):
     scale = max(np.abs(ref_re).max(), np.abs(ref_im).max())
     assert np.max(np.abs(re - ref_re)) < 1e-8 * scale
     assert np.max(np.abs(im - ref_im)) < 1e-8 * scale
+
+
+@pytest.mark.parametrize("name", ["gaas_soc_epsxyz", "gaas_soc_epsxyz_pv"])
+def test_oracle_chi_xyz(name, tmp_path):
+    """chi_xyz pairs eigenvector component p with plane wave loci[m][p], so it
+    depends on the full G order: the oracle gets the reference's order from the
+    host tables (bit-exact against the reference's -debug 3 dumps)."""
+    from conftest import golden_args
+    import picomax_b200 as pm
+    g = load_golden(name)
+    args = golden_args(g, tmp_path)
+    cr, mat, gcut, o = O.from_args(args)
+    p = pm.Problem(args)
+    G, hkl = p.gvectors()
+    K, KW = p.kpoints()
+    Q = p.qpoints()
+    p.close()
+    re, im = O.chi_xyz(cr, mat, G, hkl, K, KW, Q, **o)
+    n = re.size
+    ref_re, ref_im = g["dat"][:n].reshape(re.shape), g["dat"][n:].reshape(re.shape)
+    scale = max(np.abs(ref_re).max(), np.abs(ref_im).max())
+    assert np.max(np.abs(re - ref_re)) < 1e-8 * scale
+    assert np.max(np.abs(im - ref_im)) < 1e-8 * scale
