@@ -261,6 +261,26 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_kernel(Plan pl, ContractArg
   if (tid == 0) *s_last = -1;
   double* out = pl.part + ((size_t)item_id * pl.ntile + tile) * (kM * kN);
   int flushes = 0;
+  // The overlaps and weights of chunk c + 1 are loaded into registers while
+  // chunk c is produced and multiplied, so the L2 latency of the overlap
+  // gather is off the producer's critical path.
+  constexpr int kMPer = kKC * 16 * NCH / kThreads;
+  float2 mreg[kMPer];
+  float wreg = 0.f;
+  auto load_chunk = [&](int cc) {
+    const int t0 = pl.chunk_t0[cc], t1 = pl.chunk_t1[cc];
+#pragma unroll
+    for (int q = 0; q < kMPer; ++q) {
+      const int idx = tid + q * kThreads;
+      const int t = idx / (16 * NCH), rem = idx % (16 * NCH);
+      const int slot = rem / NCH, ch = rem % NCH;
+      const int gt = t0 + t;
+      const int ab = slot < 8 ? a0 + slot : b0 + slot - 8;
+      mreg[q] = (gt < t1 && ab < A) ? M32[((size_t)gt * A + ab) * NCH + ch] : make_float2(0.f, 0.f);
+    }
+    wreg = (tid < kKC && t0 + tid < t1) ? pl.wgt32[t0 + tid] : 0.f;
+  };
+  if (c_begin < c_end) load_chunk(c_begin);
   for (int c = c_begin; c < c_end; ++c) {
     const int n = c - c_begin, s = n & 1;
     const int g = n % kFlushChunks;  // position inside the current FP32 accumulation group
@@ -274,19 +294,12 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_kernel(Plan pl, ContractArg
     tc_fence_after();
     if (*s_abort) break;
     if (tid == 0) bulk_load(st + 2 * kABytes, pl.wbuf + (size_t)c * kWChunkBytes, kWChunkBytes, &wfull[s]);
-    // stage overlaps and weights of the chunk
-    const int t0 = pl.chunk_t0[c], t1 = pl.chunk_t1[c];
-    for (int idx = tid; idx < kKC * 16 * NCH; idx += kThreads) {
-      const int t = idx / (16 * NCH), rem = idx % (16 * NCH);
-      const int slot = rem / NCH, ch = rem % NCH;
-      const int gt = t0 + t;
-      const int ab = slot < 8 ? a0 + slot : b0 + slot - 8;
-      float2 v = make_float2(0.f, 0.f);
-      if (gt < t1 && ab < A) v = M32[((size_t)gt * A + ab) * NCH + ch];
-      sM[idx] = v;
-    }
-    if (tid < kKC) sw[tid] = (t0 + tid < t1) ? pl.wgt32[t0 + tid] : 0.f;
+    // stage overlaps and weights of the chunk (loaded one iteration ahead)
+#pragma unroll
+    for (int q = 0; q < kMPer; ++q) sM[tid + q * kThreads] = mreg[q];
+    if (tid < kKC) sw[tid] = wreg;
     __syncthreads();
+    if (c + 1 < c_end) load_chunk(c + 1);
     // split pair products into the A tile: row pp (P1) and 64 + pp (P2)
     {
       float p1[8], p2[8];
