@@ -655,7 +655,8 @@ cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev
   // one-CTA-per-SM padding of schedule 0 (L2-resident trailing blocks), a
   // register cap for 3 CTAs/SM and a two-columns-per-iteration pass were
   // slower still (120 / 106 / 97 ms): the pass is bound by dependent FP64
-  // chains and load latency at 16 warps per SM.
+  // chains and load latency at 16 warps per SM. For n = 401 (one CTA per SM by
+  // registers) a register cap for two CTAs per SM was slower too (159 vs 141 ms).
   const int ring = resident ? 0 : (variant == 1 ? 1 : (variant == 2 ? 3 : 0));
 #define PMX_HEEV(S)                                                                                          \
   if (slots <= S) {                                                                                          \
