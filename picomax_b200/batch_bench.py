@@ -149,7 +149,7 @@ def main(argv=None):
                       "per_crystal_kpts_per_s": nk_band / tl, "speedup": tl / tb, "max_abs_diff_eV": diff,
                       "setup_s": t_setup}), flush=True)
 
-    fam = ("assemble", "heev", "overlap", "contract_mixed", "contract_f64", "scale", "kk")
+    fam = ("solve_graph", "assemble", "heev", "overlap", "contract_mixed", "contract_f64", "scale", "kk")
     k0 = {f: ctx.kernel_time(f)[0] for f in fam}
     tb, cb = timed(lambda: ctx.chi_batch(chi, C.SWITCH_EPSLL, prec, epsm=True))
     kms = {f: round((ctx.kernel_time(f)[0] - k0[f]) / a.repeat, 1) for f in fam}

@@ -1872,15 +1872,25 @@ int heev_class(int n) {
   return 1 << 20;
 }
 
+// All requests in one CUDA graph: the requests are sorted by n and cut into
+// chunks of one eigensolver size class (one template instantiation) and at
+// most 2 GB of H; the assembly + eigensolver launches of every chunk are
+// captured into a graph, launched once, and the eigenvalues and status codes
+// of all chunks come back in one copy each.
 void solve_multi(pmx_ctx* c, const pmx::dev::CrystalDev* table, std::vector<SolveReq>& reqs, double2* zbase) {
   if (reqs.empty()) return;
   std::vector<int> order(reqs.size());
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return reqs[a].n > reqs[b].n; });
+  struct Chunk {
+    int first, cnt, max_n, max_nval, max_npw;
+  };
+  std::vector<Chunk> chunks;
+  std::vector<pmx::dev::EigItem> items(reqs.size());
   const size_t hmax = (size_t)2 << 30;
+  long long w = 0, hneed = 0, sneed = 0;
   size_t i0 = 0;
   while (i0 < order.size()) {
-    // one chunk: same size class, bounded workspace
     const int max_n = reqs[order[i0]].n, cls = heev_class(max_n);
     size_t i1 = i0, hb = 0;
     while (i1 < order.size() && i1 - i0 < 4096 && heev_class(reqs[order[i1]].n) == cls) {
@@ -1889,12 +1899,10 @@ void solve_multi(pmx_ctx* c, const pmx::dev::CrystalDev* table, std::vector<Solv
       hb += b;
       ++i1;
     }
-    const int cnt = (int)(i1 - i0);
-    std::vector<pmx::dev::EigItem> items(cnt);
-    long long h = 0, w = 0, sc = 0;
-    int max_nval = 1, max_npw = 1;
-    for (int i = 0; i < cnt; ++i) {
-      const SolveReq& r = reqs[order[i0 + i]];
+    Chunk ch{(int)i0, (int)(i1 - i0), max_n, 1, 1};
+    long long h = 0, sc = 0;
+    for (size_t i = i0; i < i1; ++i) {
+      const SolveReq& r = reqs[order[i]];
       if (r.nval > r.n || r.nvec > r.nval) throw CudaFail("too many eigenvalues requested", PMX_ERR_INVALID);
       pmx::dev::EigItem& it = items[i];
       it = pmx::dev::EigItem{};
@@ -1904,46 +1912,73 @@ void solve_multi(pmx_ctx* c, const pmx::dev::CrystalDev* table, std::vector<Solv
       it.nval = r.nval;
       it.want_vec = r.nvec > 0 ? 1 : 0;
       for (int x = 0; x < 3; ++x) it.k[x] = r.k[x];
-      it.h_off = h;
-      it.w_off = w;
+      it.h_off = h;   // the H workspace and the scratch are reused chunk after chunk
+      it.w_off = w;   // eigenvalues of all chunks side by side
       it.z_off = r.z_off;
       it.s_off = sc;
       h += (long long)r.n * r.n;
       w += r.nval;
       sc += (long long)pmx::dev::heev_scratch_doubles(r.n, r.nvec, max_n);
-      max_nval = std::max(max_nval, r.nval);
-      max_npw = std::max(max_npw, r.npw);
+      ch.max_nval = std::max(ch.max_nval, r.nval);
+      ch.max_npw = std::max(ch.max_npw, r.npw);
     }
-    CK(c->hbuf.ensure(sizeof(double2) * (size_t)h));
-    CK(c->wbuf.ensure(sizeof(double) * (size_t)w));
-    CK(c->scratch.ensure(sizeof(double) * (size_t)sc));
-    CK(c->info.ensure(sizeof(int) * cnt));
-    h2d(c, c->items, items.data(), sizeof(pmx::dev::EigItem) * cnt);
-    {
-      KTime kt(c, "assemble");
-      CK(pmx::dev::launch_assemble(table, c->items.as<pmx::dev::EigItem>(), cnt, max_npw, c->hbuf.as<double2>(),
-                                   c->stream));
-    }
-    {
-      KTime kt(c, "heev");
-      CK(pmx::dev::launch_heev(c->items.as<pmx::dev::EigItem>(), cnt, max_n, max_nval, c->hbuf.as<double2>(),
-                               c->wbuf.as<double>(), zbase ? zbase : c->hbuf.as<double2>(), c->scratch.as<double>(),
-                               c->info.as<int>(), c->stream, 0));
-    }
-    c->launches += 2;
-    std::vector<int> info(cnt);
-    std::vector<double> wv((size_t)w);
-    CK(cudaMemcpyAsync(info.data(), c->info.ptr, sizeof(int) * cnt, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaMemcpyAsync(wv.data(), c->wbuf.ptr, sizeof(double) * wv.size(), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    c->d2h += (long long)(sizeof(int) * cnt + sizeof(double) * wv.size());
-    for (int i = 0; i < cnt; ++i) {
-      if (info[i] != 0)
-        throw CudaFail("eigensolver failed (status " + std::to_string(info[i]) + ")", PMX_ERR_NOCONV);
-      const SolveReq& r = reqs[order[i0 + i]];
-      std::copy(wv.begin() + items[i].w_off, wv.begin() + items[i].w_off + r.nval, r.w);
-    }
+    hneed = std::max(hneed, h);
+    sneed = std::max(sneed, sc);
+    chunks.push_back(ch);
     i0 = i1;
+  }
+  const int nitems = (int)items.size();
+  CK(c->hbuf.ensure(sizeof(double2) * (size_t)hneed));
+  CK(c->wbuf.ensure(sizeof(double) * (size_t)w));
+  CK(c->scratch.ensure(sizeof(double) * (size_t)sneed));
+  CK(c->info.ensure(sizeof(int) * nitems));
+  h2d(c, c->items, items.data(), sizeof(pmx::dev::EigItem) * nitems);
+  pmx::dev::EigItem* dit = c->items.as<pmx::dev::EigItem>();
+  int* dinfo = c->info.as<int>();
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+  cudaError_t cap = cudaSuccess;
+  for (const Chunk& ch : chunks) {
+    cap = pmx::dev::launch_assemble(table, dit + ch.first, ch.cnt, ch.max_npw, c->hbuf.as<double2>(), c->stream);
+    if (cap != cudaSuccess) break;
+    cap = pmx::dev::launch_heev(dit + ch.first, ch.cnt, ch.max_n, ch.max_nval, c->hbuf.as<double2>(),
+                                c->wbuf.as<double>(), zbase ? zbase : c->hbuf.as<double2>(), c->scratch.as<double>(),
+                                dinfo + ch.first, c->stream, 0);
+    if (cap != cudaSuccess) break;
+  }
+  const cudaError_t end = cudaStreamEndCapture(c->stream, &graph);
+  CK(cap);
+  CK(end);
+  cudaError_t inst = cudaGraphInstantiate(&exec, graph, 0);
+  if (inst != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    CK(inst);
+  }
+  {
+    KTime kt(c, "solve_graph");
+    const cudaError_t e = cudaGraphLaunch(exec, c->stream);
+    if (e != cudaSuccess) {
+      cudaGraphExecDestroy(exec);
+      cudaGraphDestroy(graph);
+      CK(e);
+    }
+  }
+  c->launches += 2 * (long long)chunks.size();
+  std::vector<int> info(nitems);
+  std::vector<double> wv((size_t)w);
+  CK(cudaMemcpyAsync(info.data(), dinfo, sizeof(int) * nitems, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(wv.data(), c->wbuf.ptr, sizeof(double) * wv.size(), cudaMemcpyDeviceToHost, c->stream));
+  const cudaError_t sy = cudaStreamSynchronize(c->stream);
+  cudaGraphExecDestroy(exec);
+  cudaGraphDestroy(graph);
+  CK(sy);
+  c->d2h += (long long)(sizeof(int) * nitems + sizeof(double) * wv.size());
+  for (int i = 0; i < nitems; ++i) {
+    if (info[i] != 0)
+      throw CudaFail("eigensolver failed (status " + std::to_string(info[i]) + ")", PMX_ERR_NOCONV);
+    const SolveReq& r = reqs[order[i]];
+    std::copy(wv.begin() + items[i].w_off, wv.begin() + items[i].w_off + r.nval, r.w);
   }
 }
 
