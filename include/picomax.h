@@ -119,6 +119,11 @@ int pmx_ctx_overlap_error(const pmx_ctx* ctx, double* max_abs2_err, double* max_
  * batch of at least 148 matrices of a given size times every schedule once,
  * keeps the fastest for the rest of the context's life. New in this build. */
 int pmx_ctx_set_autotune(pmx_ctx* ctx, int on);
+/* Fixes the eigensolver schedule (0 = direct loads, then the prefetch and
+ * shared-memory-partials schedules the matrix size allows; an index beyond
+ * the last one means the last) for every later batch; -1 returns to the
+ * autotuner. For tests that compare the schedules. New in this build. */
+int pmx_ctx_set_schedule(pmx_ctx* ctx, int schedule);
 /* The autotuner's choices and trial times as JSON text (NUL-terminated,
  * truncated at len; full length in *needed). */
 int pmx_ctx_tuning(const pmx_ctx* ctx, char* buf, size_t len, size_t* needed);

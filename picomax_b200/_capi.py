@@ -37,7 +37,7 @@ EXPORTS = (
     "pmx_ctx_stage_times", "pmx_ctx_kernel_launches", "pmx_hamiltonian", "pmx_heev_batched",
     "pmx_ref_energy", "pmx_band", "pmx_chi", "pmx_kk", "pmx_main", "pmx_ctx_stream",
     "pmx_ctx_transfer_bytes", "pmx_ctx_degenerate_cuts", "pmx_chi_device", "pmx_chi_epsm",
-    "pmx_eps_macroscopic", "pmx_ctx_kernel_time", "pmx_ctx_set_autotune", "pmx_ctx_tuning",
+    "pmx_eps_macroscopic", "pmx_ctx_kernel_time", "pmx_ctx_set_autotune", "pmx_ctx_set_schedule", "pmx_ctx_tuning",
     "pmx_ctx_overlap_error",
     "pmx_heev_batched_noalloc",
     "pmx_problem_params",
@@ -109,6 +109,7 @@ def load() -> ctypes.CDLL:
         "pmx_eps_macroscopic": (c_int, [c_void_p, c_int, c_int, c_int, dp, dp, dp]),
         "pmx_ctx_kernel_time": (c_int, [c_void_p, c_char_p, dp, POINTER(c_longlong)]),
         "pmx_ctx_set_autotune": (c_int, [c_void_p, c_int]),
+        "pmx_ctx_set_schedule": (c_int, [c_void_p, c_int]),
         "pmx_ctx_overlap_error": (c_int, [c_void_p, dp, dp]),
         "pmx_heev_batched_noalloc": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
         "pmx_problem_params": (c_int, [c_void_p, dp, ip]),
@@ -306,6 +307,10 @@ class Context:
 
     def set_autotune(self, on: bool):
         self._lib.pmx_ctx_set_autotune(self.handle, 1 if on else 0)
+
+    def set_schedule(self, schedule: int):
+        """Fix the eigensolver schedule for later batches (-1: autotuner)."""
+        self._check(self._lib.pmx_ctx_set_schedule(self.handle, schedule), "set_schedule")
 
     def tuning(self) -> dict:
         import json

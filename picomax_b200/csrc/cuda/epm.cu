@@ -180,7 +180,9 @@ __host__ __device__ inline size_t heev_smem_bytes(int n, int nev, bool resident,
 // per-lane registers, column dots by warp reduction) and v^H A v; finally
 // w = tau y - tau^2/2 (v^H A v) v becomes the pending update. Three barriers
 // per step. MAXS = ceil(n / 32) register slots per lane.
-template <int MAXS, int RING, class Acc>
+// YS: the per-lane row partials of y accumulate in the warp's row of part[]
+// (shared memory) instead of registers, for schedules with more CTAs per SM.
+template <int MAXS, int RING, class Acc, bool YS = false>
 __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, double2* wprev, double2* vcur,
                                               double2* dotp, double2* tau, double2* part, double2* cnext,
                                               double2* wring, double* d, double* e, double* red) {
@@ -234,9 +236,16 @@ __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, do
     const double2 tj = tau[j];
     const bool active = tj.x != 0.0 || tj.y != 0.0;
     // ---- B: fused pass over the trailing lower triangle
-    double2 yreg[MAXS];
+    double2 yreg[YS ? 1 : MAXS];
 #pragma unroll
-    for (int s = 0; s < MAXS; ++s) yreg[s] = make_double2(0, 0);
+    for (int s = 0; s < (YS ? 1 : MAXS); ++s) yreg[s] = make_double2(0, 0);
+    if (YS) {
+#pragma unroll
+      for (int s = 0; s < MAXS; ++s) {
+        const int r = 32 * s + lane;
+        if (r >= j + 1 && r < n) part[wid * n + r] = make_double2(0, 0);
+      }
+    }
     double vhav = 0.0;
     if (active || pending) {
       // Columns c = c0 + kWarps t of this warp. With RING > 0 every lane
@@ -304,7 +313,10 @@ __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, do
               cnext[r] = v;
             }
             if (active) {
-              yreg[s] = cadd(yreg[s], cmul(v, vc));
+              if (YS)
+                part[wid * n + r] = cadd(part[wid * n + r], cmul(v, vc));
+              else
+                yreg[YS ? 0 : s] = cadd(yreg[YS ? 0 : s], cmul(v, vc));
               if (r > c) dot = cadd(dot, cmulc(v, vcur[r]));
             }
           }
@@ -327,8 +339,8 @@ __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, do
       for (int s = 0; s < MAXS; ++s) {
         const int r = 32 * s + lane;
         if (r >= j + 1 && r < n) {
-          part[wid * n + r] = yreg[s];
-          vrow += cmulc(vcur[r], yreg[s]).x;
+          if (!YS) part[wid * n + r] = yreg[YS ? 0 : s];
+          vrow += cmulc(vcur[r], part[wid * n + r]).x;
         }
       }
       vhav = warp_sum(vrow) + vhav;
@@ -365,8 +377,10 @@ __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, do
   __syncthreads();
 }
 
-template <bool RESIDENT, int MAXS, int RING>
-__global__ void __launch_bounds__(kHeevThreads, (RING >= 2 || MAXS > 9) ? 1 : 2) heev_kernel(const EigItem* __restrict__ items,
+// OCC > 0 overrides the number of resident CTAs per SM the registers are sized
+// for; YS keeps the row partials in shared memory (see tridiag_lower).
+template <bool RESIDENT, int MAXS, int RING, int OCC = 0, bool YS = false>
+__global__ void __launch_bounds__(kHeevThreads, OCC > 0 ? OCC : ((RING >= 2 || MAXS > 9) ? 1 : 2)) heev_kernel(const EigItem* __restrict__ items,
                                                                double2* __restrict__ hbuf,
                                                                double* __restrict__ wbuf,
                                                                double2* __restrict__ zbuf,
@@ -415,7 +429,8 @@ __global__ void __launch_bounds__(kHeevThreads, (RING >= 2 || MAXS > 9) ? 1 : 2)
     __syncthreads();
     tridiag_lower<MAXS, 0>(pk, n, vprev, wprev, vcur, dotp, tau, part, cnext, wring, d, e, red);
   } else {
-    tridiag_lower<MAXS, RING>(LowerFull{hbuf + it.h_off, n}, n, vprev, wprev, vcur, dotp, tau, part, cnext, wring,
+    tridiag_lower<MAXS, RING, LowerFull, YS>(LowerFull{hbuf + it.h_off, n}, n, vprev, wprev, vcur, dotp, tau, part,
+                                             cnext, wring,
                               d, e, red);
   }
 
@@ -620,27 +635,44 @@ int heev_smem_max_n() {
 }
 
 namespace {
-template <bool RES, int MAXS, int RING>
+template <bool RES, int MAXS, int RING, int OCC = 0, bool YS = false>
 cudaError_t heev_launch_t(const EigItem* items, int nitems, size_t smem, double2* hbuf, double* wbuf,
                           double2* zbuf, double* scratch, int* info, cudaStream_t st, double* tri) {
-  cudaError_t err =
-      cudaFuncSetAttribute(heev_kernel<RES, MAXS, RING>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t err = cudaFuncSetAttribute(heev_kernel<RES, MAXS, RING, OCC, YS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
-  heev_kernel<RES, MAXS, RING><<<nitems, kHeevThreads, smem, st>>>(items, hbuf, wbuf, zbuf, scratch, info, tri);
+  heev_kernel<RES, MAXS, RING, OCC, YS><<<nitems, kHeevThreads, smem, st>>>(items, hbuf, wbuf, zbuf, scratch, info,
+                                                                            tri);
   return cudaGetLastError();
 }
 }  // namespace
 
-int heev_variants(int max_n, int max_nev) {
+namespace {
+// schedules 0 (direct) and, when their shared memory fits, 1 and 2 (prefetch rings)
+int heev_ring_variants(int max_n, int max_nev) {
   const int slots = (max_n + 31) / 32;
   if (max_n <= heev_smem_max_n() && heev_resident(max_n, max_nev)) return 1;  // resident: one variant
   if (slots > 13) return 1;  // one CTA per SM already
-  // the prefetch rings only count while their shared memory fits the opt-in limit
   const int maxs = slots <= 2 ? 2 : slots <= 4 ? 4 : slots <= 6 ? 6 : slots <= 9 ? 9 : 13;
   const size_t lim = 227 * 1024;
   if (heev_smem_bytes(max_n, max_nev, false, maxs, 1) > lim) return 1;
   if (heev_smem_bytes(max_n, max_nev, false, maxs, 3) > lim) return 2;
   return 3;
+}
+// one more schedule: row partials in shared memory and one CTA more per SM
+// (3 for the 9-slot class and below, 2 for the 13-slot class), when the
+// shared memory of that many CTAs fits
+int heev_ys_occupancy(int max_n, int max_nev) {
+  const int slots = (max_n + 31) / 32;
+  if ((max_n <= heev_smem_max_n() && heev_resident(max_n, max_nev)) || slots > 13) return 0;
+  const int occ = slots <= 9 ? 3 : 2;
+  const int maxs = slots <= 2 ? 2 : slots <= 4 ? 4 : slots <= 6 ? 6 : slots <= 9 ? 9 : 13;
+  return (size_t)occ * (heev_smem_bytes(max_n, max_nev, false, maxs, 0) + 1024) <= (size_t)228 * 1024 ? occ : 0;
+}
+}  // namespace
+
+int heev_variants(int max_n, int max_nev) {
+  return heev_ring_variants(max_n, max_nev) + (heev_ys_occupancy(max_n, max_nev) ? 1 : 0);
 }
 
 cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev, double2* hbuf,
@@ -650,14 +682,19 @@ cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev
   const bool resident = max_n <= heev_smem_max_n() && heev_resident(max_n, max_nev);
   const int slots = (max_n + 31) / 32;
   // global-memory path variants: 0 = direct L2 loads (2 CTAs/SM), 1 = one-column
-  // prefetch buffer per warp (2 CTAs/SM), 2 = three-column ring (1 CTA/SM).
+  // prefetch buffer per warp (2 CTAs/SM), 2 = three-column ring (1 CTA/SM),
+  // last = direct with the row partials in shared memory and one CTA more per SM.
   // Measured on n = 274 (B200): 82 / 95 / 108 ms per 1787 matrices; a
   // one-CTA-per-SM padding of schedule 0 (L2-resident trailing blocks), a
   // register cap for 3 CTAs/SM and a two-columns-per-iteration pass were
   // slower still (120 / 106 / 97 ms): the pass is bound by dependent FP64
   // chains and load latency at 16 warps per SM. For n = 401 (one CTA per SM by
-  // registers) a register cap for two CTAs per SM was slower too (159 vs 141 ms).
-  const int ring = resident ? 0 : (variant == 1 ? 1 : (variant == 2 ? 3 : 0));
+  // registers) a register cap for two CTAs per SM was slower too (159 vs 141 ms),
+  // while the row partials in shared memory at two CTAs per SM are faster:
+  // eigenvalues of 1787 matrices, n = 362 / 401: 108 -> 80 ms, 115 -> 83 ms;
+  // at n = 274 and three CTAs per SM 71 vs 68 ms.
+  const bool ys = !resident && heev_ys_occupancy(max_n, max_nev) > 0 && variant == heev_ring_variants(max_n, max_nev);
+  const int ring = (resident || ys) ? 0 : (variant == 1 ? 1 : (variant == 2 ? 3 : 0));
 #define PMX_HEEV(S)                                                                                          \
   if (slots <= S) {                                                                                          \
     if (resident)                                                                                            \
@@ -671,6 +708,10 @@ cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev
       return heev_launch_t<false, S, (S <= 13 ? 1 : 0)>(items, nitems,                                        \
                                                         heev_smem_bytes(max_n, max_nev, false, S, 1), hbuf,   \
                                                         wbuf, zbuf, scratch, info, st, tri);                      \
+    if (ys && S <= 13)                                                                                       \
+      return heev_launch_t<false, S, 0, (S <= 9 ? 3 : 2), true>(items, nitems,                                \
+                                                                heev_smem_bytes(max_n, max_nev, false, S, 0),  \
+                                                                hbuf, wbuf, zbuf, scratch, info, st, tri);    \
     return heev_launch_t<false, S, 0>(items, nitems, heev_smem_bytes(max_n, max_nev, false, S, 0), hbuf, wbuf, \
                                       zbuf, scratch, info, st, tri);                                              \
   }

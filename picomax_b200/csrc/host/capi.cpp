@@ -247,6 +247,7 @@ struct pmx_ctx {
   // autotuner: chosen eigensolver schedule per (n, nval, vectors) and the
   // device times measured when it was chosen
   bool autotune = true;
+  int fixed_schedule = -1;  // >= 0: this eigensolver schedule on every batch (clamped to the last one)
   std::map<long long, int> heev_choice;
   std::map<long long, std::vector<float>> heev_trials;
   // named workspaces
@@ -438,7 +439,9 @@ void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int 
     int variant = 0;
     const int nvar = pmx::dev::heev_variants(n, nval);
     auto it_choice = c->heev_choice.find(key);
-    if (it_choice != c->heev_choice.end()) {
+    if (c->fixed_schedule >= 0) {
+      variant = std::min(c->fixed_schedule, nvar - 1);
+    } else if (it_choice != c->heev_choice.end()) {
       variant = it_choice->second;
     } else if (nvar > 1 && c->autotune && cnt >= 148) {
       std::vector<float> ms(nvar, 0.f);
@@ -1156,6 +1159,12 @@ extern "C" int pmx_ctx_overlap_error(const pmx_ctx* c, double* max_abs2_err, dou
 extern "C" int pmx_ctx_set_autotune(pmx_ctx* c, int on) {
   if (!c) return PMX_ERR_INVALID;
   c->autotune = on != 0;
+  return PMX_OK;
+}
+
+extern "C" int pmx_ctx_set_schedule(pmx_ctx* c, int schedule) {
+  if (!c || schedule < -1) return PMX_ERR_INVALID;
+  c->fixed_schedule = schedule;
   return PMX_OK;
 }
 

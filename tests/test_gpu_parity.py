@@ -197,27 +197,58 @@ def test_degenerate_cut_reported(ctx, tmp_path):
     assert ctx.degenerate_cuts() >= 1
 
 
-def test_heev_schedules_agree(tmp_path):
+def _qvec(K):
+    return ",".join(f"{x:.6f}" for x in np.asarray(K).ravel())
+
+
+def test_heev_schedules_agree():
     """Every eigensolver schedule the autotuner can pick gives the same spectrum."""
     from conftest import gpu_available
     if not gpu_available():
         pytest.skip("no CUDA device")
-    from picomax_b200.kgrid import write_kfile
     g = load_golden("gaas_soc_band")
     args = [str(a) for a in g["argv"]]
-    # 200 k-points so that the autotuner runs (>= 148 matrices in one batch)
+    # 200 band points so that the autotuner runs (>= 148 matrices in one batch)
     rng = np.random.default_rng(5)
     K = rng.uniform(-0.5, 0.5, (200, 3))
-    kf = os.path.join(str(tmp_path), "k.txt")
-    write_kfile(kf, K, np.ones(len(K)))
-    args = [a for a in args if a not in ("band",)]
     base = args[args.index("-crystal"):]
-    p = pm.Problem(["-switch", "band", "-kpoint", "0", "-kpointfile", kf] + base)
+    base = base[:base.index("-qpath")] + base[base.index("-qnum") + 2:]
+    p = pm.Problem(["-switch", "band", "-qvec", _qvec(K)] + base)
     c1 = pm.Context(0)
     e1 = c1.band(p)  # autotuned (trial of every schedule on the first batch)
+    assert c1.tuning()["heev"], "the autotuner did not run"
     c2 = pm.Context(0)
     c2.set_autotune(False)
     e2 = c2.band(p)  # default schedule
+    assert e1.shape == (200, 16)
     assert np.max(np.abs(e1 - e2)) < 1e-10
     c1.close()
     c2.close()
+
+
+@pytest.mark.parametrize("encut", [120, 160])
+def test_heev_each_schedule(encut):
+    """Each fixed eigensolver schedule (direct, prefetch rings, row partials in
+    shared memory) against the oracle's spectrum on the global-memory path
+    (N_G 137 and 181 plane waves with spin-orbit: n = 274 and 362)."""
+    from conftest import gpu_available
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    from picomax_b200.workloads import gaas_form_factors
+    vg, socargs = gaas_form_factors()
+    rng = np.random.default_rng(17)
+    K = rng.uniform(-0.5, 0.5, (6, 3))
+    args = ["-switch", "band", "-crystal", "zb", "-a", "5.65", "-vg", vg, "-encut", str(encut), "-qvec", _qvec(K),
+            "-nband", "24", "-nvalence", "8"] + socargs
+    p = pm.Problem(args)
+    cr, mat, gcut, o = O.from_args(args)
+    G, _ = p.gvectors()
+    ref = O.band(cr, mat, G, p.qpoints(), 24, 8)
+    assert ref.shape == (6, 24)
+    for sched in range(4):
+        c = pm.Context(0)
+        c.set_schedule(sched)
+        e = c.band(p)
+        assert np.max(np.abs(e - ref)) < 1e-9, sched
+        c.close()
+    p.close()
