@@ -101,6 +101,38 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
+def _ref_run(binary, argv, lines, sample, tmp, env):
+    """One run of the reference binary on the first `sample` k-points of the
+    workload's k-point file: (k-dependent stage seconds, Kramers-Kronig seconds)."""
+    kfs = os.path.join(tmp, "k_sample.txt")
+    with open(kfs, "w") as fh:
+        fh.write(lines[0] + "\n" + str(sample) + "\n" + "\n".join(lines[2:2 + sample]) + "\n")
+    argv = list(argv)
+    argv[argv.index("-kpointfile") + 1] = kfs
+    r = subprocess.run([binary] + argv + ["-wdir", tmp, "-outputfile", "ref"], capture_output=True, text=True,
+                       env=env)
+    if r.returncode != 0:
+        raise RuntimeError(f"reference exited {r.returncode}")
+    el = [float(x) for x in re.findall(r"Elapsed time: ([0-9.eE+-]+) s", r.stdout)]
+    # stdout order: G list, k list, [k stage, (overlaps, accumulation, KK)], total
+    kk = el[5] if len(el) > 6 else 0.0
+    return el[2] + el[3] + el[4], kk
+
+
+def _ref_plan(binary, argv, lines, tmp, env, cores, target_s=15.0):
+    """Sample size for about target_s seconds of k-dependent reference work per
+    run: a first run on one k-point per host core (the reference's k loops are
+    OpenMP-parallel), scaled up in whole multiples of the core count. Returns
+    (sample, the first run's times when that run is the sample, else None)."""
+    nk_full = int(lines[1])
+    s0 = min(cores, nk_full)
+    t0 = _ref_run(binary, argv, lines, s0, tmp, env)
+    if t0[0] >= 0.5 * target_s or s0 == nk_full:
+        return s0, t0
+    grow = max(1, int(target_s / max(t0[0], 1e-3)))
+    return min(nk_full, s0 * grow), None
+
+
 def reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -111,31 +143,20 @@ def reference_arm(args, rank, world):
     if not os.path.exists(binary):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (needs the reference tree)"}))
         return
-    kf = argv[argv.index("-kpointfile") + 1]
-    lines = open(kf).read().splitlines()
+    lines = open(argv[argv.index("-kpointfile") + 1]).read().splitlines()
     nk_full = int(lines[1])
-    sample = 64 if nk_full > 64 else nk_full
-    kfs = os.path.join(tmp, "k_sample.txt")
-    with open(kfs, "w") as fh:
-        fh.write(lines[0] + "\n" + str(sample) + "\n" + "\n".join(lines[2:2 + sample]) + "\n")
-    argv = list(argv)
-    argv[argv.index("-kpointfile") + 1] = kfs
     cores = os.cpu_count()
     env = dict(os.environ, OMP_NUM_THREADS=str(cores))
-    times = []
-    for step in range(args.warmup + args.steps):
-        r = subprocess.run([binary] + argv + ["-wdir", tmp, "-outputfile", "ref"], capture_output=True,
-                           text=True, env=env)
-        if r.returncode != 0:
-            print(json.dumps({"impl": "reference", "unavailable": f"reference exited {r.returncode}"}))
-            return
-        el = [float(x) for x in re.findall(r"Elapsed time: ([0-9.eE+-]+) s", r.stdout)]
-        # stdout order: G list, k list, [k stage, (overlaps, accumulation, KK)], total
-        k_stage, ovl, acc = el[2], el[3], el[4]
-        kk = el[5] if len(el) > 6 else 0.0
-        full = (k_stage + ovl + acc) * (nk_full / sample) + kk
-        if step >= args.warmup:
-            times.append(full)
+    try:
+        sample, _ = _ref_plan(binary, argv, lines, tmp, env, cores)  # an extra, untimed warm-up run
+        times = []
+        for step in range(args.warmup + args.steps):
+            kdep, kk = _ref_run(binary, argv, lines, sample, tmp, env)
+            if step >= args.warmup:
+                times.append(kdep * (nk_full / sample) + kk)
+    except RuntimeError as e:
+        print(json.dumps({"impl": "reference", "unavailable": str(e)}))
+        return
     t = sum(times) / len(times)
     v = nspec / t
     print(json.dumps({
@@ -145,40 +166,34 @@ def reference_arm(args, rank, world):
         "config": {"workload": args.workload, "kpoints": nk_full},
         "cpu_baseline": {"value": v, "unit": "spectra/s", "cores": cores, "kind": "reference",
                          "sample": f"first {sample} of {nk_full} k-points per step; k-dependent stage times "
-                                   f"x{nk_full // sample}, Kramers-Kronig as measured"},
+                                   f"x{nk_full / sample:.2f}, Kramers-Kronig as measured"},
         "e2e": {"value": v, "unit": "spectra/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
     shutil.rmtree(tmp, ignore_errors=True)
 
 
 def cpu_baseline_sample(wl_argv, nspec):
-    """The reference on the host cores, 64-k-point sample of the workload (see reference_arm)."""
+    """The reference on the host cores, on a sample of the workload's k-points
+    sized for about 15 s of k-dependent work (see _ref_plan)."""
     binary = os.path.join(ROOT, "oracle", "_ref", "picomax_ref_ll" if "epsLL" in wl_argv else "picomax_ref_guard")
     if not os.path.exists(binary):
         return None
     tmp = tempfile.mkdtemp(prefix="pmx_cpu_")
-    kf = wl_argv[wl_argv.index("-kpointfile") + 1]
-    lines = open(kf).read().splitlines()
+    lines = open(wl_argv[wl_argv.index("-kpointfile") + 1]).read().splitlines()
     nk_full = int(lines[1])
-    sample = min(64, nk_full)
-    kfs = os.path.join(tmp, "k.txt")
-    with open(kfs, "w") as fh:
-        fh.write(lines[0] + "\n" + str(sample) + "\n" + "\n".join(lines[2:2 + sample]) + "\n")
-    argv = list(wl_argv)
-    argv[argv.index("-kpointfile") + 1] = kfs
     cores = os.cpu_count()
-    r = subprocess.run([binary] + argv + ["-wdir", tmp, "-outputfile", "ref"], capture_output=True, text=True,
-                       env=dict(os.environ, OMP_NUM_THREADS=str(cores)))
-    shutil.rmtree(tmp, ignore_errors=True)
-    if r.returncode != 0:
+    env = dict(os.environ, OMP_NUM_THREADS=str(cores))
+    try:
+        sample, res = _ref_plan(binary, wl_argv, lines, tmp, env, cores)
+        kdep, kk = res if res is not None else _ref_run(binary, wl_argv, lines, sample, tmp, env)
+    except RuntimeError:
         return None
-    el = [float(x) for x in re.findall(r"Elapsed time: ([0-9.eE+-]+) s", r.stdout)]
-    k_stage, ovl, acc = el[2], el[3], el[4]
-    kk = el[5] if len(el) > 6 else 0.0
-    full = (k_stage + ovl + acc) * (nk_full / sample) + kk
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    full = kdep * (nk_full / sample) + kk
     return {"value": nspec / full, "unit": "spectra/s", "cores": cores, "kind": "reference",
             "sample": f"reference (oracle/_ref, OpenMP) on the first {sample} of {nk_full} k-points; "
-                      f"k-dependent stages x{nk_full // sample}, Kramers-Kronig as measured"}
+                      f"k-dependent stages x{nk_full / sample:.2f}, Kramers-Kronig as measured"}
 
 
 def ours(args, rank, world):
