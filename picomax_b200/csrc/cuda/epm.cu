@@ -246,7 +246,7 @@ __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, do
         if (r >= j + 1 && r < n) part[wid * n + r] = make_double2(0, 0);
       }
     }
-    double vhav = 0.0;
+    double vhav = 0.0;  // the same on every lane
     if (active || pending) {
       // Columns c = c0 + kWarps t of this warp. With RING > 0 every lane
       // prefetches its own rows of the next RING columns into a per-warp ring
@@ -269,16 +269,10 @@ __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, do
           cp_async_commit();
         }
       };
-#pragma unroll
-      for (int t = 0; t < RING; ++t) issue(t);
-      for (int t = 0; c0 + kWarps * t < n; ++t) {
-        const int c = c0 + kWarps * t;
-        double2* cc = acc.col(c);
-        const double2 vc = vcur[c];
-        const double2 wcc = cconj(wprev[c]), vcc = cconj(vprev[c]);
-        // slots wholly above the diagonal (rows < c) or below the matrix are
-        // skipped with warp-uniform branches, not predicated
-        double2 a[MAXS];
+      // rows r >= c of column c (t-th of this warp) into a[]; slots wholly
+      // above the diagonal or below the matrix are skipped with warp-uniform
+      // branches, not predicated
+      auto load = [&](int c, int t, double2 (&a)[MAXS]) {
         if (RING > 0) {
           cp_async_wait<(RING > 0 ? RING - 1 : 0)>();
           const double2* buf = ring + (t % (RING > 0 ? RING : 1)) * 32 * MAXS;
@@ -289,6 +283,7 @@ __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, do
             if (32 * s + 31 >= c && 32 * s < n && r >= c && r < n) a[s] = buf[32 * s + lane];
           }
         } else {
+          const double2* cc = acc.col(c);
 #pragma unroll
           for (int s = 0; s < MAXS; ++s) {
             const int r = 32 * s + lane;
@@ -296,6 +291,12 @@ __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, do
             if (32 * s + 31 >= c && 32 * s < n && r >= c && r < n) a[s] = cc[r - c];
           }
         }
+      };
+      // pending update, store back, row partials of y, this lane's column dot
+      auto update = [&](int c, const double2 (&a)[MAXS]) {
+        double2* cc = acc.col(c);
+        const double2 vc = vcur[c];
+        const double2 wcc = cconj(wprev[c]), vcc = cconj(vprev[c]);
         double2 dot = make_double2(0, 0);
 #pragma unroll
         for (int s = 0; s < MAXS; ++s) {
@@ -321,12 +322,24 @@ __device__ __forceinline__ void tridiag_lower(Acc acc, int n, double2* vprev, do
             }
           }
         }
-        issue(t + RING);
+        return dot;
+      };
+      auto finish = [&](int c, double2 dot) {
         if (active) {
           dot = warp_sum2(dot);
           if (lane == 0) dotp[c] = dot;
-          vhav += cmulc(vc, dot).x;  // conj(v_c) (column part of y_c), same on every lane
+          vhav += cmulc(vcur[c], dot).x;  // conj(v_c) (column part of y_c), same on every lane
         }
+      };
+#pragma unroll
+      for (int t = 0; t < RING; ++t) issue(t);
+      for (int t = 0; c0 + kWarps * t < n; ++t) {
+        const int c = c0 + kWarps * t;
+        double2 a[MAXS];
+        load(c, t, a);
+        const double2 dot = update(c, a);
+        issue(t + RING);
+        finish(c, dot);
       }
       if (RING > 0) cp_async_wait<0>();
     }
@@ -570,50 +583,123 @@ __global__ void __launch_bounds__(kHeevThreads, OCC > 0 ? OCC : ((RING >= 2 || M
   __syncthreads();
   const int ncl = misc[0];
   const double tiny = DBL_EPSILON * fmax(tnorm, DBL_MIN);
+  // One thread per cluster; the four work arrays of the ncl clusters are
+  // interleaved (element i of cluster cl at [i * ncl + cl]) so that the
+  // threads of a warp, which step through the rows together, read and write
+  // consecutive addresses. 4 n ncl <= 4 n nvec doubles of the item's scratch.
   for (int cl = tid; cl < ncl; cl += nthr) {
-    double* u0 = scratch + it.s_off + (size_t)4 * n * cl;
-    double* u1 = u0 + n;
-    double* u2 = u1 + n;
-    double* x = u2 + n;
+    double* u0 = scratch + it.s_off + cl;
+    double* u1 = u0 + (size_t)n * ncl;
+    double* u2 = u1 + (size_t)n * ncl;
+    double* x = u2 + (size_t)n * ncl;
+    auto X = [&](int i) -> double& { return x[(size_t)i * ncl]; };
     for (int k = clus[cl]; k < clus[cl + 1]; ++k) {
-      for (int i = 0; i < n; ++i) x[i] = hash_uniform(((unsigned long long)blockIdx.x << 20) + k, i);
+      for (int i = 0; i < n; ++i) X(i) = hash_uniform(((unsigned long long)blockIdx.x << 20) + k, i);
       for (int iter = 0; iter < kInvIters; ++iter) {
-        tri_solve(d, e, n, lam[k], tiny, x, u0, u1, u2);
+        tri_solve(d, e, n, lam[k], tiny, x, u0, u1, u2, ncl);
         for (int kp = clus[cl]; kp < k; ++kp) {
           const double2* zp = zbuf + it.z_off + (size_t)kp * n;
           double s = 0.0;
-          for (int i = 0; i < n; ++i) s += zp[i].x * x[i];
-          for (int i = 0; i < n; ++i) x[i] -= s * zp[i].x;
+          for (int i = 0; i < n; ++i) s += zp[i].x * X(i);
+          for (int i = 0; i < n; ++i) X(i) -= s * zp[i].x;
         }
         double s = 0.0, mx = 0.0;
-        for (int i = 0; i < n; ++i) mx = fmax(mx, fabs(x[i]));
+        for (int i = 0; i < n; ++i) mx = fmax(mx, fabs(X(i)));
         if (!(mx > 0.0) || !isfinite(mx)) mx = 1.0;
         for (int i = 0; i < n; ++i) {
-          x[i] /= mx;
-          s += x[i] * x[i];
+          X(i) /= mx;
+          s += X(i) * X(i);
         }
         s = 1.0 / sqrt(s);
-        for (int i = 0; i < n; ++i) x[i] *= s;
+        for (int i = 0; i < n; ++i) X(i) *= s;
       }
       double2* zk = zbuf + it.z_off + (size_t)k * n;
-      for (int i = 0; i < n; ++i) zk[i] = make_double2(x[i], 0.0);
+      for (int i = 0; i < n; ++i) zk[i] = make_double2(X(i), 0.0);
     }
   }
   __syncthreads();
 
   // ----------------------------------------------------------- back-transform
   // x = H_0 H_1 ... H_{n-2} z ; one warp per eigenvector, no block barriers.
-  for (int k = wid; k < nvec; k += nw) {
-    double2* z = zbuf + it.z_off + (size_t)k * n;
-    for (int j = n - 2; j >= 0; --j) {
-      const double2 tj = tau[j];
-      if (tj.x == 0.0 && tj.y == 0.0) continue;
-      const double2* v = (RESIDENT ? LowerPacked{Apacked, n}.col(j) : LowerFull{hbuf + it.h_off, n}.col(j)) - j;
-      double2 s = make_double2(0, 0);
-      for (int r = j + 1 + lane; r < n; r += 32) s = cadd(s, cmulc(v[r], z[r]));
-      s = cmul(tj, warp_sum2(s));
-      for (int r = j + 1 + lane; r < n; r += 32) z[r] = csub(z[r], cmul(v[r], s));
+  if constexpr (!kPartG) {
+    // z in this warp's row of part[] (free after the reduction); the reflector
+    // v_j is read once per step into registers (slot q: row j + 1 + lane + 32 q),
+    // and where the registers allow, v_{j-1} is loaded while v_j is applied.
+    constexpr int kOcc = OCC > 0 ? OCC : ((RING >= 2 || MAXS > 9) ? 1 : 2);
+    constexpr int kRegs = 65536 / (kHeevThreads * kOcc) < 255 ? 65536 / (kHeevThreads * kOcc) : 255;
+    constexpr bool kPf = 8 * MAXS + 48 <= kRegs;
+    double2* zs = part + (size_t)wid * n;
+    auto vcol = [&](int j) {
+      return RESIDENT ? LowerPacked{Apacked, n}.col(j) : LowerFull{hbuf + it.h_off, n}.col(j);
+    };
+    for (int k = wid; k < nvec; k += nw) {
+      double2* zg = zbuf + it.z_off + (size_t)k * n;
+      for (int r = lane; r < n; r += 32) zs[r] = zg[r];
       __syncwarp();
+      double2 vr[MAXS], vn[kPf ? MAXS : 1];
+#pragma unroll
+      for (int q = 0; q < MAXS; ++q) {
+        const int r = n - 1 + lane + 32 * q;  // column j = n - 2 (none for n = 1)
+        vr[q] = make_double2(0, 0);
+        if (n >= 2 && n - 1 + 32 * q < n && r < n) vr[q] = vcol(n - 2)[r - (n - 2)];
+      }
+      for (int j = n - 2; j >= 0; --j) {
+        if (kPf && j > 0) {
+          const double2* vp = vcol(j - 1);
+#pragma unroll
+          for (int q = 0; q < (kPf ? MAXS : 1); ++q) {
+            const int r = j + lane + 32 * q;
+            vn[q] = make_double2(0, 0);
+            if (j + 32 * q < n && r < n) vn[q] = vp[r - (j - 1)];
+          }
+        }
+        const double2 tj = tau[j];
+        if (tj.x != 0.0 || tj.y != 0.0) {
+          double2 sacc = make_double2(0, 0);
+#pragma unroll
+          for (int q = 0; q < MAXS; ++q) {
+            const int r = j + 1 + lane + 32 * q;
+            if (j + 1 + 32 * q < n && r < n) sacc = cadd(sacc, cmulc(vr[q], zs[r]));
+          }
+          sacc = cmul(tj, warp_sum2(sacc));
+#pragma unroll
+          for (int q = 0; q < MAXS; ++q) {
+            const int r = j + 1 + lane + 32 * q;
+            if (j + 1 + 32 * q < n && r < n) zs[r] = csub(zs[r], cmul(vr[q], sacc));
+          }
+        }
+        if (j > 0) {
+          if (kPf) {
+#pragma unroll
+            for (int q = 0; q < MAXS; ++q) vr[q] = vn[kPf ? q : 0];
+          } else {
+            const double2* vp = vcol(j - 1);
+#pragma unroll
+            for (int q = 0; q < MAXS; ++q) {
+              const int r = j + lane + 32 * q;
+              vr[q] = make_double2(0, 0);
+              if (j + 32 * q < n && r < n) vr[q] = vp[r - (j - 1)];
+            }
+          }
+        }
+      }
+      __syncwarp();
+      for (int r = lane; r < n; r += 32) zg[r] = zs[r];
+      __syncwarp();
+    }
+  } else {
+    for (int k = wid; k < nvec; k += nw) {
+      double2* z = zbuf + it.z_off + (size_t)k * n;
+      for (int j = n - 2; j >= 0; --j) {
+        const double2 tj = tau[j];
+        if (tj.x == 0.0 && tj.y == 0.0) continue;
+        const double2* v = (RESIDENT ? LowerPacked{Apacked, n}.col(j) : LowerFull{hbuf + it.h_off, n}.col(j)) - j;
+        double2 s = make_double2(0, 0);
+        for (int r = j + 1 + lane; r < n; r += 32) s = cadd(s, cmulc(v[r], z[r]));
+        s = cmul(tj, warp_sum2(s));
+        for (int r = j + 1 + lane; r < n; r += 32) z[r] = csub(z[r], cmul(v[r], s));
+        __syncwarp();
+      }
     }
   }
   if (tid == 0) info[blockIdx.x] = 0;
@@ -641,38 +727,67 @@ cudaError_t heev_launch_t(const EigItem* items, int nitems, size_t smem, double2
   cudaError_t err = cudaFuncSetAttribute(heev_kernel<RES, MAXS, RING, OCC, YS>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
-  heev_kernel<RES, MAXS, RING, OCC, YS><<<nitems, kHeevThreads, smem, st>>>(items, hbuf, wbuf, zbuf, scratch, info,
-                                                                            tri);
+  heev_kernel<RES, MAXS, RING, OCC, YS><<<nitems, kHeevThreads, smem, st>>>(items, hbuf, wbuf, zbuf, scratch,
+                                                                                 info, tri);
   return cudaGetLastError();
 }
 }  // namespace
 
 namespace {
-// schedules 0 (direct) and, when their shared memory fits, 1 and 2 (prefetch rings)
-int heev_ring_variants(int max_n, int max_nev) {
-  const int slots = (max_n + 31) / 32;
-  if (max_n <= heev_smem_max_n() && heev_resident(max_n, max_nev)) return 1;  // resident: one variant
-  if (slots > 13) return 1;  // one CTA per SM already
-  const int maxs = slots <= 2 ? 2 : slots <= 4 ? 4 : slots <= 6 ? 6 : slots <= 9 ? 9 : 13;
-  const size_t lim = 227 * 1024;
-  if (heev_smem_bytes(max_n, max_nev, false, maxs, 1) > lim) return 1;
-  if (heev_smem_bytes(max_n, max_nev, false, maxs, 3) > lim) return 2;
-  return 3;
+// register slots per lane (template MAXS) for ceil(n / 32) slots; 0 beyond n = 1216
+int heev_slot_class(int slots) {
+  const int cls[] = {2, 4, 6, 9, 13, 19, 26, 38};
+  for (int c : cls)
+    if (slots <= c) return c;
+  return 0;
 }
-// one more schedule: row partials in shared memory and one CTA more per SM
-// (3 for the 9-slot class and below, 2 for the 13-slot class), when the
-// shared memory of that many CTAs fits
-int heev_ys_occupancy(int max_n, int max_nev) {
+
+// One schedule of the global-memory path: prefetch ring depth, row partials in
+// shared memory (YS).
+struct HeevSched {
+  int ring;
+  bool ys;
+};
+
+// The schedules a matrix size allows, in autotuner order: 0 direct loads,
+// then (n <= 416) the prefetch rings whose shared memory fits (one-column,
+// three-column) and the row partials in shared memory with one CTA more per SM.
+int heev_schedules(int max_n, int max_nev, HeevSched* out) {
   const int slots = (max_n + 31) / 32;
-  if ((max_n <= heev_smem_max_n() && heev_resident(max_n, max_nev)) || slots > 13) return 0;
-  const int occ = slots <= 9 ? 3 : 2;
-  const int maxs = slots <= 2 ? 2 : slots <= 4 ? 4 : slots <= 6 ? 6 : slots <= 9 ? 9 : 13;
-  return (size_t)occ * (heev_smem_bytes(max_n, max_nev, false, maxs, 0) + 1024) <= (size_t)228 * 1024 ? occ : 0;
+  int k = 0;
+  out[k++] = {0, false};
+  if (max_n <= heev_smem_max_n() && heev_resident(max_n, max_nev)) return k;  // resident: one schedule
+  const int maxs = heev_slot_class(slots);
+  const size_t lim = 227 * 1024;
+  if (maxs <= 13) {
+    if (heev_smem_bytes(max_n, max_nev, false, maxs, 1) <= lim) out[k++] = {1, false};
+    if (heev_smem_bytes(max_n, max_nev, false, maxs, 3) <= lim) out[k++] = {3, false};
+    const int ctas = maxs <= 9 ? 3 : 2;
+    if ((size_t)ctas * (heev_smem_bytes(max_n, max_nev, false, maxs, 0) + 1024) <= (size_t)228 * 1024)
+      out[k++] = {0, true};
+  }
+  return k;
+}
+
+template <int S>
+cudaError_t heev_dispatch(bool resident, const HeevSched& sc, const EigItem* items, int nitems, size_t smem,
+                          double2* hbuf, double* wbuf, double2* zbuf, double* scratch, int* info, cudaStream_t st,
+                          double* tri) {
+  if (resident) return heev_launch_t<true, S, 0>(items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
+  if constexpr (S <= 13) {
+    if (sc.ring == 3) return heev_launch_t<false, S, 3>(items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
+    if (sc.ring == 1) return heev_launch_t<false, S, 1>(items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
+    if (sc.ys)
+      return heev_launch_t<false, S, 0, (S <= 9 ? 3 : 2), true>(items, nitems, smem, hbuf, wbuf, zbuf, scratch, info,
+                                                                st, tri);
+  }
+  return heev_launch_t<false, S, 0>(items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
 }
 }  // namespace
 
 int heev_variants(int max_n, int max_nev) {
-  return heev_ring_variants(max_n, max_nev) + (heev_ys_occupancy(max_n, max_nev) ? 1 : 0);
+  HeevSched sc[8];
+  return heev_schedules(max_n, max_nev, sc);
 }
 
 cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev, double2* hbuf,
@@ -681,9 +796,9 @@ cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev
   if (nitems <= 0) return cudaSuccess;
   const bool resident = max_n <= heev_smem_max_n() && heev_resident(max_n, max_nev);
   const int slots = (max_n + 31) / 32;
-  // global-memory path variants: 0 = direct L2 loads (2 CTAs/SM), 1 = one-column
-  // prefetch buffer per warp (2 CTAs/SM), 2 = three-column ring (1 CTA/SM),
-  // last = direct with the row partials in shared memory and one CTA more per SM.
+  // global-memory path schedules (heev_schedules): direct L2 loads (2 CTAs/SM),
+  // one-column prefetch buffer per warp (2 CTAs/SM), three-column ring (1 CTA/SM),
+  // direct with the row partials in shared memory and one CTA more per SM.
   // Measured on n = 274 (B200): 82 / 95 / 108 ms per 1787 matrices; a
   // one-CTA-per-SM padding of schedule 0 (L2-resident trailing blocks), a
   // register cap for 3 CTAs/SM and a two-columns-per-iteration pass were
@@ -691,40 +806,28 @@ cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev
   // chains and load latency at 16 warps per SM. For n = 401 (one CTA per SM by
   // registers) a register cap for two CTAs per SM was slower too (159 vs 141 ms),
   // while the row partials in shared memory at two CTAs per SM are faster:
-  // eigenvalues of 1787 matrices, n = 362 / 401: 108 -> 80 ms, 115 -> 83 ms;
-  // at n = 274 and three CTAs per SM 71 vs 68 ms.
-  const bool ys = !resident && heev_ys_occupancy(max_n, max_nev) > 0 && variant == heev_ring_variants(max_n, max_nev);
-  const int ring = (resident || ys) ? 0 : (variant == 1 ? 1 : (variant == 2 ? 3 : 0));
-#define PMX_HEEV(S)                                                                                          \
-  if (slots <= S) {                                                                                          \
-    if (resident)                                                                                            \
-      return heev_launch_t<true, S, 0>(items, nitems, heev_smem_bytes(max_n, max_nev, true), hbuf, wbuf, zbuf, \
-                                       scratch, info, st, tri);                                                   \
-    if (ring == 3 && S <= 13)                                                                                \
-      return heev_launch_t<false, S, (S <= 13 ? 3 : 0)>(items, nitems,                                        \
-                                                        heev_smem_bytes(max_n, max_nev, false, S, 3), hbuf,   \
-                                                        wbuf, zbuf, scratch, info, st, tri);                      \
-    if (ring == 1 && S <= 13)                                                                                \
-      return heev_launch_t<false, S, (S <= 13 ? 1 : 0)>(items, nitems,                                        \
-                                                        heev_smem_bytes(max_n, max_nev, false, S, 1), hbuf,   \
-                                                        wbuf, zbuf, scratch, info, st, tri);                      \
-    if (ys && S <= 13)                                                                                       \
-      return heev_launch_t<false, S, 0, (S <= 9 ? 3 : 2), true>(items, nitems,                                \
-                                                                heev_smem_bytes(max_n, max_nev, false, S, 0),  \
-                                                                hbuf, wbuf, zbuf, scratch, info, st, tri);    \
-    return heev_launch_t<false, S, 0>(items, nitems, heev_smem_bytes(max_n, max_nev, false, S, 0), hbuf, wbuf, \
-                                      zbuf, scratch, info, st, tri);                                              \
+  // eigenvalues of 778 matrices, n = 401: 115 -> 83 ms (1787 matrices of
+  // n = 362: 108 -> 80 ms); at n = 274 and three CTAs per SM 71 vs 68 ms.
+  // Two further forms were slower on every size: the column dots of four
+  // columns reduced in one transposed butterfly (n = 274 / 401: 75 / 113 ms
+  // against 68 / 115), and two columns per warp iteration with the partials
+  // in shared memory (83 / 150 ms against 65 / 87).
+  HeevSched sc[8];
+  const int nsc = heev_schedules(max_n, max_nev, sc);
+  const HeevSched sched = sc[std::min(std::max(variant, 0), nsc - 1)];
+  const size_t smem = heev_smem_bytes(max_n, max_nev, resident, resident ? 0 : heev_slot_class(slots),
+                                      resident ? 0 : sched.ring);
+  switch (heev_slot_class(slots)) {
+    case 2: return heev_dispatch<2>(resident, sched, items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
+    case 4: return heev_dispatch<4>(resident, sched, items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
+    case 6: return heev_dispatch<6>(resident, sched, items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
+    case 9: return heev_dispatch<9>(resident, sched, items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
+    case 13: return heev_dispatch<13>(resident, sched, items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
+    case 19: return heev_dispatch<19>(resident, sched, items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
+    case 26: return heev_dispatch<26>(resident, sched, items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
+    case 38: return heev_dispatch<38>(resident, sched, items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
+    default: return cudaErrorInvalidValue;  // n > 1216
   }
-  PMX_HEEV(2)
-  PMX_HEEV(4)
-  PMX_HEEV(6)
-  PMX_HEEV(9)
-  PMX_HEEV(13)
-  PMX_HEEV(19)
-  PMX_HEEV(26)
-  PMX_HEEV(38)
-#undef PMX_HEEV
-  return cudaErrorInvalidValue;  // n > 1216
 }
 
 }  // namespace dev

@@ -601,9 +601,12 @@ extern "C" int pmx_heev_batched(pmx_ctx* ctx, int n, int batch, const double* A,
     if (batch == 0) return (int)PMX_OK;
     CK(cudaMemcpyAsync(ctx->hbuf.ptr, A, hb * batch, cudaMemcpyHostToDevice, ctx->stream));
     h2d(ctx, ctx->items, items.data(), sizeof(pmx::dev::EigItem) * batch);
-    CK(pmx::dev::launch_heev(ctx->items.as<pmx::dev::EigItem>(), batch, n, nev, ctx->hbuf.as<double2>(),
-                             ctx->wbuf.as<double>(), ctx->zk.as<double2>(), ctx->scratch.as<double>(),
-                             ctx->info.as<int>(), ctx->stream));
+    {
+      KTime kt(ctx, "heev");
+      CK(pmx::dev::launch_heev(ctx->items.as<pmx::dev::EigItem>(), batch, n, nev, ctx->hbuf.as<double2>(),
+                               ctx->wbuf.as<double>(), ctx->zk.as<double2>(), ctx->scratch.as<double>(),
+                               ctx->info.as<int>(), ctx->stream, std::max(ctx->fixed_schedule, 0)));
+    }
     ctx->launches += 1;
     std::vector<int> info(batch);
     CK(cudaMemcpyAsync(info.data(), ctx->info.ptr, sizeof(int) * batch, cudaMemcpyDeviceToHost, ctx->stream));

@@ -229,7 +229,7 @@ def test_heev_schedules_agree():
 @pytest.mark.parametrize("encut", [120, 160])
 def test_heev_each_schedule(encut):
     """Each fixed eigensolver schedule (direct, prefetch rings, row partials in
-    shared memory) against the oracle's spectrum on the global-memory path
+    shared memory, grouped column-dot reductions) against the oracle's spectrum on the global-memory path
     (N_G 137 and 181 plane waves with spin-orbit: n = 274 and 362)."""
     from conftest import gpu_available
     if not gpu_available():
@@ -245,7 +245,7 @@ def test_heev_each_schedule(encut):
     G, _ = p.gvectors()
     ref = O.band(cr, mat, G, p.qpoints(), 24, 8)
     assert ref.shape == (6, 24)
-    for sched in range(4):
+    for sched in range(6):
         c = pm.Context(0)
         c.set_schedule(sched)
         e = c.band(p)
