@@ -723,10 +723,13 @@ int heev_smem_max_n() {
 namespace {
 template <bool RES, int MAXS, int RING, int OCC = 0, bool YS = false>
 cudaError_t heev_launch_t(const EigItem* items, int nitems, size_t smem, double2* hbuf, double* wbuf,
-                          double2* zbuf, double* scratch, int* info, cudaStream_t st, double* tri) {
+                          double2* zbuf, double* scratch, int* info, cudaStream_t st, double* tri, int* occ) {
   cudaError_t err = cudaFuncSetAttribute(heev_kernel<RES, MAXS, RING, OCC, YS>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
+  if (occ)  // resident CTAs per SM instead of a launch
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, heev_kernel<RES, MAXS, RING, OCC, YS>, kHeevThreads,
+                                                         smem);
   heev_kernel<RES, MAXS, RING, OCC, YS><<<nitems, kHeevThreads, smem, st>>>(items, hbuf, wbuf, zbuf, scratch,
                                                                                  info, tri);
   return cudaGetLastError();
@@ -772,17 +775,25 @@ int heev_schedules(int max_n, int max_nev, HeevSched* out) {
 template <int S>
 cudaError_t heev_dispatch(bool resident, const HeevSched& sc, const EigItem* items, int nitems, size_t smem,
                           double2* hbuf, double* wbuf, double2* zbuf, double* scratch, int* info, cudaStream_t st,
-                          double* tri) {
-  if (resident) return heev_launch_t<true, S, 0>(items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
+                          double* tri, int* occ) {
+  if (resident)
+    return heev_launch_t<true, S, 0>(items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri, occ);
   if constexpr (S <= 13) {
-    if (sc.ring == 3) return heev_launch_t<false, S, 3>(items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
-    if (sc.ring == 1) return heev_launch_t<false, S, 1>(items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
+    if (sc.ring == 3)
+      return heev_launch_t<false, S, 3>(items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri, occ);
+    if (sc.ring == 1)
+      return heev_launch_t<false, S, 1>(items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri, occ);
     if (sc.ys)
       return heev_launch_t<false, S, 0, (S <= 9 ? 3 : 2), true>(items, nitems, smem, hbuf, wbuf, zbuf, scratch, info,
-                                                                st, tri);
+                                                                st, tri, occ);
   }
-  return heev_launch_t<false, S, 0>(items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
+  return heev_launch_t<false, S, 0>(items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri, occ);
 }
+
+// Launch (occ == nullptr) or occupancy query of one schedule.
+cudaError_t heev_run(const EigItem* items, int nitems, int max_n, int max_nev, double2* hbuf, double* wbuf,
+                     double2* zbuf, double* scratch, int* info, cudaStream_t st, int variant, double* tri,
+                     int* occ);
 }  // namespace
 
 int heev_variants(int max_n, int max_nev) {
@@ -794,6 +805,37 @@ cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev
                         double* wbuf, double2* zbuf, double* scratch, int* info, cudaStream_t st, int variant,
                         double* tri) {
   if (nitems <= 0) return cudaSuccess;
+  return heev_run(items, nitems, max_n, max_nev, hbuf, wbuf, zbuf, scratch, info, st, variant, tri, nullptr);
+}
+
+int heev_batch_unit(int max_n, int max_nev) {
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
+    return 1;
+  int l = 1;
+  const int nv = heev_variants(max_n, max_nev);
+  for (int v = 0; v < nv; ++v) {
+    int occ = 0;
+    if (heev_run(nullptr, 0, max_n, max_nev, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, v, nullptr,
+                 &occ) != cudaSuccess ||
+        occ <= 0)
+      continue;
+    int a = l, b = occ;
+    while (b) {
+      const int t = a % b;
+      a = b;
+      b = t;
+    }
+    l = l / a * occ;
+  }
+  return l * sms;
+}
+
+namespace {
+cudaError_t heev_run(const EigItem* items, int nitems, int max_n, int max_nev, double2* hbuf, double* wbuf,
+                     double2* zbuf, double* scratch, int* info, cudaStream_t st, int variant, double* tri,
+                     int* occ) {
   const bool resident = max_n <= heev_smem_max_n() && heev_resident(max_n, max_nev);
   const int slots = (max_n + 31) / 32;
   // global-memory path schedules (heev_schedules): direct L2 loads (2 CTAs/SM),
@@ -818,17 +860,22 @@ cudaError_t launch_heev(const EigItem* items, int nitems, int max_n, int max_nev
   const size_t smem = heev_smem_bytes(max_n, max_nev, resident, resident ? 0 : heev_slot_class(slots),
                                       resident ? 0 : sched.ring);
   switch (heev_slot_class(slots)) {
-    case 2: return heev_dispatch<2>(resident, sched, items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
-    case 4: return heev_dispatch<4>(resident, sched, items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
-    case 6: return heev_dispatch<6>(resident, sched, items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
-    case 9: return heev_dispatch<9>(resident, sched, items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
-    case 13: return heev_dispatch<13>(resident, sched, items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
-    case 19: return heev_dispatch<19>(resident, sched, items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
-    case 26: return heev_dispatch<26>(resident, sched, items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
-    case 38: return heev_dispatch<38>(resident, sched, items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri);
+#define PMX_HEEV_CASE(S) \
+  case S:                \
+    return heev_dispatch<S>(resident, sched, items, nitems, smem, hbuf, wbuf, zbuf, scratch, info, st, tri, occ);
+    PMX_HEEV_CASE(2)
+    PMX_HEEV_CASE(4)
+    PMX_HEEV_CASE(6)
+    PMX_HEEV_CASE(9)
+    PMX_HEEV_CASE(13)
+    PMX_HEEV_CASE(19)
+    PMX_HEEV_CASE(26)
+    PMX_HEEV_CASE(38)
+#undef PMX_HEEV_CASE
     default: return cudaErrorInvalidValue;  // n > 1216
   }
 }
+}  // namespace
 
 }  // namespace dev
 }  // namespace pmx

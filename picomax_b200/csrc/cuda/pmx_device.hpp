@@ -63,6 +63,11 @@ int heev_smem_max_n();
 size_t heev_scratch_doubles(int n, int nvec, int max_n);
 // Number of schedules launch_heev offers for matrices of size max_n.
 int heev_variants(int max_n, int max_nev);
+// Batch size unit of the eigensolver on the current device: the SM count
+// times the least common multiple of the resident CTAs per SM of every
+// schedule for (max_n, max_nev). A batch that is a multiple of it fills every
+// wave of CTAs whichever schedule runs.
+int heev_batch_unit(int max_n, int max_nev);
 
 }  // namespace dev
 }  // namespace pmx

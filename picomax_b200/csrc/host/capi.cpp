@@ -260,7 +260,7 @@ struct pmx_ctx {
   // several crystals at once (batched entry points)
   DevBuf b_g, b_hkl, b_vloc, b_vso, b_crystal;
   double m2_err = 0.0, m2_max = 0.0;  // |M|^2 error of the mixed path's FP32 overlaps (last call)
-  cudaEvent_t ev[2] = {nullptr, nullptr};
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // 0-1 stage timers, 2-3 the autotuner
 };
 
 namespace {
@@ -402,6 +402,10 @@ void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int 
   const size_t hbytes = (size_t)n * n * sizeof(double2);
   int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)nk, ((size_t)2 << 30) / hbytes));
   chunk = std::min(chunk, 4096);
+  if (nk > chunk) {  // several chunks: each a whole number of waves of CTAs
+    const int unit = pmx::dev::heev_batch_unit(n, nval);
+    if (chunk >= unit) chunk = chunk / unit * unit;
+  }
   CK(c->hbuf.ensure(hbytes * chunk));
   CK(c->wbuf.ensure(sizeof(double) * (size_t)nk * nval));
   const size_t sstride = pmx::dev::heev_scratch_doubles(n, vec ? nvec : 0, n);
@@ -446,13 +450,13 @@ void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int 
     } else if (nvar > 1 && c->autotune && cnt >= 148) {
       std::vector<float> ms(nvar, 0.f);
       for (int v = 0; v < nvar; ++v) {
-        CK(cudaEventRecord(c->ev[0], c->stream));
+        CK(cudaEventRecord(c->ev[2], c->stream));
         CK(pmx::dev::launch_heev(c->items.as<pmx::dev::EigItem>(), cnt, n, nval, c->hbuf.as<double2>(),
                                  c->wbuf.as<double>(), vec ? zdev : c->hbuf.as<double2>(), c->scratch.as<double>(),
                                  c->info.as<int>(), c->stream, v));
-        CK(cudaEventRecord(c->ev[1], c->stream));
-        CK(cudaEventSynchronize(c->ev[1]));
-        CK(cudaEventElapsedTime(&ms[v], c->ev[0], c->ev[1]));
+        CK(cudaEventRecord(c->ev[3], c->stream));
+        CK(cudaEventSynchronize(c->ev[3]));
+        CK(cudaEventElapsedTime(&ms[v], c->ev[2], c->ev[3]));
         c->launches += 1;
         // H is overwritten by the reduction: rebuild it for the next candidate
         CK(pmx::dev::launch_assemble(dc.dev, c->items.as<pmx::dev::EigItem>(), cnt, dc.npw, c->hbuf.as<double2>(),
@@ -521,7 +525,8 @@ extern "C" int pmx_ctx_create(int device, pmx_ctx** out) {
   c->device = device;
   if (cudaSetDevice(device) != cudaSuccess) return PMX_ERR_CUDA;
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return PMX_ERR_CUDA;
-  if (cudaEventCreate(&c->ev[0]) != cudaSuccess || cudaEventCreate(&c->ev[1]) != cudaSuccess) return PMX_ERR_CUDA;
+  for (auto& e : c->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return PMX_ERR_CUDA;
   *out = c.release();
   return PMX_OK;
 }
@@ -1911,6 +1916,12 @@ void solve_multi(pmx_ctx* c, const pmx::dev::CrystalDev* table, std::vector<Solv
       hb += b;
       ++i1;
     }
+    if (i1 < order.size() && heev_class(reqs[order[i1]].n) == cls) {
+      // cut by the H or item limit with more of this class to come: a whole
+      // number of waves of CTAs
+      const int unit = pmx::dev::heev_batch_unit(max_n, reqs[order[i0]].nval);
+      if ((int)(i1 - i0) >= unit) i1 = i0 + (i1 - i0) / unit * unit;
+    }
     Chunk ch{(int)i0, (int)(i1 - i0), max_n, 1, 1};
     long long h = 0, sc = 0;
     for (size_t i = i0; i < i1; ++i) {
@@ -1947,16 +1958,49 @@ void solve_multi(pmx_ctx* c, const pmx::dev::CrystalDev* table, std::vector<Solv
   h2d(c, c->items, items.data(), sizeof(pmx::dev::EigItem) * nitems);
   pmx::dev::EigItem* dit = c->items.as<pmx::dev::EigItem>();
   int* dinfo = c->info.as<int>();
+  // eigensolver schedule per chunk: fixed, cached, or timed now (before the
+  // capture) on the first chunk of at least 148 matrices of its key; the
+  // trial results are recomputed by the graph
+  std::vector<int> variant(chunks.size(), 0);
+  for (size_t ci = 0; ci < chunks.size(); ++ci) {
+    const Chunk& ch = chunks[ci];
+    const bool vec = zbase != nullptr;
+    const long long key = ((long long)ch.max_n * 1024 + ch.max_nval) * 2 + (vec ? 1 : 0);
+    const int nvar = pmx::dev::heev_variants(ch.max_n, ch.max_nval);
+    auto cached = c->heev_choice.find(key);
+    if (c->fixed_schedule >= 0) {
+      variant[ci] = std::min(c->fixed_schedule, nvar - 1);
+    } else if (cached != c->heev_choice.end()) {
+      variant[ci] = cached->second;
+    } else if (nvar > 1 && c->autotune && ch.cnt >= 148) {
+      std::vector<float> ms(nvar, 0.f);
+      for (int v = 0; v < nvar; ++v) {
+        CK(pmx::dev::launch_assemble(table, dit + ch.first, ch.cnt, ch.max_npw, c->hbuf.as<double2>(), c->stream));
+        CK(cudaEventRecord(c->ev[2], c->stream));
+        CK(pmx::dev::launch_heev(dit + ch.first, ch.cnt, ch.max_n, ch.max_nval, c->hbuf.as<double2>(),
+                                 c->wbuf.as<double>(), zbase ? zbase : c->hbuf.as<double2>(),
+                                 c->scratch.as<double>(), dinfo + ch.first, c->stream, v));
+        CK(cudaEventRecord(c->ev[3], c->stream));
+        CK(cudaEventSynchronize(c->ev[3]));
+        CK(cudaEventElapsedTime(&ms[v], c->ev[2], c->ev[3]));
+        c->launches += 2;
+      }
+      variant[ci] = (int)(std::min_element(ms.begin(), ms.end()) - ms.begin());
+      c->heev_choice[key] = variant[ci];
+      c->heev_trials[key] = ms;
+    }
+  }
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
   cudaError_t cap = cudaSuccess;
-  for (const Chunk& ch : chunks) {
+  for (size_t ci = 0; ci < chunks.size(); ++ci) {
+    const Chunk& ch = chunks[ci];
     cap = pmx::dev::launch_assemble(table, dit + ch.first, ch.cnt, ch.max_npw, c->hbuf.as<double2>(), c->stream);
     if (cap != cudaSuccess) break;
     cap = pmx::dev::launch_heev(dit + ch.first, ch.cnt, ch.max_n, ch.max_nval, c->hbuf.as<double2>(),
                                 c->wbuf.as<double>(), zbase ? zbase : c->hbuf.as<double2>(), c->scratch.as<double>(),
-                                dinfo + ch.first, c->stream, 0);
+                                dinfo + ch.first, c->stream, variant[ci]);
     if (cap != cudaSuccess) break;
   }
   const cudaError_t end = cudaStreamEndCapture(c->stream, &graph);
