@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="gaas_epsij")
     ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="leave out the timed reference sample (minutes of host time on the larger workloads)")
     return ap.parse_args()
 
 
@@ -99,6 +101,17 @@ class ClockSampler:
         reasons = sorted({n for s in self.samples for n, v in zip(names, s[4:8]) if v.lower() == "active"})
         return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
                 "samples": len(self.samples)}
+
+
+def profiled_heev_bytes(n):
+    """DRAM bytes per matrix of the eigensolver at size n from the committed
+    ncu summary (dram__bytes_read.sum + dram__bytes_write.sum of one capture
+    divided by its matrices), or None when no capture covers this n."""
+    path = os.path.join(ROOT, "profiles", "heev_kernel_gaas_epsij_8.md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(rf"dram_bytes_per_matrix n={n}: ([0-9.eE+]+)", open(path).read())
+    return float(m.group(1)) if m else None
 
 
 def _ref_run(binary, argv, lines, sample, tmp, env):
@@ -293,8 +306,12 @@ def ours(args, rank, world):
         ms_launch = per["heev"][0] / max(per["heev"][1], 1)
         flops_launch = flops / max(per["heev"][1], 1)
         ach = flops_launch / (ms_launch * 1e-3) / 1e12
+        bpm = profiled_heev_bytes(n)
+        traffic = bpm * nsolves / max(per["heev"][1], 1) if bpm else None
         roof = {"kernel": "heev_kernel", "bound": "fp64", "achieved": ach, "peak": FP64_TFLOPS_NOMINAL,
-                "unit": "TFLOP/s", "frac": ach / FP64_TFLOPS_NOMINAL, "traffic": None,
+                "unit": "TFLOP/s", "frac": ach / FP64_TFLOPS_NOMINAL, "traffic": traffic,
+                "traffic_source": "DRAM bytes per matrix of the ncu capture in profiles/heev_kernel_gaas_epsij_8.md "
+                                  "x matrices per launch" if bpm else None,
                 "peak_source": "nominal B200 FP64 (no measured FP64 peak in MEASURED_PEAKS.json)",
                 "per_launch_ms": ms_launch, "launches_per_step": per["heev"][1]}
     elif dom == "contract_mixed":
@@ -322,7 +339,7 @@ def ours(args, rank, world):
         "degenerate_cuts": ctx.degenerate_cuts(),
         "autotune": ctx.tuning(),
     }
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline_sample(argv, nspec)
         out["cpu_baseline"] = cb
     if rank == 0:
