@@ -13,14 +13,20 @@
 // written out and the pieces are summed in FP64 in a fixed order, so results
 // are deterministic.
 //
-// Pipeline of one CTA (256 threads, two shared-memory stages):
-//   thread 0   bulk-copies the precomputed W chunk (hi and lo, 32 KB, already
-//              in the canonical K-major UMMA layout) into the stage
-//   all        stage the overlaps of the chunk and write the split P tile
-//   thread 0   waits for the W copy, issues 6 MMAs, commits to the stage's
-//              mbarrier; the stage is refilled two chunks later.
+// Pipeline of one CTA (8 producer warps + 1 control warp, two shared-memory
+// stages):
+//   control    bulk-copies the precomputed W chunk (hi and lo, 32 KB, already
+//              in the canonical K-major UMMA layout) into a stage once the
+//              stage's previous MMAs completed; waits for the stage's A tile
+//              and W copy, issues 6 MMAs and commits them to the stage's
+//              mbarrier
+//   producers  stage the overlaps of the chunk in shared memory (named
+//              barrier among the producers only), write the split P tile and
+//              arrive on the stage's A-full mbarrier; warps 0-3 move the FP32
+//              accumulator to the FP64 tile after every 64 chunks.
 // Every mbarrier wait is bounded; on expiry the CTA records an error code,
-// drains its own MMAs (bounded), frees its TMEM and returns.
+// drains its own MMAs (bounded), frees its TMEM and returns. The producers
+// leave their loop together: the decision is an OR over a named barrier.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -41,7 +47,8 @@ constexpr int kM = 128;        // MMA rows
 constexpr int kPairs = 64;     // pairs per tile (kM / 2)
 constexpr int kN = 256;        // frequencies per tile
 constexpr int kKC = 32;        // transitions per chunk
-constexpr int kThreads = 256;
+constexpr int kProducers = 256;              // warps 0-7
+constexpr int kThreads = kProducers + 32;    // + the control warp (W copies, MMA issue)
 constexpr int kFlushChunks = 64;  // chunks (2048 transitions) per FP32 accumulation before the FP64 flush
 constexpr int kTargetCtas = 4 * 148;  // K-split so that the grid covers the SMs a few times
 constexpr unsigned kWaitLimit = 1u << 26;
@@ -120,6 +127,25 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t adesc, uint64_t
       : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Named barrier 1 over the producer warps, returning the OR of v over them
+// (every producer gets the same answer).
+__device__ __forceinline__ bool producers_sync_or(bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 q, %1, 0;\n\t"
+      "bar.red.or.pred p, 1, %2, q;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)v), "n"(kProducers)
+      : "memory");
+  return r != 0;
+}
+
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                    smem_u32(bar))
@@ -134,22 +160,21 @@ __device__ __forceinline__ void async_proxy_fence() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
-  __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
-  return *reinterpret_cast<uint32_t*>(&v);
-}
 
-// hi/lo split of 8 values into two 16-byte rows of a core matrix.
+// hi/lo split of 8 values into two 16-byte rows of a core matrix:
+// hi = bf16_rn(x), lo = bf16_rn(x - hi), two values per conversion.
 __device__ __forceinline__ void split8(const float* x, uint4& hi, uint4& lo) {
-  float h[8], l[8];
+  uint32_t h[4], l[4];
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const __nv_bfloat16 b = __float2bfloat16_rn(x[i]);
-    h[i] = __bfloat162float(b);
-    l[i] = x[i] - h[i];
+  for (int i = 0; i < 4; ++i) {
+    const __nv_bfloat162 hb = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);
+    const float2 hf = __bfloat1622float2(hb);
+    const __nv_bfloat162 lb = __floats2bfloat162_rn(x[2 * i] - hf.x, x[2 * i + 1] - hf.y);
+    h[i] = *reinterpret_cast<const uint32_t*>(&hb);
+    l[i] = *reinterpret_cast<const uint32_t*>(&lb);
   }
-  hi = make_uint4(pack_bf16(h[0], h[1]), pack_bf16(h[2], h[3]), pack_bf16(h[4], h[5]), pack_bf16(h[6], h[7]));
-  lo = make_uint4(pack_bf16(l[0], l[1]), pack_bf16(l[2], l[3]), pack_bf16(l[4], l[5]), pack_bf16(l[6], l[7]));
+  hi = make_uint4(h[0], h[1], h[2], h[3]);
+  lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
 __device__ __forceinline__ double broaden_m(int model, double eps, double x) {
@@ -180,9 +205,28 @@ struct Plan {
   int2* tiles;       // [ntile] (a block, b block)
   float* wgt32;      // [T]
   uint8_t* wbuf;     // [nchunk][32 KB]
-  double* part;      // [nitem][ntile][128][256] FP64 partial tiles
+  double* part;      // [nitem][ntile] FP64 partial tiles of 128 x 256, see part_index
   int* err;          // error flag
 };
+
+// Layout of a 128 x 256 partial tile: four 32-row blocks (one per TMEM lane
+// quarter), each column-major: a flush pass of one warp (32 rows x 32
+// columns) is one contiguous 8 KB block.
+__host__ __device__ constexpr int part_index(int row, int col) { return (row >> 5) * (kN * 32) + col * 32 + (row & 31); }
+
+__device__ __forceinline__ void bulk_store(void* gdst, const void* ssrc, uint32_t bytes, bool add) {
+  if (add)
+    asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f64 [%0], [%1], %2;" ::"l"(gdst),
+                 "r"(smem_u32(ssrc)), "r"(bytes)
+                 : "memory");
+  else
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(smem_u32(ssrc)),
+                 "r"(bytes)
+                 : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 }  // namespace
 
@@ -216,23 +260,34 @@ __global__ void __launch_bounds__(256) wgen_kernel(Plan pl, ContractArgs a) {
 
 // ------------------------------------------------------------- main GEMM
 template <int NCH>
-__global__ void __launch_bounds__(kThreads, 1) mixed_kernel(Plan pl, ContractArgs a, const float2* __restrict__ M32) {
+__global__ void __launch_bounds__(kThreads, 2) mixed_kernel(Plan pl, ContractArgs a, const float2* __restrict__ M32) {
   const int tile = blockIdx.x, item_id = blockIdx.y;
   const int2 tb = pl.tiles[tile];
   const int4 it = pl.item[item_id];
-  const int c_begin = it.y, c_end = it.z;
+  const int c_begin = it.y, nch = it.z - it.y;
   const int A = 3 * a.neps;
   const int a0 = tb.x * 8, b0 = tb.y * 8;
   const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31;
+  // the chunks of an item are consecutive 32-transition slices of one
+  // frequency tile's range
+  const int t_first = nch > 0 ? pl.chunk_t0[c_begin] : 0, t_end = nch > 0 ? pl.chunk_t1[c_begin] : 0;
 
+  // overlaps staged per chunk: double-buffered when small (NCH = 1), so that
+  // one producer barrier per chunk suffices
+  constexpr int kSMBuf = NCH == 1 ? 2 : 1;
+  constexpr int kSMElems = kKC * 16 * NCH;
   extern __shared__ __align__(1024) uint8_t smem[];
   // stage layout: [A hi 8K][A lo 8K][B hi 16K][B lo 16K] x 2
-  uint8_t* stage[2] = {smem, smem + 2 * kABytes + kWChunkBytes};
-  float2* sM = reinterpret_cast<float2*>(smem + 2 * (2 * kABytes + kWChunkBytes));  // [kKC][16][NCH]
-  float* sw = reinterpret_cast<float*>(sM + kKC * 16 * NCH);                        // [kKC]
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sw + kKC);                            // wfull[2], mdone[2]
-  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(bars + 4);
+  auto stage = [&](int s) { return smem + s * (2 * kABytes + kWChunkBytes); };
+  float2* sM = reinterpret_cast<float2*>(smem + 2 * (2 * kABytes + kWChunkBytes));  // [kSMBuf][kKC][16][NCH]
+  float* sw = reinterpret_cast<float*>(sM + kSMBuf * kSMElems);                      // [kSMBuf][kKC]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sw + kSMBuf * kKC);  // wfull[2], mdone[2], afull[2]
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(bars + 6);
   int* s_abort = reinterpret_cast<int*>(s_tmem + 1);  // s_abort[0], last committed chunk s_abort[1]
+  int* s_last = s_abort + 1;
+  uint64_t* wfull = bars;
+  uint64_t* mdone = bars + 2;
+  uint64_t* afull = bars + 4;
 
   if (wid == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(s_tmem)),
@@ -241,111 +296,34 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_kernel(Plan pl, ContractArg
   }
   if (tid == 0) {
     for (int i = 0; i < 4; ++i) mbar_init(&bars[i], 1);
+    for (int i = 4; i < 6; ++i) mbar_init(&bars[i], kProducers);
     *s_abort = 0;
+    *s_last = -1;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *s_tmem;
-  uint64_t* wfull = bars;
-  uint64_t* mdone = bars + 2;
-
-  // pair handled by this thread for P production: 64 pairs x 4 groups of 8 transitions
-  const int pp = tid >> 2, kg = tid & 3;
-  const int ia = pp >> 3, ib = pp & 7;
-  const int av = a0 + ia, bv = b0 + ib;
-  const bool valid = av < A && bv < A && (av / 3) >= (bv / 3);
-
-  int* s_last = s_abort + 1;  // index (from c_begin) of the last committed chunk, -1 if none
-  if (tid == 0) *s_last = -1;
-  double* out = pl.part + ((size_t)item_id * pl.ntile + tile) * (kM * kN);
-  int flushes = 0;
-  // The overlaps and weights of chunk c + 1 are loaded into registers while
-  // chunk c is produced and multiplied, so the L2 latency of the overlap
-  // gather is off the producer's critical path.
-  constexpr int kMPer = kKC * 16 * NCH / kThreads;
-  float2 mreg[kMPer];
-  float wreg = 0.f;
-  auto load_chunk = [&](int cc) {
-    const int t0 = pl.chunk_t0[cc], t1 = pl.chunk_t1[cc];
-#pragma unroll
-    for (int q = 0; q < kMPer; ++q) {
-      const int idx = tid + q * kThreads;
-      const int t = idx / (16 * NCH), rem = idx % (16 * NCH);
-      const int slot = rem / NCH, ch = rem % NCH;
-      const int gt = t0 + t;
-      const int ab = slot < 8 ? a0 + slot : b0 + slot - 8;
-      mreg[q] = (gt < t1 && ab < A) ? M32[((size_t)gt * A + ab) * NCH + ch] : make_float2(0.f, 0.f);
-    }
-    wreg = (tid < kKC && t0 + tid < t1) ? pl.wgt32[t0 + tid] : 0.f;
+  // a bounded wait that gives up at once when the CTA already aborted
+  auto wait = [&](uint64_t* bar, uint32_t parity, int code) {
+    if (*(volatile int*)s_abort) return false;
+    if (mbar_wait(bar, parity)) return true;
+    atomicExch(pl.err, code);
+    *(volatile int*)s_abort = 1;
+    return false;
   };
-  if (c_begin < c_end) load_chunk(c_begin);
-  for (int c = c_begin; c < c_end; ++c) {
-    const int n = c - c_begin, s = n & 1;
-    const int g = n % kFlushChunks;  // position inside the current FP32 accumulation group
-    uint8_t* st = stage[s];
-    // the stage is free once the MMAs of chunk n-2 (same stage) completed
-    if (tid == 0 && n >= 2 && !*s_abort && !mbar_wait(&mdone[s], ((n - 2) >> 1) & 1)) {
-      atomicExch(pl.err, 1);
-      *s_abort = 1;
-    }
-    __syncthreads();
-    tc_fence_after();
-    if (*s_abort) break;
-    if (tid == 0) bulk_load(st + 2 * kABytes, pl.wbuf + (size_t)c * kWChunkBytes, kWChunkBytes, &wfull[s]);
-    // stage overlaps and weights of the chunk (loaded one iteration ahead)
-#pragma unroll
-    for (int q = 0; q < kMPer; ++q) sM[tid + q * kThreads] = mreg[q];
-    if (tid < kKC) sw[tid] = wreg;
-    __syncthreads();
-    if (c + 1 < c_end) load_chunk(c + 1);
-    // split pair products into the A tile: row pp (P1) and 64 + pp (P2)
-    {
-      float p1[8], p2[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const int t = kg * 8 + q;
-        float reO = 0.f, imO = 0.f;
-        if (valid) {
-          const float2* ma = sM + ((size_t)t * 16 + ia) * NCH;
-          const float2* mb = sM + ((size_t)t * 16 + 8 + ib) * NCH;
-          if (NCH == 1) {
-            reO = ma[0].x * mb[0].x + ma[0].y * mb[0].y;
-            imO = ma[0].y * mb[0].x - ma[0].x * mb[0].y;
-          } else {
-            // reO = Re(S_a S_b*) - Re(X_a X_b*), S = up + dn, X = ud + du
-            // imO = Im(up_a up_b* + dn_a dn_b* - ud_a ud_b* - du_a du_b*)
-            const float sax = ma[0].x + ma[1].x, say = ma[0].y + ma[1].y;
-            const float sbx = mb[0].x + mb[1].x, sby = mb[0].y + mb[1].y;
-            const float xax = ma[2].x + ma[3].x, xay = ma[2].y + ma[3].y;
-            const float xbx = mb[2].x + mb[3].x, xby = mb[2].y + mb[3].y;
-            reO = (sax * sbx + say * sby) - (xax * xbx + xay * xby);
-            imO = (ma[0].y * mb[0].x - ma[0].x * mb[0].y) + (ma[1].y * mb[1].x - ma[1].x * mb[1].y) -
-                  (ma[2].y * mb[2].x - ma[2].x * mb[2].y) - (ma[3].y * mb[3].x - ma[3].x * mb[3].y);
-          }
-        }
-        p1[q] = sw[t] * reO;
-        p2[q] = -sw[t] * imO;
-      }
-      uint4 h1, l1, h2, l2;
-      split8(p1, h1, l1);
-      split8(p2, h2, l2);
-      const int o1 = core_off(pp, kg * 8, kM), o2 = core_off(kPairs + pp, kg * 8, kM);
-      *reinterpret_cast<uint4*>(st + o1) = h1;
-      *reinterpret_cast<uint4*>(st + kABytes + o1) = l1;
-      *reinterpret_cast<uint4*>(st + o2) = h2;
-      *reinterpret_cast<uint4*>(st + kABytes + o2) = l2;
-    }
-    async_proxy_fence();
-    __syncthreads();
-    if (tid == 0) {
-      if (!mbar_wait(&wfull[s], (n >> 1) & 1)) {
-        atomicExch(pl.err, 2);
-        *s_abort = 1;
-      } else {
+
+  if (wid == kProducers / 32) {
+    // ------------------------------------------------------------ control
+    if (lane == 0) {
+      for (int n = 0; n < 2 && n < nch; ++n)
+        bulk_load(stage(n) + 2 * kABytes, pl.wbuf + (size_t)(c_begin + n) * kWChunkBytes, kWChunkBytes, &wfull[n]);
+      for (int n = 0; n < nch; ++n) {
+        const int s = n & 1, g = n % kFlushChunks;
+        if (!wait(&afull[s], (n >> 1) & 1, 5) || !wait(&wfull[s], (n >> 1) & 1, 2)) break;
         tc_fence_after();
-        const uint32_t sa = smem_u32(st);
+        const uint32_t sa = smem_u32(stage(s));
         const uint32_t sb = sa + 2 * kABytes;
 #pragma unroll
         for (int ks = 0; ks < kKC / 16; ++ks) {
@@ -360,85 +338,201 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_kernel(Plan pl, ContractArg
           mma_bf16(tmem, alo, bhi, 1u);
         }
         mma_commit(&mdone[s]);
-        *s_last = n;
-      }
-    }
-    // flush the FP32 accumulator into the CTA's FP64 tile at the end of every
-    // group and of the range (the commit of chunk n covers all earlier MMAs)
-    if (g == kFlushChunks - 1 || c == c_end - 1) {
-      if (tid == 0 && !*s_abort && !mbar_wait(&mdone[s], (n >> 1) & 1)) {
-        atomicExch(pl.err, 4);
-        *s_abort = 1;
-      }
-      __syncthreads();
-      tc_fence_after();
-      if (*s_abort) break;
-      if (wid < 4) {
-        const int row = wid * 32 + lane;
-        for (int cb = 0; cb < kN; cb += 8) {
-          uint32_t r[8];
-          const uint32_t taddr = tmem + ((uint32_t)(wid * 32) << 16) + cb;
-          asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-                         "=r"(r[7])
-                       : "r"(taddr));
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-          double* dst = out + (size_t)row * kN + cb;
-#pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const double v = (double)__uint_as_float(r[q]);
-            dst[q] = flushes == 0 ? v : dst[q] + v;
-          }
+        *(volatile int*)s_last = n;
+        // the other stage is free once chunk n-1's MMAs (queued ahead of
+        // chunk n's) completed: its W copy for chunk n+1 starts then
+        if (n >= 1 && n + 1 < nch) {
+          if (!wait(&mdone[s ^ 1], ((n - 1) >> 1) & 1, 1)) break;
+          bulk_load(stage(s ^ 1) + 2 * kABytes, pl.wbuf + (size_t)(c_begin + n + 1) * kWChunkBytes, kWChunkBytes,
+                    &wfull[s ^ 1]);
         }
       }
-      ++flushes;
-      tc_fence_before();
-      __syncthreads();
     }
+    __syncwarp();
+  } else {
+    // ---------------------------------------------------------- producers
+    // pair handled by this thread: 64 pairs x 4 groups of 8 transitions
+    const int pp = tid >> 2, kg = tid & 3;
+    const int ia = pp >> 3, ib = pp & 7;
+    const int av = a0 + ia, bv = b0 + ib;
+    const bool valid = av < A && bv < A && (av / 3) >= (bv / 3);
+    double* out = pl.part + ((size_t)item_id * pl.ntile + tile) * (kM * kN);
+    int flushes = 0;
+    // The overlaps and weights of chunk n + 1 are loaded into registers while
+    // chunk n is produced, so the L2 latency of the overlap gather is off the
+    // producers' critical path.
+    constexpr int kMPer = kSMElems / kProducers;
+    float2 mreg[kMPer];
+    float wreg = 0.f;
+    auto load_chunk = [&](int n) {
+      const int t0 = t_first + n * kKC;
+#pragma unroll
+      for (int q = 0; q < kMPer; ++q) {
+        const int idx = tid + q * kProducers;
+        const int t = idx / (16 * NCH), rem = idx % (16 * NCH);
+        const int slot = rem / NCH, ch = rem % NCH;
+        const int gt = t0 + t;
+        const int ab = slot < 8 ? a0 + slot : b0 + slot - 8;
+        mreg[q] = (gt < t_end && ab < A) ? M32[((size_t)gt * A + ab) * NCH + ch] : make_float2(0.f, 0.f);
+      }
+      wreg = (tid < kKC && t0 + tid < t_end) ? pl.wgt32[t0 + tid] : 0.f;
+    };
+    if (nch > 0) load_chunk(0);
+    for (int n = 0; n < nch; ++n) {
+      const int s = n & 1, g = n % kFlushChunks, sb = kSMBuf == 2 ? s : 0;
+      uint8_t* st = stage(s);
+      float2* sMb = sM + sb * kSMElems;
+      float* swb = sw + sb * kKC;
+      // the stage is free once the MMAs of chunk n-2 completed
+      bool fail = n >= 2 && !wait(&mdone[s], ((n - 2) >> 1) & 1, 1);
+      // with one overlap buffer, every producer has finished reading chunk
+      // n-1's overlaps before any overwrites them
+      if (kSMBuf == 1 && producers_sync_or(fail)) break;
+#pragma unroll
+      for (int q = 0; q < kMPer; ++q) sMb[tid + q * kProducers] = mreg[q];
+      if (tid < kKC) swb[tid] = wreg;
+      fail = fail || *(volatile int*)s_abort;
+      if (producers_sync_or(fail)) break;
+      if (n + 1 < nch) load_chunk(n + 1);
+      // split pair products into the A tile: row pp (P1) and 64 + pp (P2)
+      {
+        float p1[8], p2[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int t = kg * 8 + q;
+          float reO = 0.f, imO = 0.f;
+          if (valid) {
+            const float2* ma = sMb + ((size_t)t * 16 + ia) * NCH;
+            const float2* mb = sMb + ((size_t)t * 16 + 8 + ib) * NCH;
+            if (NCH == 1) {
+              reO = ma[0].x * mb[0].x + ma[0].y * mb[0].y;
+              imO = ma[0].y * mb[0].x - ma[0].x * mb[0].y;
+            } else {
+              // reO = Re(S_a S_b*) - Re(X_a X_b*), S = up + dn, X = ud + du
+              // imO = Im(up_a up_b* + dn_a dn_b* - ud_a ud_b* - du_a du_b*)
+              const float sax = ma[0].x + ma[1].x, say = ma[0].y + ma[1].y;
+              const float sbx = mb[0].x + mb[1].x, sby = mb[0].y + mb[1].y;
+              const float xax = ma[2].x + ma[3].x, xay = ma[2].y + ma[3].y;
+              const float xbx = mb[2].x + mb[3].x, xby = mb[2].y + mb[3].y;
+              reO = (sax * sbx + say * sby) - (xax * xbx + xay * xby);
+              imO = (ma[0].y * mb[0].x - ma[0].x * mb[0].y) + (ma[1].y * mb[1].x - ma[1].x * mb[1].y) -
+                    (ma[2].y * mb[2].x - ma[2].x * mb[2].y) - (ma[3].y * mb[3].x - ma[3].x * mb[3].y);
+            }
+          }
+          p1[q] = swb[t] * reO;
+          p2[q] = -swb[t] * imO;
+        }
+        uint4 h1, l1, h2, l2;
+        split8(p1, h1, l1);
+        split8(p2, h2, l2);
+        const int o1 = core_off(pp, kg * 8, kM), o2 = core_off(kPairs + pp, kg * 8, kM);
+        *reinterpret_cast<uint4*>(st + o1) = h1;
+        *reinterpret_cast<uint4*>(st + kABytes + o1) = l1;
+        *reinterpret_cast<uint4*>(st + o2) = h2;
+        *reinterpret_cast<uint4*>(st + kABytes + o2) = l2;
+      }
+      async_proxy_fence();
+      mbar_arrive(&afull[s]);
+      // warps 0-3 (TMEM lanes 0-127) move the FP32 accumulator into the FP64
+      // tile after the group's last chunk: 32 columns at a time through this
+      // warp's 8 KB of the stage of chunk n (free until chunk n + 2, which
+      // waits for these warps), then one bulk copy (first flush) or bulk
+      // FP64 add into the tile. A flush starts once the previous one's bulk
+      // operations completed, so the additions happen in a fixed order. Their
+      // next A-full arrival tells the control warp that the accumulator and
+      // the stage may be overwritten.
+      if ((g == kFlushChunks - 1 || n == nch - 1) && wid < 4) {
+        if (wait(&mdone[s], (n >> 1) & 1, 4)) {
+          tc_fence_after();
+          double* stg = reinterpret_cast<double*>(st) + wid * (32 * 32);
+          double* dst = out + part_index(wid * 32, 0);
+          if (lane == 0) bulk_wait_all();
+          __syncwarp();
+          for (int cb = 0; cb < kN; cb += 32) {
+            uint32_t r[32];
+            const uint32_t taddr = tmem + ((uint32_t)(wid * 32) << 16) + cb;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            // the previous pass's bulk operation has read the staging block
+            if (lane == 0) bulk_wait_read();
+            __syncwarp();
+#pragma unroll
+            for (int q = 0; q < 32; ++q) stg[q * 32 + lane] = (double)__uint_as_float(r[q]);
+            async_proxy_fence();
+            __syncwarp();
+            if (lane == 0) bulk_store(dst + cb * 32, stg, 32 * 32 * sizeof(double), flushes > 0);
+          }
+          if (lane == 0) bulk_wait_read();
+          __syncwarp();
+          tc_fence_before();
+        }
+      }
+      if (g == kFlushChunks - 1 || n == nch - 1) ++flushes;
+    }
+    // an empty range (or an abort before the first flush) still owns its
+    // tile: the producers zero it
+    if (flushes == 0)
+      for (int idx = tid; idx < kM * kN; idx += kProducers) out[idx] = 0.0;
+    // every bulk copy of this CTA has completed before it exits
+    if (wid < 4 && lane == 0) bulk_wait_all();
   }
   __syncthreads();
-  // drain: the last commit completes after every earlier MMA of this thread;
-  // it is waited for on every path before TMEM is read or freed.
-  const int nlast = *s_last;
-  if (tid == 0 && nlast >= 0 && !mbar_wait(&mdone[nlast & 1], (nlast >> 1) & 1)) {
-    atomicExch(pl.err, 3);
-    *s_abort = 1;
-  }
-  __syncthreads();
-  tc_fence_after();
-  // an empty range still owns its tile: zero it
-  if (flushes == 0)
-    for (int idx = tid; idx < kM * kN; idx += kThreads) out[idx] = 0.0;
+  // drain: the last commit completes after every earlier MMA of the control
+  // thread; it is waited for on every path before TMEM is freed
+  const int nlast = *(volatile int*)s_last;
+  if (tid == kProducers && nlast >= 0 && !mbar_wait(&mdone[nlast & 1], (nlast >> 1) & 1)) atomicExch(pl.err, 3);
   tc_fence_before();
   __syncthreads();
+  tc_fence_after();
   if (wid == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kN));
 }
 
 // Sums the FP64 partial tiles of each frequency tile's pieces in piece order
-// and scatters rows to acc[2][9][np][nf] (P1 -> Im, P2 -> Re).
+// and scatters rows to acc[2][9][np][nf] (P1 -> Im, P2 -> Re). 32 columns
+// at a time go through shared memory so that both the reads of the tiles
+// (part_index: rows fastest) and the writes of acc (frequency fastest)
+// coalesce.
 __global__ void __launch_bounds__(256) reduce_kernel(Plan pl, ContractArgs a) {
+  constexpr int kCB = 32;
+  __shared__ double sT[kM][kCB + 1];
   const int tile = blockIdx.x, ft = blockIdx.y;
   const int2 tb = pl.tiles[tile];
   const int2 ir = pl.ft_items[ft];
   const int A = 3 * a.neps;
   const size_t blk = (size_t)9 * a.np * a.nf;
-  for (int idx = threadIdx.x; idx < kM * kN; idx += blockDim.x) {
-    const int row = idx / kN, col = idx % kN;
-    const int f = ft * kN + col;
-    if (f >= a.nf) continue;
-    const int pp = row & (kPairs - 1);
-    const int av = tb.x * 8 + (pp >> 3), bv = tb.y * 8 + (pp & 7);
-    if (av >= A || bv >= A) continue;
-    const int m = av / 3, i = av % 3, n = bv / 3, j = bv % 3;
-    if (n > m) continue;
-    double s = 0.0;
-    for (int itm = ir.x; itm < ir.y; ++itm)
-      s += pl.part[((size_t)itm * pl.ntile + tile) * (kM * kN) + idx];
-    const size_t o = ((size_t)(i * 3 + j) * a.np + (size_t)m * (m + 1) / 2 + n) * a.nf + f;
-    if (row < kPairs)
-      a.acc[blk + o] = s;  // Im part
-    else
-      a.acc[o] = s;  // Re part
+  for (int cb = 0; cb < kN; cb += kCB) {
+    for (int idx = threadIdx.x; idx < kM * kCB; idx += blockDim.x) {
+      const int row = idx % kM, col = cb + idx / kM;
+      double s = 0.0;
+      for (int itm = ir.x; itm < ir.y; ++itm)
+        s += pl.part[((size_t)itm * pl.ntile + tile) * (kM * kN) + part_index(row, col)];
+      sT[row][col - cb] = s;
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kM * kCB; idx += blockDim.x) {
+      const int row = idx / kCB, c = idx % kCB;
+      const int f = ft * kN + cb + c;
+      if (f >= a.nf) continue;
+      const int pp = row & (kPairs - 1);
+      const int av = tb.x * 8 + (pp >> 3), bv = tb.y * 8 + (pp & 7);
+      if (av >= A || bv >= A) continue;
+      const int m = av / 3, i = av % 3, n = bv / 3, j = bv % 3;
+      if (n > m) continue;
+      const size_t o = ((size_t)(i * 3 + j) * a.np + (size_t)m * (m + 1) / 2 + n) * a.nf + f;
+      if (row < kPairs)
+        a.acc[blk + o] = sT[row][c];  // Im part
+      else
+        a.acc[o] = sT[row][c];  // Re part
+    }
+    __syncthreads();
   }
 }
 
@@ -508,8 +602,9 @@ size_t mixed_workspace_bytes(const ContractArgs& a, long long T) {
 }
 
 size_t mixed_smem_bytes(int nch) {
-  return (size_t)2 * (2 * kABytes + kWChunkBytes) + (size_t)kKC * 16 * nch * sizeof(float2) + kKC * sizeof(float) +
-         4 * sizeof(uint64_t) + 4 * sizeof(int);
+  const int nbuf = nch == 1 ? 2 : 1;  // overlap buffers (see mixed_kernel)
+  return (size_t)2 * (2 * kABytes + kWChunkBytes) + (size_t)nbuf * kKC * 16 * nch * sizeof(float2) +
+         (size_t)nbuf * kKC * sizeof(float) + 6 * sizeof(uint64_t) + 4 * sizeof(int);
 }
 
 // Precision diagnostic of the FP32 overlap copies: max ||M32|^2 - |M|^2| and
