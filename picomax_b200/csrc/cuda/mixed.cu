@@ -275,11 +275,15 @@ __global__ void __launch_bounds__(kThreads, 2) mixed_kernel(Plan pl, ContractArg
   // overlaps staged per chunk: double-buffered when small (NCH = 1), so that
   // one producer barrier per chunk suffices
   constexpr int kSMBuf = NCH == 1 ? 2 : 1;
-  constexpr int kSMElems = kKC * 16 * NCH;
+  // staged overlaps: 16 slot rows (8 a-side, 8 b-side) of kKC transitions x
+  // NCH, each row padded by 16 bytes so that the producers' 16-byte reads of
+  // 8 different b-rows by a quarter warp fall into distinct banks
+  constexpr int kRow = kKC * NCH + 2;
+  constexpr int kSMElems = 16 * kRow;
   extern __shared__ __align__(1024) uint8_t smem[];
   // stage layout: [A hi 8K][A lo 8K][B hi 16K][B lo 16K] x 2
   auto stage = [&](int s) { return smem + s * (2 * kABytes + kWChunkBytes); };
-  float2* sM = reinterpret_cast<float2*>(smem + 2 * (2 * kABytes + kWChunkBytes));  // [kSMBuf][kKC][16][NCH]
+  float2* sM = reinterpret_cast<float2*>(smem + 2 * (2 * kABytes + kWChunkBytes));  // [kSMBuf][16][kRow]
   float* sw = reinterpret_cast<float*>(sM + kSMBuf * kSMElems);                      // [kSMBuf][kKC]
   uint64_t* bars = reinterpret_cast<uint64_t*>(sw + kSMBuf * kKC);  // wfull[2], mdone[2], afull[2]
   uint32_t* s_tmem = reinterpret_cast<uint32_t*>(bars + 6);
@@ -351,9 +355,10 @@ __global__ void __launch_bounds__(kThreads, 2) mixed_kernel(Plan pl, ContractArg
     __syncwarp();
   } else {
     // ---------------------------------------------------------- producers
-    // pair handled by this thread: 64 pairs x 4 groups of 8 transitions
-    const int pp = tid >> 2, kg = tid & 3;
-    const int ia = pp >> 3, ib = pp & 7;
+    // pair handled by this thread: 64 pairs x 4 groups of 8 transitions; a
+    // warp shares the a-side row, a quarter warp the transition group
+    const int ia = wid, ib = tid & 7, kg = (tid >> 3) & 3;
+    const int pp = ia * 8 + ib;
     const int av = a0 + ia, bv = b0 + ib;
     const bool valid = av < A && bv < A && (av / 3) >= (bv / 3);
     double* out = pl.part + ((size_t)item_id * pl.ntile + tile) * (kM * kN);
@@ -361,7 +366,7 @@ __global__ void __launch_bounds__(kThreads, 2) mixed_kernel(Plan pl, ContractArg
     // The overlaps and weights of chunk n + 1 are loaded into registers while
     // chunk n is produced, so the L2 latency of the overlap gather is off the
     // producers' critical path.
-    constexpr int kMPer = kSMElems / kProducers;
+    constexpr int kMPer = kKC * 16 * NCH / kProducers;
     float2 mreg[kMPer];
     float wreg = 0.f;
     auto load_chunk = [&](int n) {
@@ -389,7 +394,11 @@ __global__ void __launch_bounds__(kThreads, 2) mixed_kernel(Plan pl, ContractArg
       // n-1's overlaps before any overwrites them
       if (kSMBuf == 1 && producers_sync_or(fail)) break;
 #pragma unroll
-      for (int q = 0; q < kMPer; ++q) sMb[tid + q * kProducers] = mreg[q];
+      for (int q = 0; q < kMPer; ++q) {
+        const int idx = tid + q * kProducers;
+        const int t = idx / (16 * NCH), rem = idx % (16 * NCH);
+        sMb[(rem / NCH) * kRow + t * NCH + rem % NCH] = mreg[q];
+      }
       if (tid < kKC) swb[tid] = wreg;
       fail = fail || *(volatile int*)s_abort;
       if (producers_sync_or(fail)) break;
@@ -397,30 +406,55 @@ __global__ void __launch_bounds__(kThreads, 2) mixed_kernel(Plan pl, ContractArg
       // split pair products into the A tile: row pp (P1) and 64 + pp (P2)
       {
         float p1[8], p2[8];
+        // this thread's 8 transitions are contiguous in both rows: 16-byte
+        // loads (all 8 up front for NCH = 1, per transition for NCH = 4)
+        const float4* pa = reinterpret_cast<const float4*>(sMb + ia * kRow + kg * 8 * NCH);
+        const float4* pb = reinterpret_cast<const float4*>(sMb + (8 + ib) * kRow + kg * 8 * NCH);
+        float4 a1[NCH == 1 ? 4 : 1], b1[NCH == 1 ? 4 : 1];
+        if (NCH == 1) {
+#pragma unroll
+          for (int i = 0; i < (NCH == 1 ? 4 : 1); ++i) {
+            a1[i] = pa[i];
+            b1[i] = pb[i];
+          }
+        }
+        float w8[8];
+        {
+          const float4* pw = reinterpret_cast<const float4*>(swb + kg * 8);
+          const float4 w0 = pw[0], w1 = pw[1];
+          w8[0] = w0.x; w8[1] = w0.y; w8[2] = w0.z; w8[3] = w0.w;
+          w8[4] = w1.x; w8[5] = w1.y; w8[6] = w1.z; w8[7] = w1.w;
+        }
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-          const int t = kg * 8 + q;
           float reO = 0.f, imO = 0.f;
           if (valid) {
-            const float2* ma = sMb + ((size_t)t * 16 + ia) * NCH;
-            const float2* mb = sMb + ((size_t)t * 16 + 8 + ib) * NCH;
             if (NCH == 1) {
-              reO = ma[0].x * mb[0].x + ma[0].y * mb[0].y;
-              imO = ma[0].y * mb[0].x - ma[0].x * mb[0].y;
+              const float4 va = a1[(q >> 1) & (NCH == 1 ? 3 : 0)], vb = b1[(q >> 1) & (NCH == 1 ? 3 : 0)];
+              const float2 a = (q & 1) ? make_float2(va.z, va.w) : make_float2(va.x, va.y);
+              const float2 b = (q & 1) ? make_float2(vb.z, vb.w) : make_float2(vb.x, vb.y);
+              reO = a.x * b.x + a.y * b.y;
+              imO = a.y * b.x - a.x * b.y;
             } else {
+              // channels up, dn, ud, du of transition q: 2 x 16 bytes per row
+              const float4 a01 = pa[2 * q], a23 = pa[2 * q + 1], b01 = pb[2 * q], b23 = pb[2 * q + 1];
+              const float2 a[4] = {make_float2(a01.x, a01.y), make_float2(a01.z, a01.w), make_float2(a23.x, a23.y),
+                                   make_float2(a23.z, a23.w)};
+              const float2 b[4] = {make_float2(b01.x, b01.y), make_float2(b01.z, b01.w), make_float2(b23.x, b23.y),
+                                   make_float2(b23.z, b23.w)};
               // reO = Re(S_a S_b*) - Re(X_a X_b*), S = up + dn, X = ud + du
               // imO = Im(up_a up_b* + dn_a dn_b* - ud_a ud_b* - du_a du_b*)
-              const float sax = ma[0].x + ma[1].x, say = ma[0].y + ma[1].y;
-              const float sbx = mb[0].x + mb[1].x, sby = mb[0].y + mb[1].y;
-              const float xax = ma[2].x + ma[3].x, xay = ma[2].y + ma[3].y;
-              const float xbx = mb[2].x + mb[3].x, xby = mb[2].y + mb[3].y;
+              const float sax = a[0].x + a[1].x, say = a[0].y + a[1].y;
+              const float sbx = b[0].x + b[1].x, sby = b[0].y + b[1].y;
+              const float xax = a[2].x + a[3].x, xay = a[2].y + a[3].y;
+              const float xbx = b[2].x + b[3].x, xby = b[2].y + b[3].y;
               reO = (sax * sbx + say * sby) - (xax * xbx + xay * xby);
-              imO = (ma[0].y * mb[0].x - ma[0].x * mb[0].y) + (ma[1].y * mb[1].x - ma[1].x * mb[1].y) -
-                    (ma[2].y * mb[2].x - ma[2].x * mb[2].y) - (ma[3].y * mb[3].x - ma[3].x * mb[3].y);
+              imO = (a[0].y * b[0].x - a[0].x * b[0].y) + (a[1].y * b[1].x - a[1].x * b[1].y) -
+                    (a[2].y * b[2].x - a[2].x * b[2].y) - (a[3].y * b[3].x - a[3].x * b[3].y);
             }
           }
-          p1[q] = swb[t] * reO;
-          p2[q] = -swb[t] * imO;
+          p1[q] = w8[q] * reO;
+          p2[q] = -w8[q] * imO;
         }
         uint4 h1, l1, h2, l2;
         split8(p1, h1, l1);
@@ -602,8 +636,8 @@ size_t mixed_workspace_bytes(const ContractArgs& a, long long T) {
 }
 
 size_t mixed_smem_bytes(int nch) {
-  const int nbuf = nch == 1 ? 2 : 1;  // overlap buffers (see mixed_kernel)
-  return (size_t)2 * (2 * kABytes + kWChunkBytes) + (size_t)nbuf * kKC * 16 * nch * sizeof(float2) +
+  const int nbuf = nch == 1 ? 2 : 1;  // overlap buffers of padded rows (see mixed_kernel)
+  return (size_t)2 * (2 * kABytes + kWChunkBytes) + (size_t)nbuf * 16 * (kKC * nch + 2) * sizeof(float2) +
          (size_t)nbuf * kKC * sizeof(float) + 6 * sizeof(uint64_t) + 4 * sizeof(int);
 }
 

@@ -103,7 +103,7 @@ def workload(name: str, workdir: str):
 
     si_band / si_epsLL: config 1 (Si, 121-point path; 8^3 grid, NEPS 15, 1000 w)
     gaas_epsij[_N]:     config 2 (GaAs + SOC, N^3 grid (16), NEPS 27, 2000 w, Lorentzian)
-    wz_epsLL:           config 3 (wurtzite, N_G 401, 24x24x16 grid, NEPS 59, 2000 w)
+    wz_epsLL[_N]:       config 3 (wurtzite, N_G 401, 24x24x16 grid (N x N x 3N/4), NEPS 59, 2000 w)
     te_band / te_epsLL: config 5 (trigonal Te + SOC, 2 N_G = 570; 121-point path; 10x10x8 grid)"""
     os.makedirs(workdir, exist_ok=True)
     if name == "si_band":
@@ -127,9 +127,12 @@ def workload(name: str, workdir: str):
                 "-nvalence", "8", "-nfreq", "2000", "-dfreq", "0.0125", "-delta", "1", "-epsilon", "0.05",
                 "-kk", "1"] + soc
         return argv, 1, 1 + 2 * nk
-    if name == "wz_epsLL":
-        kf = os.path.join(workdir, "k_wz_24_16.txt")
-        nk = make_kfile(kf, "wz", 24, 24, 16, f=1.626)
+    if name == "wz_epsLL" or name.startswith("wz_epsLL_"):
+        # wz_epsLL_N: the same on an N x N x (3N/4) grid (profiling-size cases)
+        n = int(name.split("_")[-1]) if name.count("_") == 2 else 24
+        nz = max(1, 3 * n // 4) if n != 24 else 16
+        kf = os.path.join(workdir, f"k_wz_{n}_{nz}.txt")
+        nk = make_kfile(kf, "wz", n, n, nz, f=1.626)
         argv = ["-switch", "epsLL", "-crystal", "wz", "-a", "3.19", "-f", "1.626", "-u", "0.375",
                 "-vg", wz_form_factors(), "-encut", "260", "-kpoint", "0", "-kpointfile", kf,
                 "-qvec", "0.01,0,0", "-neps", "59", "-nband", "48", "-nvalence", "16", "-nfreq", "2000",
