@@ -779,8 +779,25 @@ Transitions build_transitions(const Problem& p, int soc, int nval, const std::ve
       }
     blk += (long long)cs.size() * vs.size();
   }
-  if (sort_by_window)
-    std::stable_sort(raw.begin(), raw.end(), [](const Raw& a, const Raw& b) { return a.f0 < b.f0; });
+  if (sort_by_window && !raw.empty()) {
+    // stable sort by window start: a counting sort over the f0 range (a few
+    // thousand frequencies), the comparison sort only for an unusual range
+    int lo = raw[0].f0, hi = raw[0].f0;
+    for (const Raw& r : raw) {
+      lo = std::min(lo, r.f0);
+      hi = std::max(hi, r.f0);
+    }
+    if ((long long)hi - lo < (1LL << 24)) {
+      std::vector<long long> cnt((size_t)(hi - lo) + 2, 0);
+      for (const Raw& r : raw) ++cnt[(size_t)(r.f0 - lo) + 1];
+      for (size_t i = 1; i < cnt.size(); ++i) cnt[i] += cnt[i - 1];
+      std::vector<Raw> sorted(raw.size());
+      for (const Raw& r : raw) sorted[(size_t)cnt[(size_t)(r.f0 - lo)]++] = r;
+      raw.swap(sorted);
+    } else {
+      std::stable_sort(raw.begin(), raw.end(), [](const Raw& a, const Raw& b) { return a.f0 < b.f0; });
+    }
+  }
   T.T = (long long)raw.size();
   T.dest.assign(std::max<long long>(blk, 1), -1);
   T.dE.resize(raw.size());
