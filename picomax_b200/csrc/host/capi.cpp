@@ -694,9 +694,15 @@ Transitions build_transitions(const Problem& p, int soc, int nval, const std::ve
     int f0;
   };
   std::vector<Raw> raw;
+  raw.reserve((size_t)nk * (size_t)(NB / 2 + 1) * (size_t)(NB / 2 + 1));
+  T.cidx.reserve((size_t)nk * NB);
+  T.vidx.reserve((size_t)nk * NB);
   long long blk = 0;
   const double df = p.dfreq, w0 = p.freq.empty() ? 0.0 : p.freq[0];
   const int nh = 2 * p.npw();
+  std::vector<int> cs, vs;  // distinct solved conduction / valence states of a k-point
+  cs.reserve(NB);
+  vs.reserve(NB);
   for (int k = 0; k < nk; ++k) {
     const int kg = k0 + k;  // global k index
     if (NB < nh) {
@@ -740,7 +746,8 @@ Transitions build_transitions(const Problem& p, int soc, int nval, const std::ve
     while (nc < NB && spinor_eig(wk, nval, k, NB - 1 - nc, soc) - off > 0) ++nc;
     while (nv < NB && spinor_eig(wq, nval, k, nv, soc) - off <= 0) ++nv;
     // distinct solved states
-    std::vector<int> cs, vs;
+    cs.clear();
+    vs.clear();
     for (int c = 0; c < nc; ++c) {
       const int st = soc ? NB - 1 - c : (NB - 1 - c) / 2;
       if (cs.empty() || cs.back() != st) cs.push_back(st);
