@@ -20,9 +20,12 @@ namespace pmx {
 namespace dev {
 
 // ------------------------------------------------------------------- overlaps
-// One CTA per (k, conduction chunk). Each warp owns (c, v) pairs and sums over
-// the plane waves p with loci[m][p] != -1, accumulating the moments
-// sum_p conj(c(p)) v(loci p) {1, G_p.x, G_p.y, G_p.z} per spin channel. The
+// One CTA per (k, conduction chunk, valence chunk), the chunks' eigenvectors
+// staged in shared memory (rows padded by 16 bytes). Each thread owns one
+// (m, c, v) task at a time (pairs fastest, so a warp shares m and its loci
+// row) and sums over the plane waves p with loci[m][p] != -1, accumulating
+// the moments sum_p conj(c(p)) v(loci p) {1, G_p.x, G_p.y, G_p.z} per spin
+// channel in registers: no cross-lane reductions. The
 // orbital current u_i^H (G_p + k + q/2 + G_m/2) and the SOC current
 // u_i^H v_soc(G_m) (src/pmx_chi.cpp:203-266, constant over p because
 // G_loci - G_p = G_m) are then applied to the moments.
@@ -37,100 +40,98 @@ __global__ void __launch_bounds__(256) overlap_kernel(OverlapArgs a) {
   const int v_hi = min(nvd, v_lo + a.vchunk);
   if (c_lo >= c_hi || v_lo >= v_hi) return;
   const int nvl = v_hi - v_lo;
-  const int n = a.n, npw = a.npw;
+  const int n = a.n, npw = a.npw, ldn = n + 1;
   extern __shared__ __align__(16) unsigned char smraw[];
-  double2* sc = reinterpret_cast<double2*>(smraw);          // [cchunk][n]
-  double2* sv = sc + (size_t)a.cchunk * n;                   // [vchunk][n]
-  double* sg = reinterpret_cast<double*>(sv + (size_t)a.vchunk * n);  // [npw][3]
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+  double2* sc = reinterpret_cast<double2*>(smraw);           // [cchunk][ldn]
+  double2* sv = sc + (size_t)a.cchunk * ldn;                  // [vchunk][ldn]
+  double* sg = reinterpret_cast<double*>(sv + (size_t)a.vchunk * ldn);  // [npw][3]
+  const int tid = threadIdx.x;
   for (int c = c_lo; c < c_hi; ++c) {
     const double2* src = a.zk + ((size_t)k * a.nev + a.cidx[a.cbase[k] + c]) * n;
-    for (int r = tid; r < n; r += blockDim.x) sc[(size_t)(c - c_lo) * n + r] = src[r];
+    for (int r = tid; r < n; r += blockDim.x) sc[(size_t)(c - c_lo) * ldn + r] = src[r];
   }
   for (int v = v_lo; v < v_hi; ++v) {
     const double2* src = a.zq + ((size_t)k * a.nev + a.vidx[a.vbase[k] + v]) * n;
-    for (int r = tid; r < n; r += blockDim.x) sv[(size_t)(v - v_lo) * n + r] = src[r];
+    for (int r = tid; r < n; r += blockDim.x) sv[(size_t)(v - v_lo) * ldn + r] = src[r];
   }
   for (int r = tid; r < 3 * npw; r += blockDim.x) sg[r] = a.G[r];
   __syncthreads();
   const double kx = a.kpts[3 * k], ky = a.kpts[3 * k + 1], kz = a.kpts[3 * k + 2];
   const int npair = (c_hi - c_lo) * nvl;
   const int A = 3 * a.neps;
-  for (int m = 0; m < a.neps; ++m) {
+  const int ntask = a.neps * npair;
+  for (int task = tid; task < ntask; task += blockDim.x) {
+    const int m = task / npair, pr = task - m * npair;
+    const int cl = pr / nvl, v = v_lo + pr % nvl;
+    const long long dst = a.dest[a.blkoff[k] + (long long)(c_lo + cl) * nvd + v];
+    if (dst < 0) continue;
     const int* loci = a.loci + (size_t)m * npw;
-    // w = k + q/2 + G_m/2, as in (G_p + K + Q/2 + G_m/2) at src/pmx_chi.cpp:535
-    const double wx = (kx + a.q[0] / 2) + a.G[3 * m] / 2;
-    const double wy = (ky + a.q[1] / 2) + a.G[3 * m + 1] / 2;
-    const double wz = (kz + a.q[2] / 2) + a.G[3 * m + 2] / 2;
-    for (int pr = wid; pr < npair; pr += nw) {
-      const int cl = pr / nvl, v = v_lo + pr % nvl;
-      const double2* cvec = sc + (size_t)cl * n;
-      const double2* vvec = sv + (size_t)(v - v_lo) * n;
-      // moments: [0..3] spin-summed or up-up, [4..7] down-down, [8] up-down, [9] down-up
-      double2 mo[10];
+    const double2* cvec = sc + (size_t)cl * ldn;
+    const double2* vvec = sv + (size_t)(v - v_lo) * ldn;
+    // moments: [0..3] spin-summed or up-up, [4..7] down-down, [8] up-down, [9] down-up
+    double2 mo[10];
 #pragma unroll
-      for (int q = 0; q < 10; ++q) mo[q] = make_double2(0, 0);
-      for (int p = lane; p < npw; p += 32) {
-        const int lp = loci[p];
-        if (lp < 0) continue;
-        const double gx = sg[3 * p], gy = sg[3 * p + 1], gz = sg[3 * p + 2];
-        if (!a.soc) {
-          const double2 s = cmulc(cvec[p], vvec[lp]);
+    for (int q = 0; q < 10; ++q) mo[q] = make_double2(0, 0);
+    for (int p = 0; p < npw; ++p) {
+      const int lp = loci[p];
+      if (lp < 0) continue;
+      const double gx = sg[3 * p], gy = sg[3 * p + 1], gz = sg[3 * p + 2];
+      if (!a.soc) {
+        const double2 s = cmulc(cvec[p], vvec[lp]);
+        mo[0] = cadd(mo[0], s);
+        mo[1] = cadd(mo[1], cscale(s, gx));
+        mo[2] = cadd(mo[2], cscale(s, gy));
+        mo[3] = cadd(mo[3], cscale(s, gz));
+      } else {
+        const double2 cu = cvec[2 * p], cd = cvec[2 * p + 1];
+        const double2 vu = vvec[2 * lp], vd = vvec[2 * lp + 1];
+        const double2 uu = cmulc(cu, vu), dd = cmulc(cd, vd);
+        if (a.nch == 4) {
+          mo[0] = cadd(mo[0], uu);
+          mo[1] = cadd(mo[1], cscale(uu, gx));
+          mo[2] = cadd(mo[2], cscale(uu, gy));
+          mo[3] = cadd(mo[3], cscale(uu, gz));
+          mo[4] = cadd(mo[4], dd);
+          mo[5] = cadd(mo[5], cscale(dd, gx));
+          mo[6] = cadd(mo[6], cscale(dd, gy));
+          mo[7] = cadd(mo[7], cscale(dd, gz));
+          mo[8] = cadd(mo[8], cmulc(cu, vd));
+          mo[9] = cadd(mo[9], cmulc(cd, vu));
+        } else {
+          const double2 s = cadd(uu, dd);
           mo[0] = cadd(mo[0], s);
           mo[1] = cadd(mo[1], cscale(s, gx));
           mo[2] = cadd(mo[2], cscale(s, gy));
           mo[3] = cadd(mo[3], cscale(s, gz));
-        } else {
-          const double2 cu = cvec[2 * p], cd = cvec[2 * p + 1];
-          const double2 vu = vvec[2 * lp], vd = vvec[2 * lp + 1];
-          const double2 uu = cmulc(cu, vu), dd = cmulc(cd, vd);
-          if (a.nch == 4) {
-            mo[0] = cadd(mo[0], uu);
-            mo[1] = cadd(mo[1], cscale(uu, gx));
-            mo[2] = cadd(mo[2], cscale(uu, gy));
-            mo[3] = cadd(mo[3], cscale(uu, gz));
-            mo[4] = cadd(mo[4], dd);
-            mo[5] = cadd(mo[5], cscale(dd, gx));
-            mo[6] = cadd(mo[6], cscale(dd, gy));
-            mo[7] = cadd(mo[7], cscale(dd, gz));
-            mo[8] = cadd(mo[8], cmulc(cu, vd));
-            mo[9] = cadd(mo[9], cmulc(cd, vu));
-          } else {
-            const double2 s = cadd(uu, dd);
-            mo[0] = cadd(mo[0], s);
-            mo[1] = cadd(mo[1], cscale(s, gx));
-            mo[2] = cadd(mo[2], cscale(s, gy));
-            mo[3] = cadd(mo[3], cscale(s, gz));
-          }
         }
       }
-      const int nmo = a.nch == 4 ? 10 : 4;
-      for (int q = 0; q < nmo; ++q) mo[q] = warp_sum2(mo[q]);
-      const long long dst = a.dest[a.blkoff[k] + (long long)(c_lo + cl) * nvd + v];
-      if (dst < 0) continue;
-      double2* out = a.M + ((size_t)dst * A + 3 * m) * a.nch;
-      if (lane < 3) {
-        const int i = lane;
-        const double2* u = a.uvec + ((size_t)m * 3 + i) * 3;  // u_i of q+G_m
-        const double2 s = a.ssoc[m * 3 + i];                  // u_i^H v_soc(G_m)
-        // orbital current of a moment set: sum_x conj(u_x) (M_x + w_x M_0)
-        auto orb = [&](const double2* mm) {
-          double2 r = cmulc(u[0], cadd(mm[1], cscale(mm[0], wx)));
-          r = cadd(r, cmulc(u[1], cadd(mm[2], cscale(mm[0], wy))));
-          r = cadd(r, cmulc(u[2], cadd(mm[3], cscale(mm[0], wz))));
-          return r;
-        };
-        if (a.mode == 1) {  // epsLL: L = density, T = u.(v_orb + v_soc)
-          out[(size_t)i * a.nch] = i == 0 ? mo[0] : cadd(orb(mo), cmul(s, mo[0]));
-        } else if (a.nch == 1) {  // epsij without SOC: single channel, orbital current
-          out[(size_t)i * a.nch] = orb(mo);
-        } else {  // epsij with SOC: up, down, updown, downup
-          double2* o = out + (size_t)i * 4;
-          o[0] = orb(mo);
-          o[1] = orb(mo + 4);
-          o[2] = cmul(s, mo[8]);
-          o[3] = cmul(s, mo[9]);
-        }
+    }
+    // w = k + q/2 + G_m/2, as in (G_p + K + Q/2 + G_m/2) at src/pmx_chi.cpp:535
+    const double wx = (kx + a.q[0] / 2) + a.G[3 * m] / 2;
+    const double wy = (ky + a.q[1] / 2) + a.G[3 * m + 1] / 2;
+    const double wz = (kz + a.q[2] / 2) + a.G[3 * m + 2] / 2;
+    double2* out = a.M + ((size_t)dst * A + 3 * m) * a.nch;
+#pragma unroll 1
+    for (int i = 0; i < 3; ++i) {
+      const double2* u = a.uvec + ((size_t)m * 3 + i) * 3;  // u_i of q+G_m
+      const double2 s = a.ssoc[m * 3 + i];                  // u_i^H v_soc(G_m)
+      // orbital current of a moment set: sum_x conj(u_x) (M_x + w_x M_0)
+      auto orb = [&](const double2* mm) {
+        double2 r = cmulc(u[0], cadd(mm[1], cscale(mm[0], wx)));
+        r = cadd(r, cmulc(u[1], cadd(mm[2], cscale(mm[0], wy))));
+        r = cadd(r, cmulc(u[2], cadd(mm[3], cscale(mm[0], wz))));
+        return r;
+      };
+      if (a.mode == 1) {  // epsLL: L = density, T = u.(v_orb + v_soc)
+        out[(size_t)i * a.nch] = i == 0 ? mo[0] : cadd(orb(mo), cmul(s, mo[0]));
+      } else if (a.nch == 1) {  // epsij without SOC: single channel, orbital current
+        out[(size_t)i * a.nch] = orb(mo);
+      } else {  // epsij with SOC: up, down, updown, downup
+        double2* o = out + (size_t)i * 4;
+        o[0] = orb(mo);
+        o[1] = orb(mo + 4);
+        o[2] = cmul(s, mo[8]);
+        o[3] = cmul(s, mo[9]);
       }
     }
   }
@@ -149,7 +150,7 @@ cudaError_t launch_overlap(const OverlapArgs& a, int nk, cudaStream_t st) {
 }
 
 size_t overlap_smem_bytes(int cchunk, int vchunk, int n, int npw) {
-  return ((size_t)cchunk * n + (size_t)vchunk * n) * sizeof(double2) + (size_t)3 * npw * sizeof(double);
+  return ((size_t)cchunk + vchunk) * (n + 1) * sizeof(double2) + (size_t)3 * npw * sizeof(double);
 }
 
 bool overlap_tiles(int ncd_max, int nvd_max, int n, int npw, int& cchunk, int& vchunk) {

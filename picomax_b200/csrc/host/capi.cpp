@@ -677,10 +677,16 @@ struct Transitions {
 // counts k and k+q points where state NBAND-1 and NBAND are degenerate.
 // k0/k1 restrict the list to k-points [k0, k1) (wk/wq and the per-k arrays
 // then count from k0).
-Transitions build_transitions(const Problem& p, int soc, int nval, const std::vector<double>& wk,
+// The result lives in a per-thread buffer that the next call on the thread
+// rebuilds in place (large vectors freed and allocated every call would be
+// paged in again each time).
+const Transitions& build_transitions(const Problem& p, int soc, int nval, const std::vector<double>& wk,
                               const std::vector<double>& wq, double off, bool sort_by_window, int& cuts,
                               int k0 = 0, int k1 = -1, int* ties = nullptr, bool xyz = false) {
-  Transitions T;
+  static thread_local Transitions T;
+  T.T = 0;
+  T.cidx.clear();
+  T.vidx.clear();
   if (k1 < 0) k1 = p.nk();
   const int nk = k1 - k0, NB = p.nband;
   T.ncd.resize(nk);
@@ -693,7 +699,9 @@ Transitions build_transitions(const Problem& p, int soc, int nval, const std::ve
     double dE, w;
     int f0;
   };
-  std::vector<Raw> raw;
+  // kept across calls: the list is rebuilt for every q and reused in place
+  static thread_local std::vector<Raw> raw;
+  raw.clear();
   raw.reserve((size_t)nk * (size_t)(NB / 2 + 1) * (size_t)(NB / 2 + 1));
   T.cidx.reserve((size_t)nk * NB);
   T.vidx.reserve((size_t)nk * NB);
@@ -786,35 +794,39 @@ Transitions build_transitions(const Problem& p, int soc, int nval, const std::ve
       }
     blk += (long long)cs.size() * vs.size();
   }
-  if (sort_by_window && !raw.empty()) {
-    // stable sort by window start: a counting sort over the f0 range (a few
-    // thousand frequencies), the comparison sort only for an unusual range
-    int lo = raw[0].f0, hi = raw[0].f0;
-    for (const Raw& r : raw) {
-      lo = std::min(lo, r.f0);
-      hi = std::max(hi, r.f0);
-    }
-    if ((long long)hi - lo < (1LL << 24)) {
-      std::vector<long long> cnt((size_t)(hi - lo) + 2, 0);
-      for (const Raw& r : raw) ++cnt[(size_t)(r.f0 - lo) + 1];
-      for (size_t i = 1; i < cnt.size(); ++i) cnt[i] += cnt[i - 1];
-      std::vector<Raw> sorted(raw.size());
-      for (const Raw& r : raw) sorted[(size_t)cnt[(size_t)(r.f0 - lo)]++] = r;
-      raw.swap(sorted);
-    } else {
-      std::stable_sort(raw.begin(), raw.end(), [](const Raw& a, const Raw& b) { return a.f0 < b.f0; });
-    }
-  }
+  // transition t of the output: raw entries in k order, stably sorted by
+  // window start when asked (a counting sort over the f0 range, a few
+  // thousand frequencies, scattering straight into the output arrays; the
+  // comparison sort only for an unusual range)
   T.T = (long long)raw.size();
   T.dest.assign(std::max<long long>(blk, 1), -1);
   T.dE.resize(raw.size());
   T.wgt.resize(raw.size());
   T.f0.resize(raw.size());
-  for (size_t t = 0; t < raw.size(); ++t) {
-    T.dest[raw[t].src] = (long long)t;
-    T.dE[t] = raw[t].dE;
-    T.wgt[t] = raw[t].w;
-    T.f0[t] = raw[t].f0;
+  auto put = [&](size_t t, const Raw& r) {
+    T.dest[r.src] = (long long)t;
+    T.dE[t] = r.dE;
+    T.wgt[t] = r.w;
+    T.f0[t] = r.f0;
+  };
+  int lo = 0, hi = 0;
+  if (!raw.empty()) {
+    lo = hi = raw[0].f0;
+    for (const Raw& r : raw) {
+      lo = std::min(lo, r.f0);
+      hi = std::max(hi, r.f0);
+    }
+  }
+  if (!sort_by_window || raw.empty()) {
+    for (size_t t = 0; t < raw.size(); ++t) put(t, raw[t]);
+  } else if ((long long)hi - lo < (1LL << 24)) {
+    std::vector<long long> pos((size_t)(hi - lo) + 2, 0);
+    for (const Raw& r : raw) ++pos[(size_t)(r.f0 - lo) + 1];
+    for (size_t i = 1; i < pos.size(); ++i) pos[i] += pos[i - 1];
+    for (const Raw& r : raw) put((size_t)pos[(size_t)(r.f0 - lo)]++, r);
+  } else {
+    std::stable_sort(raw.begin(), raw.end(), [](const Raw& a, const Raw& b) { return a.f0 < b.f0; });
+    for (size_t t = 0; t < raw.size(); ++t) put(t, raw[t]);
   }
   return T;
 }
@@ -907,7 +919,7 @@ void chi_process_q(pmx_ctx* ctx, const Problem& p, const ChiPlan& pl, const DevC
   const bool pv = pl.pv;
   pmx::dev::ScaleArgs sa = pl.sa;
   const Vec3 Q = p.lat.Q[q];
-  Transitions T = build_transitions(p, dc.soc, nval, wk, wq, off, mode == 0, ctx->degenerate_cuts, 0, -1,
+  const Transitions& T = build_transitions(p, dc.soc, nval, wk, wq, off, mode == 0, ctx->degenerate_cuts, 0, -1,
                                     &ctx->occupation_ties, mode == 2);
   // per-m polarisation and SOC-current tables
   std::vector<double2> uv((size_t)neps * 9), ss((size_t)neps * 3);
@@ -1632,7 +1644,7 @@ extern "C" int pmx_epsm_vjp(pmx_ctx* ctx, const pmx_problem* P, const double* ch
           nsx = std::min(n, nsx + 8);
         }
         int cuts = 0;
-        Transitions T = build_transitions(p, dc.soc, nvl, wk, wq, off, false, cuts, k0, k1);
+        const Transitions& T = build_transitions(p, dc.soc, nvl, wk, wq, off, false, cuts, k0, k1);
         std::vector<double> kp(3 * (size_t)cnt);
         for (int i = 0; i < cnt; ++i)
           for (int x = 0; x < 3; ++x) kp[3 * i + x] = ks[i][x];
