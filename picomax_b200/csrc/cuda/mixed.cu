@@ -9,9 +9,9 @@
 // Operands are split into BF16 pairs, x = hi + lo, and every chunk issues
 // hi*hi + hi*lo + lo*hi as tcgen05.mma kind::f16 with an FP32 accumulator in
 // TMEM (products dropped: lo*lo, ~2^-16 of each term). The transition range
-// of a frequency tile is cut into pieces; each piece's FP32 partial tile is
-// written out and the pieces are summed in FP64 in a fixed order, so results
-// are deterministic.
+// of a frequency tile is cut into pieces; each piece adds its FP32
+// accumulator into an FP64 partial tile every 64 chunks, and the pieces'
+// tiles are summed in FP64 in a fixed order, so results are deterministic.
 //
 // Pipeline of one CTA (8 producer warps + 1 control warp, two shared-memory
 // stages):
