@@ -17,6 +17,7 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../../include/picomax.h"
@@ -803,11 +804,18 @@ const Transitions& build_transitions(const Problem& p, int soc, int nval, const 
   T.dE.resize(raw.size());
   T.wgt.resize(raw.size());
   T.f0.resize(raw.size());
-  auto put = [&](size_t t, const Raw& r) {
-    T.dest[r.src] = (long long)t;
-    T.dE[t] = r.dE;
-    T.wgt[t] = r.w;
-    T.f0[t] = r.f0;
+  // plain pointers: the worker threads below must not name this thread's
+  // thread_local buffers (each thread has its own)
+  long long* o_dest = T.dest.data();
+  double* o_dE = T.dE.data();
+  double* o_wgt = T.wgt.data();
+  int* o_f0 = T.f0.data();
+  const Raw* in = raw.data();
+  auto put = [=](size_t t, const Raw& r) {
+    o_dest[r.src] = (long long)t;
+    o_dE[t] = r.dE;
+    o_wgt[t] = r.w;
+    o_f0[t] = r.f0;
   };
   int lo = 0, hi = 0;
   if (!raw.empty()) {
@@ -820,10 +828,36 @@ const Transitions& build_transitions(const Problem& p, int soc, int nval, const 
   if (!sort_by_window || raw.empty()) {
     for (size_t t = 0; t < raw.size(); ++t) put(t, raw[t]);
   } else if ((long long)hi - lo < (1LL << 24)) {
-    std::vector<long long> pos((size_t)(hi - lo) + 2, 0);
-    for (const Raw& r : raw) ++pos[(size_t)(r.f0 - lo) + 1];
-    for (size_t i = 1; i < pos.size(); ++i) pos[i] += pos[i - 1];
-    for (const Raw& r : raw) put((size_t)pos[(size_t)(r.f0 - lo)]++, r);
+    // parallel stable counting sort: contiguous parts of the k-ordered list,
+    // one histogram per part; bucket b of part j starts after bucket b of
+    // parts < j and after all smaller buckets, so the order is the serial one
+    const size_t nb = (size_t)(hi - lo) + 1, nr = raw.size();
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int parts = (int)std::min<size_t>(std::min<unsigned>(hw, 16u), std::max<size_t>(1, nr / 32768));
+    std::vector<std::vector<long long>> cnt(parts, std::vector<long long>(nb, 0));
+    auto range = [&](int j) { return std::make_pair(nr * j / parts, nr * (j + 1) / parts); };
+    auto run = [&](auto&& fn) {
+      std::vector<std::thread> th;
+      for (int j = 1; j < parts; ++j) th.emplace_back(fn, j);
+      fn(0);
+      for (auto& t : th) t.join();
+    };
+    run([&](int j) {
+      const auto rg = range(j);
+      for (size_t t = rg.first; t < rg.second; ++t) ++cnt[j][(size_t)(in[t].f0 - lo)];
+    });
+    long long acc = 0;
+    for (size_t b = 0; b < nb; ++b)
+      for (int j = 0; j < parts; ++j) {
+        const long long c = cnt[j][b];
+        cnt[j][b] = acc;
+        acc += c;
+      }
+    run([&](int j) {
+      const auto rg = range(j);
+      std::vector<long long>& pos = cnt[j];
+      for (size_t t = rg.first; t < rg.second; ++t) put((size_t)pos[(size_t)(in[t].f0 - lo)]++, in[t]);
+    });
   } else {
     std::stable_sort(raw.begin(), raw.end(), [](const Raw& a, const Raw& b) { return a.f0 < b.f0; });
     for (size_t t = 0; t < raw.size(); ++t) put(t, raw[t]);
