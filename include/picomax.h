@@ -115,6 +115,11 @@ int pmx_ctx_kernel_time(const pmx_ctx* ctx, const char* family, double* ms, long
  * call: max over all transitions and G of ||M_fp32|^2 - |M|^2| and max |M|^2.
  * New diagnostic (no reference counterpart). */
 int pmx_ctx_overlap_error(const pmx_ctx* ctx, double* max_abs2_err, double* max_abs2);
+/* Tensor-core work of the mixed path: tcgen05 MMA instructions (M 128, N 256,
+ * K 16, BF16 operands, 2*128*256*16 flop each; the split products hi*hi,
+ * hi*lo and lo*hi counted separately) issued by the mixed contractions of
+ * this context so far. New diagnostic (no reference counterpart). */
+int pmx_ctx_mixed_mmas(const pmx_ctx* ctx, long long* mmas);
 /* Autotuner of the batched eigensolver schedule (on by default): the first
  * batch of at least 148 matrices of a given size times every schedule once,
  * keeps the fastest for the rest of the context's life. New in this build. */

@@ -37,7 +37,7 @@ EXPORTS = (
     "pmx_ctx_stage_times", "pmx_ctx_kernel_launches", "pmx_hamiltonian", "pmx_heev_batched",
     "pmx_ref_energy", "pmx_band", "pmx_chi", "pmx_kk", "pmx_main", "pmx_ctx_stream",
     "pmx_ctx_transfer_bytes", "pmx_ctx_degenerate_cuts", "pmx_chi_device", "pmx_chi_epsm",
-    "pmx_eps_macroscopic", "pmx_ctx_kernel_time", "pmx_ctx_set_autotune", "pmx_ctx_set_schedule", "pmx_ctx_tuning",
+    "pmx_eps_macroscopic", "pmx_ctx_kernel_time", "pmx_ctx_set_autotune", "pmx_ctx_set_schedule", "pmx_ctx_tuning", "pmx_ctx_mixed_mmas",
     "pmx_ctx_overlap_error",
     "pmx_heev_batched_noalloc",
     "pmx_problem_params",
@@ -110,6 +110,7 @@ def load() -> ctypes.CDLL:
         "pmx_ctx_kernel_time": (c_int, [c_void_p, c_char_p, dp, POINTER(c_longlong)]),
         "pmx_ctx_set_autotune": (c_int, [c_void_p, c_int]),
         "pmx_ctx_set_schedule": (c_int, [c_void_p, c_int]),
+        "pmx_ctx_mixed_mmas": (c_int, [c_void_p, POINTER(c_longlong)]),
         "pmx_ctx_overlap_error": (c_int, [c_void_p, dp, dp]),
         "pmx_heev_batched_noalloc": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
         "pmx_problem_params": (c_int, [c_void_p, dp, ip]),
@@ -307,6 +308,12 @@ class Context:
 
     def set_autotune(self, on: bool):
         self._lib.pmx_ctx_set_autotune(self.handle, 1 if on else 0)
+
+    def mixed_mmas(self) -> int:
+        """tcgen05 MMA instructions (M128 N256 K16) of the mixed contractions so far."""
+        v = c_longlong()
+        self._check(self._lib.pmx_ctx_mixed_mmas(self.handle, ctypes.byref(v)), "mixed_mmas")
+        return int(v.value)
 
     def set_schedule(self, schedule: int):
         """Fix the eigensolver schedule for later batches (-1: autotuner)."""

@@ -673,8 +673,10 @@ __global__ void m_to_f32_kernel(const double2* __restrict__ M, float2* __restric
   }
 }
 
-cudaError_t launch_contract_mixed(const ContractArgs& a, long long T, void* ws, int& nlaunch, cudaStream_t st) {
+cudaError_t launch_contract_mixed(const ContractArgs& a, long long T, void* ws, int& nlaunch, cudaStream_t st,
+                                  long long* mmas) {
   nlaunch = 0;
+  if (mmas) *mmas = 0;
   const int nft = (a.nf + kN - 1) / kN;
   // transition range of every 256-wide frequency tile (the FP64 tiles are 64 wide)
   std::vector<int2> tr(nft);
@@ -778,6 +780,8 @@ cudaError_t launch_contract_mixed(const ContractArgs& a, long long T, void* ws, 
   e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return e;
   if (err != 0) return cudaErrorTimeout;
+  // every chunk is multiplied by every pair tile: 3 products x 2 K steps
+  if (mmas) *mmas = 6LL * pl.ntile * pl.nchunk;
   return cudaSuccess;
 }
 

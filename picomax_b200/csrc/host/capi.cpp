@@ -261,6 +261,7 @@ struct pmx_ctx {
   // several crystals at once (batched entry points)
   DevBuf b_g, b_hkl, b_vloc, b_vso, b_crystal;
   double m2_err = 0.0, m2_max = 0.0;  // |M|^2 error of the mixed path's FP32 overlaps (last call)
+  long long mixed_mmas = 0;            // tcgen05 MMA instructions of the mixed contractions so far
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // 0-1 stage timers, 2-3 the autotuner
 };
 
@@ -1082,7 +1083,9 @@ void chi_process_q(pmx_ctx* ctx, const Problem& p, const ChiPlan& pl, const DevC
       ca.stats = ctx->stats.as<double>();
       {
         KTime kt(ctx, "contract_mixed");
-        CK(pmx::dev::launch_contract_mixed(ca, (long long)T.T, ctx->mixws.ptr, nl, st));
+        long long mm = 0;
+        CK(pmx::dev::launch_contract_mixed(ca, (long long)T.T, ctx->mixws.ptr, nl, st, &mm));
+        ctx->mixed_mmas += mm;
       }
       ctx->launches += nl;
       double sv[2] = {0, 0};
@@ -1231,6 +1234,12 @@ extern "C" int pmx_ctx_overlap_error(const pmx_ctx* c, double* max_abs2_err, dou
   if (!c) return PMX_ERR_INVALID;
   if (max_abs2_err) *max_abs2_err = c->m2_err;
   if (max_abs2) *max_abs2 = c->m2_max;
+  return PMX_OK;
+}
+
+extern "C" int pmx_ctx_mixed_mmas(const pmx_ctx* c, long long* mmas) {
+  if (!c || !mmas) return PMX_ERR_INVALID;
+  *mmas = c->mixed_mmas;
   return PMX_OK;
 }
 
