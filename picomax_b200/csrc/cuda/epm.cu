@@ -23,6 +23,7 @@
 #include "pmx_common.cuh"
 #include "pmx_device.hpp"
 #include "pmx_tri.cuh"
+#include "pmx_trieig.cuh"
 
 namespace pmx {
 namespace dev {
@@ -34,7 +35,18 @@ __global__ void __launch_bounds__(256) assemble_kernel(const CrystalDev* __restr
   const EigItem it = items[blockIdx.y];
   const CrystalDev C = crystals[it.crystal];
   const int npw = C.npw, n = it.n, side = C.side, off = 2 * C.imax;
+  const int ld = it.ld > 0 ? it.ld : n;
   double2* H = hbuf + it.h_off;
+  if (ld > n) {  // zero padding: rows n..ld-1 of every column, then columns n..ld-1
+    const long long pr = (long long)(ld - n) * ld, total = pr + (long long)n * (ld - n);
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+      if (idx < pr)
+        H[(idx / (ld - n)) * ld + n + idx % (ld - n)] = make_double2(0, 0);
+      else
+        H[(n + (idx - pr) / n) * (long long)ld + (idx - pr) % n] = make_double2(0, 0);
+    }
+  }
   const double kx = it.k[0], ky = it.k[1], kz = it.k[2];
   const long long total = (long long)npw * npw;
   for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
@@ -53,7 +65,7 @@ __global__ void __launch_bounds__(256) assemble_kernel(const CrystalDev* __restr
       h0 = C.vloc[((long long)dh * side + dk) * side + dl];
     }
     if (!C.soc) {
-      H[(long long)j * n + i] = lower ? h0 : cconj(h0);
+      H[(long long)j * ld + i] = lower ? h0 : cconj(h0);
       continue;
     }
     // spin-orbit block of the lower pair (a, b): q = G_b - G_a
@@ -79,8 +91,8 @@ __global__ void __launch_bounds__(256) assemble_kernel(const CrystalDev* __restr
         blk[1][0] = make_double2(sx.x - sy.y, sx.y + sy.x);  // Sx + i Sy
       }
     }
-    double2* col0 = H + (long long)(2 * j) * n + 2 * i;
-    double2* col1 = col0 + n;
+    double2* col0 = H + (long long)(2 * j) * ld + 2 * i;
+    double2* col1 = col0 + ld;
     if (lower) {
       col0[0] = blk[0][0];
       col0[1] = blk[1][0];
@@ -111,37 +123,11 @@ namespace {
 
 constexpr int kHeevThreads = 256;
 constexpr int kWarps = kHeevThreads / 32;
-constexpr int kBisectIters = 200;   // cap; multisection converges in ~15
-constexpr int kInvIters = 3;
-
-__device__ __forceinline__ int sturm_count(const double* d, const double* e2, int n, double x,
-                                           double pivmin) {
-  double q = d[0] - x;
-  if (fabs(q) < pivmin) q = -pivmin;
-  int c = q < 0.0;
-  for (int i = 1; i < n; ++i) {
-    q = d[i] - x - e2[i - 1] / q;
-    if (fabs(q) < pivmin) q = -pivmin;
-    c += q < 0.0;
-  }
-  return c;
-}
-
-__device__ __forceinline__ double hash_uniform(unsigned long long a, unsigned long long b) {
-  unsigned long long x = a * 0x9E3779B97F4A7C15ull ^ (b + 0x632BE59BD9B4E019ull);
-  x ^= x >> 31;
-  x *= 0xBF58476D1CE4E5B9ull;
-  x ^= x >> 27;
-  x *= 0x94D049BB133111EBull;
-  x ^= x >> 31;
-  return ((double)(x >> 11) * (1.0 / 9007199254740992.0)) * 2.0 - 1.0;  // (-1, 1)
-}
-
 // Lower triangle of an n x n matrix; col(c)[r - c] = A(r, c) for r >= c.
-struct LowerFull {  // column-major n x n in global memory (upper half unused)
+struct LowerFull {  // column-major in global memory, leading dimension ld (upper half unused)
   double2* A;
-  int n;
-  __device__ __forceinline__ double2* col(int c) const { return A + (size_t)c * n + c; }
+  int ld;
+  __device__ __forceinline__ double2* col(int c) const { return A + (size_t)c * ld + c; }
 };
 struct LowerPacked {  // packed columns in shared memory
   double2* A;
@@ -402,6 +388,7 @@ __global__ void __launch_bounds__(kHeevThreads, OCC > 0 ? OCC : ((RING >= 2 || M
                                                                double* __restrict__ tri_out) {
   const EigItem it = items[blockIdx.x];
   const int n = it.n, nev = it.nval, nvec = it.want_vec ? it.nev : 0;
+  const int ld = it.ld > 0 ? it.ld : n;  // leading dimension of the item's matrix
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int nthr = blockDim.x, nw = nthr >> 5;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -437,114 +424,19 @@ __global__ void __launch_bounds__(kHeevThreads, OCC > 0 ? OCC : ((RING >= 2 || M
     const LowerPacked pk{Apacked, n};
     for (int c = wid; c < n; c += nw) {
       double2* dst = pk.col(c);
-      for (int r = c + lane; r < n; r += 32) dst[r - c] = src[(size_t)c * n + r];
+      for (int r = c + lane; r < n; r += 32) dst[r - c] = src[(size_t)c * ld + r];
     }
     __syncthreads();
     tridiag_lower<MAXS, 0>(pk, n, vprev, wprev, vcur, dotp, tau, part, cnext, wring, d, e, red);
   } else {
-    tridiag_lower<MAXS, RING, LowerFull, YS>(LowerFull{hbuf + it.h_off, n}, n, vprev, wprev, vcur, dotp, tau, part,
+    tridiag_lower<MAXS, RING, LowerFull, YS>(LowerFull{hbuf + it.h_off, ld}, n, vprev, wprev, vcur, dotp, tau, part,
                                              cnext, wring,
                               d, e, red);
   }
 
   // ------------------------------------------------------------- eigenvalues
-  // Gershgorin interval, pivmin, and negligible off-diagonals set to zero.
-  if (tid == 0) {
-    double glo = d[0], ghi = d[0], emax2 = 0.0, tnorm = 0.0;
-    for (int i = 0; i < n; ++i) {
-      const double el = i > 0 ? fabs(e[i - 1]) : 0.0, er = i < n - 1 ? fabs(e[i]) : 0.0;
-      glo = fmin(glo, d[i] - el - er);
-      ghi = fmax(ghi, d[i] + el + er);
-      tnorm = fmax(tnorm, fabs(d[i]) + el + er);
-    }
-    for (int i = 0; i < n - 1; ++i) {
-      if (fabs(e[i]) <= DBL_EPSILON * (fabs(d[i]) + fabs(d[i + 1]))) e[i] = 0.0;
-      e2[i] = e[i] * e[i];
-      emax2 = fmax(emax2, e2[i]);
-    }
-    const double pad = 2.0 * DBL_EPSILON * tnorm * n + DBL_MIN;
-    red[0] = glo - pad;
-    red[1] = ghi + pad;
-    red[2] = DBL_MIN * fmax(1.0, emax2);
-    red[3] = tnorm;
-  }
-  __syncthreads();
-  const double pivmin = red[2], tnorm = red[3];
-  for (int k = tid; k < nev; k += nthr) {
-    lo[k] = red[0];
-    hi[k] = red[1];
-  }
-  // multisection: G threads per eigenvalue probe G interior points at once
-  const int G = nev > 0 ? max(1, nthr / nev) : 1;
-  __syncthreads();
-  int converged = 0;
-  if (nev > nthr) {
-    // more eigenvalues than threads: plain bisection, each thread owns the
-    // eigenvalues tid, tid + nthr, ...
-    for (int iter = 0; iter < kBisectIters; ++iter) {
-      int done = 1;
-      for (int k = tid; k < nev; k += nthr) {
-        double l = lo[k], h = hi[k];
-        const double tol = 2.0 * DBL_EPSILON * fmax(fabs(l), fabs(h)) + 4.0 * pivmin;
-        if (h - l > tol) {
-          const double x = l + 0.5 * (h - l);
-          if (sturm_count(d, e2, n, x, pivmin) <= k)
-            l = x;
-          else
-            h = x;
-          lo[k] = l;
-          hi[k] = h;
-          done &= (h - l) <= tol ? 1 : 0;
-        }
-      }
-      done = __syncthreads_and(done);
-      if (done) {
-        converged = 1;
-        break;
-      }
-    }
-  }
-  for (int iter = 0; iter < kBisectIters && !converged && nev <= nthr; ++iter) {
-    const int k = tid / G, g = tid % G;
-    if (k < nev) {
-      const double l = lo[k], h = hi[k];
-      const double x = l + (h - l) * (double)(g + 1) / (double)(G + 1);
-      xs[tid] = x;
-      cnt[tid] = sturm_count(d, e2, n, x, pivmin);
-    }
-    __syncthreads();
-    int done = 1;
-    if (tid < nev) {
-      const int kk = tid;
-      double l = lo[kk], h = hi[kk];
-      const double tol = 2.0 * DBL_EPSILON * fmax(fabs(l), fabs(h)) + 4.0 * pivmin;
-      if (h - l > tol) {
-        for (int gg = 0; gg < G; ++gg) {
-          const int t = kk * G + gg;
-          if (cnt[t] <= kk)
-            l = fmax(l, xs[t]);
-          else
-            h = fmin(h, xs[t]);
-        }
-        lo[kk] = l;
-        hi[kk] = h;
-        done = (h - l) <= tol;
-      }
-    }
-    done = __syncthreads_and(done);
-    if (done) {
-      converged = 1;
-      break;
-    }
-  }
-  int finite = 1;
-  for (int k = tid; k < nev; k += nthr) {
-    lam[k] = 0.5 * (lo[k] + hi[k]);
-    wbuf[it.w_off + k] = lam[k];
-    finite &= isfinite(lam[k]) ? 1 : 0;
-  }
-  finite = __syncthreads_and(finite);
-  const int status = !finite ? 2 : (!converged ? 1 : 0);
+  const TriWork tw{d, e, e2, red, lam, lo, hi, xs, cnt, clus, misc};
+  const int status = tri_eigvals(tw, n, nev, wbuf + it.w_off);
   if (tri_out) {
     // H = Q T Q^H for the adjoint: T (d, e after deflation), the reflector
     // scalars tau, and (resident path) the reflectors back into hbuf
@@ -561,7 +453,7 @@ __global__ void __launch_bounds__(kHeevThreads, OCC > 0 ? OCC : ((RING >= 2 || M
       double2* dst = hbuf + it.h_off;
       for (int c = wid; c < n; c += nw) {
         const double2* col = pk.col(c);
-        for (int r = c + lane; r < n; r += 32) dst[(size_t)c * n + r] = col[r - c];
+        for (int r = c + lane; r < n; r += 32) dst[(size_t)c * ld + r] = col[r - c];
       }
     }
   }
@@ -571,53 +463,7 @@ __global__ void __launch_bounds__(kHeevThreads, OCC > 0 ? OCC : ((RING >= 2 || M
   }
 
   // ----------------------------------------------- tridiagonal eigenvectors
-  // clusters of eigenvalues closer than 1e-5 |T| are reorthogonalised.
-  if (tid == 0) {
-    int nc = 0;
-    const double gap = 1e-5 * tnorm;
-    for (int k = 0; k < nvec; ++k)
-      if (k == 0 || lam[k] - lam[k - 1] > gap) clus[nc++] = k;
-    clus[nc] = nvec;
-    misc[0] = nc;
-  }
-  __syncthreads();
-  const int ncl = misc[0];
-  const double tiny = DBL_EPSILON * fmax(tnorm, DBL_MIN);
-  // One thread per cluster; the four work arrays of the ncl clusters are
-  // interleaved (element i of cluster cl at [i * ncl + cl]) so that the
-  // threads of a warp, which step through the rows together, read and write
-  // consecutive addresses. 4 n ncl <= 4 n nvec doubles of the item's scratch.
-  for (int cl = tid; cl < ncl; cl += nthr) {
-    double* u0 = scratch + it.s_off + cl;
-    double* u1 = u0 + (size_t)n * ncl;
-    double* u2 = u1 + (size_t)n * ncl;
-    double* x = u2 + (size_t)n * ncl;
-    auto X = [&](int i) -> double& { return x[(size_t)i * ncl]; };
-    for (int k = clus[cl]; k < clus[cl + 1]; ++k) {
-      for (int i = 0; i < n; ++i) X(i) = hash_uniform(((unsigned long long)blockIdx.x << 20) + k, i);
-      for (int iter = 0; iter < kInvIters; ++iter) {
-        tri_solve(d, e, n, lam[k], tiny, x, u0, u1, u2, ncl);
-        for (int kp = clus[cl]; kp < k; ++kp) {
-          const double2* zp = zbuf + it.z_off + (size_t)kp * n;
-          double s = 0.0;
-          for (int i = 0; i < n; ++i) s += zp[i].x * X(i);
-          for (int i = 0; i < n; ++i) X(i) -= s * zp[i].x;
-        }
-        double s = 0.0, mx = 0.0;
-        for (int i = 0; i < n; ++i) mx = fmax(mx, fabs(X(i)));
-        if (!(mx > 0.0) || !isfinite(mx)) mx = 1.0;
-        for (int i = 0; i < n; ++i) {
-          X(i) /= mx;
-          s += X(i) * X(i);
-        }
-        s = 1.0 / sqrt(s);
-        for (int i = 0; i < n; ++i) X(i) *= s;
-      }
-      double2* zk = zbuf + it.z_off + (size_t)k * n;
-      for (int i = 0; i < n; ++i) zk[i] = make_double2(X(i), 0.0);
-    }
-  }
-  __syncthreads();
+  tri_eigvecs(tw, n, nvec, zbuf + it.z_off, scratch + it.s_off, blockIdx.x);
 
   // ----------------------------------------------------------- back-transform
   // x = H_0 H_1 ... H_{n-2} z ; one warp per eigenvector, no block barriers.
@@ -630,7 +476,7 @@ __global__ void __launch_bounds__(kHeevThreads, OCC > 0 ? OCC : ((RING >= 2 || M
     constexpr bool kPf = 8 * MAXS + 48 <= kRegs;
     double2* zs = part + (size_t)wid * n;
     auto vcol = [&](int j) {
-      return RESIDENT ? LowerPacked{Apacked, n}.col(j) : LowerFull{hbuf + it.h_off, n}.col(j);
+      return RESIDENT ? LowerPacked{Apacked, n}.col(j) : LowerFull{hbuf + it.h_off, ld}.col(j);
     };
     for (int k = wid; k < nvec; k += nw) {
       double2* zg = zbuf + it.z_off + (size_t)k * n;
@@ -693,7 +539,7 @@ __global__ void __launch_bounds__(kHeevThreads, OCC > 0 ? OCC : ((RING >= 2 || M
       for (int j = n - 2; j >= 0; --j) {
         const double2 tj = tau[j];
         if (tj.x == 0.0 && tj.y == 0.0) continue;
-        const double2* v = (RESIDENT ? LowerPacked{Apacked, n}.col(j) : LowerFull{hbuf + it.h_off, n}.col(j)) - j;
+        const double2* v = (RESIDENT ? LowerPacked{Apacked, n}.col(j) : LowerFull{hbuf + it.h_off, ld}.col(j)) - j;
         double2 s = make_double2(0, 0);
         for (int r = j + 1 + lane; r < n; r += 32) s = cadd(s, cmulc(v[r], z[r]));
         s = cmul(tj, warp_sum2(s));

@@ -39,9 +39,13 @@ struct EigItem {
   long long w_off;    // double offset of nval eigenvalues
   long long z_off;    // double2 offset of nev eigenvectors (column s at z_off + s*n)
   long long s_off;    // double offset of the item's scratch (heev_scratch_doubles)
+  int ld;             // leading dimension of the matrix (0: n); rows n..ld-1 and columns
+                      // n..ld-1 of the workspace are zero when ld > n
+  long long r_off;    // double2 offset of the two-stage path's band reflectors (heev2_reflector_count)
 };
 
-// Fills H(k) of every item (full Hermitian storage) into hbuf.
+// Fills H(k) of every item (full Hermitian storage, leading dimension
+// EigItem::ld, padding rows and columns zero) into hbuf.
 cudaError_t launch_assemble(const CrystalDev* crystals, const EigItem* items, int nitems,
                             int max_npw, double2* hbuf, cudaStream_t st);
 
@@ -68,6 +72,17 @@ int heev_variants(int max_n, int max_nev);
 // schedule for (max_n, max_nev). A batch that is a multiple of it fills every
 // wave of CTAs whichever schedule runs.
 int heev_batch_unit(int max_n, int max_nev);
+
+// Two-stage eigensolver (eig2.cu): dense -> band (16 sub-diagonals) on the
+// FP64 tensor cores, band -> tridiagonal by bulge chasing in shared memory,
+// bisection + inverse iteration, back-transforms. Items carry ld =
+// heev2_ld(n) (the workspace padded with zeros, see launch_assemble) and
+// r_off, spaced by at least heev2_rbuf_double2(ld) double2 in rbuf.
+int heev2_ld(int n);
+bool heev2_supported(int max_n);
+size_t heev2_rbuf_double2(int ld);
+cudaError_t launch_heev2(const EigItem* items, int nitems, int max_n, int max_nval, int max_nvec, double2* hbuf,
+                         double* wbuf, double2* zbuf, double* scratch, double2* rbuf, int* info, cudaStream_t st);
 
 }  // namespace dev
 }  // namespace pmx

@@ -1,0 +1,230 @@
+// Eigenpairs of a real symmetric tridiagonal matrix T (diagonal d, off-diagonal
+// e) by one CTA: multisection bisection on Sturm counts for the lowest nval
+// eigenvalues, then inverse iteration with modified Gram-Schmidt inside
+// eigenvalue clusters for the lowest nvec eigenvectors. Shared by the one-stage
+// eigensolver (heev_kernel) and the tridiagonal stage of the two-stage one.
+//
+// LAPACK's dstebz / dstein (the tridiagonal stages behind Eigen's
+// SelfAdjointEigenSolver results in the reference, src/pmx_epm.cpp:232) are
+// the published methods restated here: Gershgorin interval, pivmin-guarded
+// Sturm counts, bisection to 2 eps |lambda| + 4 pivmin, inverse iteration from
+// a pseudo-random start.
+#pragma once
+
+#include <cfloat>
+#include <cmath>
+
+#include <cuda_runtime.h>
+
+#include "pmx_common.cuh"
+#include "pmx_tri.cuh"
+
+namespace pmx {
+namespace dev {
+
+constexpr int kTriBisectIters = 200;  // cap; multisection converges in ~15 rounds
+constexpr int kTriInvIters = 3;
+
+__device__ __forceinline__ int sturm_count(const double* d, const double* e2, int n, double x, double pivmin) {
+  double q = d[0] - x;
+  if (fabs(q) < pivmin) q = -pivmin;
+  int c = q < 0.0;
+  for (int i = 1; i < n; ++i) {
+    q = d[i] - x - e2[i - 1] / q;
+    if (fabs(q) < pivmin) q = -pivmin;
+    c += q < 0.0;
+  }
+  return c;
+}
+
+__device__ __forceinline__ double hash_uniform(unsigned long long a, unsigned long long b) {
+  unsigned long long x = a * 0x9E3779B97F4A7C15ull ^ (b + 0x632BE59BD9B4E019ull);
+  x ^= x >> 31;
+  x *= 0xBF58476D1CE4E5B9ull;
+  x ^= x >> 27;
+  x *= 0x94D049BB133111EBull;
+  x ^= x >> 31;
+  return ((double)(x >> 11) * (1.0 / 9007199254740992.0)) * 2.0 - 1.0;  // (-1, 1)
+}
+
+// Shared-memory work arrays of the tridiagonal stage.
+struct TriWork {
+  double* d;     // [n] diagonal
+  double* e;     // [n] off-diagonal (e[n-1] unused); negligible entries are zeroed
+  double* e2;    // [n] squares of e
+  double* red;   // [4+] Gershgorin interval, pivmin, |T|
+  double* lam;   // [nval] eigenvalues
+  double* lo;    // [nval] bisection brackets
+  double* hi;    // [nval]
+  double* xs;    // [blockDim.x] multisection probes
+  int* cnt;      // [blockDim.x] their Sturm counts
+  int* clus;     // [nvec + 1] cluster starts
+  int* misc;     // [4]
+};
+
+// Lowest nval eigenvalues of T into lam[] and wout[]. Returns 0, 1 (bisection
+// did not converge) or 2 (non-finite eigenvalue). Every thread of the block
+// calls it; contains block barriers.
+__device__ inline int tri_eigvals(const TriWork& W, int n, int nval, double* __restrict__ wout) {
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  double *d = W.d, *e = W.e, *e2 = W.e2, *red = W.red, *lo = W.lo, *hi = W.hi, *xs = W.xs, *lam = W.lam;
+  int* cnt = W.cnt;
+  // Gershgorin interval, pivmin, and negligible off-diagonals set to zero.
+  if (tid == 0) {
+    double glo = d[0], ghi = d[0], emax2 = 0.0, tnorm = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double el = i > 0 ? fabs(e[i - 1]) : 0.0, er = i < n - 1 ? fabs(e[i]) : 0.0;
+      glo = fmin(glo, d[i] - el - er);
+      ghi = fmax(ghi, d[i] + el + er);
+      tnorm = fmax(tnorm, fabs(d[i]) + el + er);
+    }
+    for (int i = 0; i < n - 1; ++i) {
+      if (fabs(e[i]) <= DBL_EPSILON * (fabs(d[i]) + fabs(d[i + 1]))) e[i] = 0.0;
+      e2[i] = e[i] * e[i];
+      emax2 = fmax(emax2, e2[i]);
+    }
+    const double pad = 2.0 * DBL_EPSILON * tnorm * n + DBL_MIN;
+    red[0] = glo - pad;
+    red[1] = ghi + pad;
+    red[2] = DBL_MIN * fmax(1.0, emax2);
+    red[3] = tnorm;
+  }
+  __syncthreads();
+  const double pivmin = red[2];
+  for (int k = tid; k < nval; k += nthr) {
+    lo[k] = red[0];
+    hi[k] = red[1];
+  }
+  // multisection: G threads per eigenvalue probe G interior points at once
+  const int G = nval > 0 ? max(1, nthr / nval) : 1;
+  __syncthreads();
+  int converged = 0;
+  if (nval > nthr) {
+    // more eigenvalues than threads: plain bisection, each thread owns the
+    // eigenvalues tid, tid + nthr, ...
+    for (int iter = 0; iter < kTriBisectIters; ++iter) {
+      int done = 1;
+      for (int k = tid; k < nval; k += nthr) {
+        double l = lo[k], h = hi[k];
+        const double tol = 2.0 * DBL_EPSILON * fmax(fabs(l), fabs(h)) + 4.0 * pivmin;
+        if (h - l > tol) {
+          const double x = l + 0.5 * (h - l);
+          if (sturm_count(d, e2, n, x, pivmin) <= k)
+            l = x;
+          else
+            h = x;
+          lo[k] = l;
+          hi[k] = h;
+          done &= (h - l) <= tol ? 1 : 0;
+        }
+      }
+      done = __syncthreads_and(done);
+      if (done) {
+        converged = 1;
+        break;
+      }
+    }
+  }
+  for (int iter = 0; iter < kTriBisectIters && !converged && nval <= nthr; ++iter) {
+    const int k = tid / G, g = tid % G;
+    if (k < nval) {
+      const double l = lo[k], h = hi[k];
+      const double x = l + (h - l) * (double)(g + 1) / (double)(G + 1);
+      xs[tid] = x;
+      cnt[tid] = sturm_count(d, e2, n, x, pivmin);
+    }
+    __syncthreads();
+    int done = 1;
+    if (tid < nval) {
+      const int kk = tid;
+      double l = lo[kk], h = hi[kk];
+      const double tol = 2.0 * DBL_EPSILON * fmax(fabs(l), fabs(h)) + 4.0 * pivmin;
+      if (h - l > tol) {
+        for (int gg = 0; gg < G; ++gg) {
+          const int t = kk * G + gg;
+          if (cnt[t] <= kk)
+            l = fmax(l, xs[t]);
+          else
+            h = fmin(h, xs[t]);
+        }
+        lo[kk] = l;
+        hi[kk] = h;
+        done = (h - l) <= tol;
+      }
+    }
+    done = __syncthreads_and(done);
+    if (done) {
+      converged = 1;
+      break;
+    }
+  }
+  int finite = 1;
+  for (int k = tid; k < nval; k += nthr) {
+    lam[k] = 0.5 * (lo[k] + hi[k]);
+    wout[k] = lam[k];
+    finite &= isfinite(lam[k]) ? 1 : 0;
+  }
+  finite = __syncthreads_and(finite);
+  return !finite ? 2 : (!converged ? 1 : 0);
+}
+
+// Lowest nvec eigenvectors of T (after tri_eigvals) as real vectors in the
+// real parts of z[k * n + i] (imaginary parts zero). Clusters of eigenvalues
+// closer than 1e-5 |T| are reorthogonalised. One thread per cluster; the four
+// work arrays of the clusters are interleaved in `scratch` (element i of
+// cluster cl at [i * ncl + cl], 4 n nvec doubles at most) so that the threads
+// of a warp, which step through the rows together, read and write consecutive
+// addresses. `seed` makes the pseudo-random start vectors differ per matrix.
+__device__ inline void tri_eigvecs(const TriWork& W, int n, int nvec, double2* __restrict__ z,
+                                   double* __restrict__ scratch, unsigned long long seed) {
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const double* d = W.d;
+  const double* e = W.e;
+  const double* lam = W.lam;
+  const double tnorm = W.red[3];
+  if (tid == 0) {
+    int nc = 0;
+    const double gap = 1e-5 * tnorm;
+    for (int k = 0; k < nvec; ++k)
+      if (k == 0 || lam[k] - lam[k - 1] > gap) W.clus[nc++] = k;
+    W.clus[nc] = nvec;
+    W.misc[0] = nc;
+  }
+  __syncthreads();
+  const int ncl = W.misc[0];
+  const double tiny = DBL_EPSILON * fmax(tnorm, DBL_MIN);
+  for (int cl = tid; cl < ncl; cl += nthr) {
+    double* u0 = scratch + cl;
+    double* u1 = u0 + (size_t)n * ncl;
+    double* u2 = u1 + (size_t)n * ncl;
+    double* x = u2 + (size_t)n * ncl;
+    auto X = [&](int i) -> double& { return x[(size_t)i * ncl]; };
+    for (int k = W.clus[cl]; k < W.clus[cl + 1]; ++k) {
+      for (int i = 0; i < n; ++i) X(i) = hash_uniform((seed << 20) + k, i);
+      for (int iter = 0; iter < kTriInvIters; ++iter) {
+        tri_solve(d, e, n, lam[k], tiny, x, u0, u1, u2, ncl);
+        for (int kp = W.clus[cl]; kp < k; ++kp) {
+          const double2* zp = z + (size_t)kp * n;
+          double s = 0.0;
+          for (int i = 0; i < n; ++i) s += zp[i].x * X(i);
+          for (int i = 0; i < n; ++i) X(i) -= s * zp[i].x;
+        }
+        double s = 0.0, mx = 0.0;
+        for (int i = 0; i < n; ++i) mx = fmax(mx, fabs(X(i)));
+        if (!(mx > 0.0) || !isfinite(mx)) mx = 1.0;
+        for (int i = 0; i < n; ++i) {
+          X(i) /= mx;
+          s += X(i) * X(i);
+        }
+        s = 1.0 / sqrt(s);
+        for (int i = 0; i < n; ++i) X(i) *= s;
+      }
+      double2* zk = z + (size_t)k * n;
+      for (int i = 0; i < n; ++i) zk[i] = make_double2(X(i), 0.0);
+    }
+  }
+  __syncthreads();
+}
+
+}  // namespace dev
+}  // namespace pmx

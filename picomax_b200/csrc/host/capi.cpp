@@ -252,7 +252,7 @@ struct pmx_ctx {
   std::map<long long, int> heev_choice;
   std::map<long long, std::vector<float>> heev_trials;
   // named workspaces
-  DevBuf crystal, g, hkl, vloc, vso, items, hbuf, wbuf, zk, zq, scratch, info;
+  DevBuf crystal, g, hkl, vloc, vso, items, hbuf, wbuf, zk, zq, scratch, info, rbuf;
   DevBuf loci, kpts, uvec, ssoc, qgn, ncd, nvd, cbase, vbase, cidx, vidx, blkoff, dest;
   DevBuf M, dE, wgt, f0, trange, acc, accpv, chi, chi2, mixws, epsm, stats;
   // adjoint workspaces
@@ -388,6 +388,37 @@ DevCrystal upload_crystal(pmx_ctx* c, const pmx_problem* P, int force_spinor) {
   return d;
 }
 
+// Eigensolver dispatch. Where the two-stage solver applies (matrices too
+// large for the shared-memory-resident one-stage kernel, padded size <= 416,
+// and no export of the one-stage reduction for the adjoint) it is schedule 0
+// and the one-stage schedules follow; otherwise only the one-stage schedules
+// are offered. A launch's items then carry the padded leading dimension and
+// a slot of the band reflector buffer (ctx rbuf).
+bool use_two_stage(int max_n, bool tri) {
+  return !tri && max_n > pmx::dev::heev_smem_max_n() && pmx::dev::heev2_supported(max_n);
+}
+int eig_variants(int max_n, int max_nval, bool tri) {
+  return (use_two_stage(max_n, tri) ? 1 : 0) + pmx::dev::heev_variants(max_n, max_nval);
+}
+// leading dimension / reflector slot (double2) of an item of size n in a
+// launch whose largest matrix is max_n
+int eig_ld(int n, int max_n, bool tri) { return use_two_stage(max_n, tri) ? pmx::dev::heev2_ld(n) : n; }
+size_t eig_rstride(int n, int max_n, bool tri) {
+  return use_two_stage(max_n, tri) ? pmx::dev::heev2_rbuf_double2(pmx::dev::heev2_ld(n)) : 0;
+}
+cudaError_t eig_launch(pmx_ctx* c, const pmx::dev::EigItem* items, int nitems, int max_n, int max_nval,
+                       int max_nvec, double2* hbuf, double* wbuf, double2* zbuf, double* scratch, int* info,
+                       int variant, double* tri = nullptr) {
+  if (use_two_stage(max_n, tri != nullptr)) {
+    if (variant == 0)
+      return pmx::dev::launch_heev2(items, nitems, max_n, max_nval, max_nvec, hbuf, wbuf, zbuf, scratch,
+                                    c->rbuf.as<double2>(), info, c->stream);
+    variant -= 1;
+  }
+  return pmx::dev::launch_heev(items, nitems, max_n, max_nval, hbuf, wbuf, zbuf, scratch, info, c->stream, variant,
+                               tri);
+}
+
 // Assembles and diagonalises H(k) for every k; the lowest nval eigenvalues
 // go to w (host, [nk][nval]); with zdev the lowest nvec eigenvectors go to
 // zdev ([nk][nvec][n]).
@@ -401,7 +432,9 @@ void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int 
   if (nk == 0) return;
   if (nval > n) throw CudaFail("too many eigenvalues requested", PMX_ERR_INVALID);
   const bool vec = zdev != nullptr && nvec > 0;
-  const size_t hbytes = (size_t)n * n * sizeof(double2);
+  const bool tri_req = tri != nullptr;
+  const int ld = eig_ld(n, n, tri_req);
+  const size_t hbytes = (size_t)ld * ld * sizeof(double2);
   int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)nk, ((size_t)2 << 30) / hbytes));
   chunk = std::min(chunk, 4096);
   if (nk > chunk) {  // several chunks: each a whole number of waves of CTAs
@@ -414,6 +447,8 @@ void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int 
   const bool per_item = vec || n > 832;  // without vectors the scratch holds only the large-n partial sums
   CK(c->scratch.ensure(sizeof(double) * sstride * (per_item ? chunk : 1)));
   CK(c->info.ensure(sizeof(int) * chunk));
+  const size_t rstride = eig_rstride(n, n, tri_req);
+  if (rstride) CK(c->rbuf.ensure(sizeof(double2) * rstride * chunk));
   std::vector<pmx::dev::EigItem> items(chunk);
   std::vector<int> info(chunk);
   for (int k0 = 0; k0 < nk; k0 += chunk) {
@@ -427,10 +462,12 @@ void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int 
       it.nval = nval;
       it.want_vec = vec ? 1 : 0;
       for (int x = 0; x < 3; ++x) it.k[x] = ks[k0 + i][x];
-      it.h_off = (long long)i * n * n;
+      it.h_off = (long long)i * ld * ld;
       it.w_off = (long long)(k0 + i) * nval;
       it.z_off = (long long)(k0 + i) * nvec * n;
       it.s_off = per_item ? (long long)(i * sstride) : 0;
+      it.ld = ld;
+      it.r_off = (long long)(i * rstride);
     }
     h2d(c, c->items, items.data(), sizeof(pmx::dev::EigItem) * cnt);
     {
@@ -443,7 +480,7 @@ void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int 
     // last so the results come from it)
     const long long key = ((long long)n * 1024 + nval) * 2 + (vec ? 1 : 0);
     int variant = 0;
-    const int nvar = pmx::dev::heev_variants(n, nval);
+    const int nvar = eig_variants(n, nval, tri_req);
     auto it_choice = c->heev_choice.find(key);
     if (c->fixed_schedule >= 0) {
       variant = std::min(c->fixed_schedule, nvar - 1);
@@ -453,9 +490,9 @@ void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int 
       std::vector<float> ms(nvar, 0.f);
       for (int v = 0; v < nvar; ++v) {
         CK(cudaEventRecord(c->ev[2], c->stream));
-        CK(pmx::dev::launch_heev(c->items.as<pmx::dev::EigItem>(), cnt, n, nval, c->hbuf.as<double2>(),
-                                 c->wbuf.as<double>(), vec ? zdev : c->hbuf.as<double2>(), c->scratch.as<double>(),
-                                 c->info.as<int>(), c->stream, v));
+        CK(eig_launch(c, c->items.as<pmx::dev::EigItem>(), cnt, n, nval, vec ? nvec : 0, c->hbuf.as<double2>(),
+                      c->wbuf.as<double>(), vec ? zdev : c->hbuf.as<double2>(), c->scratch.as<double>(),
+                      c->info.as<int>(), v));
         CK(cudaEventRecord(c->ev[3], c->stream));
         CK(cudaEventSynchronize(c->ev[3]));
         CK(cudaEventElapsedTime(&ms[v], c->ev[2], c->ev[3]));
@@ -471,9 +508,9 @@ void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int 
     }
     {
       KTime kt(c, "heev");
-      CK(pmx::dev::launch_heev(c->items.as<pmx::dev::EigItem>(), cnt, n, nval, c->hbuf.as<double2>(),
-                               c->wbuf.as<double>(), vec ? zdev : c->hbuf.as<double2>(), c->scratch.as<double>(),
-                               c->info.as<int>(), c->stream, variant, tri ? tri + (size_t)k0 * 4 * n : nullptr));
+      CK(eig_launch(c, c->items.as<pmx::dev::EigItem>(), cnt, n, nval, vec ? nvec : 0, c->hbuf.as<double2>(),
+                    c->wbuf.as<double>(), vec ? zdev : c->hbuf.as<double2>(), c->scratch.as<double>(),
+                    c->info.as<int>(), variant, tri ? tri + (size_t)k0 * 4 * n : nullptr));
     }
     c->launches += 2;
     CK(cudaMemcpyAsync(info.data(), c->info.ptr, sizeof(int) * cnt, cudaMemcpyDeviceToHost, c->stream));
@@ -586,8 +623,11 @@ extern "C" int pmx_hamiltonian(pmx_ctx* ctx, const pmx_problem* P, const double*
 extern "C" int pmx_heev_batched(pmx_ctx* ctx, int n, int batch, const double* A, int nev, double* w, double* z) {
   if (n <= 0 || batch < 0 || nev <= 0 || nev > n || (batch > 0 && (!A || !w))) return PMX_ERR_INVALID;
   return guarded(ctx, [&]() {
-    const size_t hb = sizeof(double2) * (size_t)n * n;
+    const int ld = eig_ld(n, n, false);
+    const size_t hb = sizeof(double2) * (size_t)ld * ld;
     CK(ctx->hbuf.ensure(std::max<size_t>(hb * batch, 16)));
+    const size_t rstride = eig_rstride(n, n, false);
+    if (rstride) CK(ctx->rbuf.ensure(sizeof(double2) * rstride * std::max(batch, 1)));
     CK(ctx->wbuf.ensure(std::max<size_t>(sizeof(double) * (size_t)batch * nev, 16)));
     CK(ctx->zk.ensure(std::max<size_t>(sizeof(double2) * (size_t)batch * nev * n, 16)));
     const size_t sstride = pmx::dev::heev_scratch_doubles(n, z ? nev : 0, n);
@@ -600,19 +640,29 @@ extern "C" int pmx_heev_batched(pmx_ctx* ctx, int n, int batch, const double* A,
       items[i].nev = z ? nev : 0;
       items[i].nval = nev;
       items[i].want_vec = z ? 1 : 0;
-      items[i].h_off = (long long)i * n * n;
+      items[i].h_off = (long long)i * ld * ld;
       items[i].w_off = (long long)i * nev;
       items[i].z_off = (long long)i * nev * n;
       items[i].s_off = (long long)(i * sstride);
+      items[i].ld = ld;
+      items[i].r_off = (long long)(i * rstride);
     }
     if (batch == 0) return (int)PMX_OK;
-    CK(cudaMemcpyAsync(ctx->hbuf.ptr, A, hb * batch, cudaMemcpyHostToDevice, ctx->stream));
+    if (ld == n) {
+      CK(cudaMemcpyAsync(ctx->hbuf.ptr, A, hb * batch, cudaMemcpyHostToDevice, ctx->stream));
+    } else {  // columns of n into the zero-padded ld x ld layout
+      CK(cudaMemsetAsync(ctx->hbuf.ptr, 0, hb * batch, ctx->stream));
+      for (int i = 0; i < batch; ++i)
+        CK(cudaMemcpy2DAsync(ctx->hbuf.as<double2>() + (size_t)i * ld * ld, sizeof(double2) * ld,
+                             A + (size_t)2 * i * n * n, sizeof(double2) * n, sizeof(double2) * n, n,
+                             cudaMemcpyHostToDevice, ctx->stream));
+    }
     h2d(ctx, ctx->items, items.data(), sizeof(pmx::dev::EigItem) * batch);
     {
       KTime kt(ctx, "heev");
-      CK(pmx::dev::launch_heev(ctx->items.as<pmx::dev::EigItem>(), batch, n, nev, ctx->hbuf.as<double2>(),
-                               ctx->wbuf.as<double>(), ctx->zk.as<double2>(), ctx->scratch.as<double>(),
-                               ctx->info.as<int>(), ctx->stream, std::max(ctx->fixed_schedule, 0)));
+      CK(eig_launch(ctx, ctx->items.as<pmx::dev::EigItem>(), batch, n, nev, z ? nev : 0, ctx->hbuf.as<double2>(),
+                    ctx->wbuf.as<double>(), ctx->zk.as<double2>(), ctx->scratch.as<double>(), ctx->info.as<int>(),
+                    std::min(std::max(ctx->fixed_schedule, 0), eig_variants(n, nev, false) - 1)));
     }
     ctx->launches += 1;
     std::vector<int> info(batch);
@@ -1979,18 +2029,19 @@ void solve_multi(pmx_ctx* c, const pmx::dev::CrystalDev* table, std::vector<Solv
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return reqs[a].n > reqs[b].n; });
   struct Chunk {
-    int first, cnt, max_n, max_nval, max_npw;
+    int first, cnt, max_n, max_nval, max_npw, max_nvec;
   };
   std::vector<Chunk> chunks;
   std::vector<pmx::dev::EigItem> items(reqs.size());
   const size_t hmax = (size_t)2 << 30;
-  long long w = 0, hneed = 0, sneed = 0;
+  long long w = 0, hneed = 0, sneed = 0, rneed = 0;
   size_t i0 = 0;
   while (i0 < order.size()) {
     const int max_n = reqs[order[i0]].n, cls = heev_class(max_n);
     size_t i1 = i0, hb = 0;
     while (i1 < order.size() && i1 - i0 < 4096 && heev_class(reqs[order[i1]].n) == cls) {
-      const size_t b = (size_t)reqs[order[i1]].n * reqs[order[i1]].n * sizeof(double2);
+      const size_t ldi = (size_t)eig_ld(reqs[order[i1]].n, max_n, false);
+      const size_t b = ldi * ldi * sizeof(double2);
       if (i1 > i0 && hb + b > hmax) break;
       hb += b;
       ++i1;
@@ -2001,8 +2052,8 @@ void solve_multi(pmx_ctx* c, const pmx::dev::CrystalDev* table, std::vector<Solv
       const int unit = pmx::dev::heev_batch_unit(max_n, reqs[order[i0]].nval);
       if ((int)(i1 - i0) >= unit) i1 = i0 + (i1 - i0) / unit * unit;
     }
-    Chunk ch{(int)i0, (int)(i1 - i0), max_n, 1, 1};
-    long long h = 0, sc = 0;
+    Chunk ch{(int)i0, (int)(i1 - i0), max_n, 1, 1, 0};
+    long long h = 0, sc = 0, rb = 0;
     for (size_t i = i0; i < i1; ++i) {
       const SolveReq& r = reqs[order[i]];
       if (r.nval > r.n || r.nvec > r.nval) throw CudaFail("too many eigenvalues requested", PMX_ERR_INVALID);
@@ -2018,7 +2069,11 @@ void solve_multi(pmx_ctx* c, const pmx::dev::CrystalDev* table, std::vector<Solv
       it.w_off = w;   // eigenvalues of all chunks side by side
       it.z_off = r.z_off;
       it.s_off = sc;
-      h += (long long)r.n * r.n;
+      it.ld = eig_ld(r.n, max_n, false);
+      it.r_off = rb;
+      h += (long long)it.ld * it.ld;
+      rb += (long long)eig_rstride(r.n, max_n, false);
+      ch.max_nvec = std::max(ch.max_nvec, r.nvec);
       w += r.nval;
       sc += (long long)pmx::dev::heev_scratch_doubles(r.n, r.nvec, max_n);
       ch.max_nval = std::max(ch.max_nval, r.nval);
@@ -2026,6 +2081,7 @@ void solve_multi(pmx_ctx* c, const pmx::dev::CrystalDev* table, std::vector<Solv
     }
     hneed = std::max(hneed, h);
     sneed = std::max(sneed, sc);
+    rneed = std::max(rneed, rb);
     chunks.push_back(ch);
     i0 = i1;
   }
@@ -2034,6 +2090,7 @@ void solve_multi(pmx_ctx* c, const pmx::dev::CrystalDev* table, std::vector<Solv
   CK(c->wbuf.ensure(sizeof(double) * (size_t)w));
   CK(c->scratch.ensure(sizeof(double) * (size_t)sneed));
   CK(c->info.ensure(sizeof(int) * nitems));
+  if (rneed) CK(c->rbuf.ensure(sizeof(double2) * (size_t)rneed));
   h2d(c, c->items, items.data(), sizeof(pmx::dev::EigItem) * nitems);
   pmx::dev::EigItem* dit = c->items.as<pmx::dev::EigItem>();
   int* dinfo = c->info.as<int>();
@@ -2045,7 +2102,7 @@ void solve_multi(pmx_ctx* c, const pmx::dev::CrystalDev* table, std::vector<Solv
     const Chunk& ch = chunks[ci];
     const bool vec = zbase != nullptr;
     const long long key = ((long long)ch.max_n * 1024 + ch.max_nval) * 2 + (vec ? 1 : 0);
-    const int nvar = pmx::dev::heev_variants(ch.max_n, ch.max_nval);
+    const int nvar = eig_variants(ch.max_n, ch.max_nval, false);
     auto cached = c->heev_choice.find(key);
     if (c->fixed_schedule >= 0) {
       variant[ci] = std::min(c->fixed_schedule, nvar - 1);
@@ -2056,9 +2113,9 @@ void solve_multi(pmx_ctx* c, const pmx::dev::CrystalDev* table, std::vector<Solv
       for (int v = 0; v < nvar; ++v) {
         CK(pmx::dev::launch_assemble(table, dit + ch.first, ch.cnt, ch.max_npw, c->hbuf.as<double2>(), c->stream));
         CK(cudaEventRecord(c->ev[2], c->stream));
-        CK(pmx::dev::launch_heev(dit + ch.first, ch.cnt, ch.max_n, ch.max_nval, c->hbuf.as<double2>(),
-                                 c->wbuf.as<double>(), zbase ? zbase : c->hbuf.as<double2>(),
-                                 c->scratch.as<double>(), dinfo + ch.first, c->stream, v));
+        CK(eig_launch(c, dit + ch.first, ch.cnt, ch.max_n, ch.max_nval, zbase ? ch.max_nvec : 0,
+                      c->hbuf.as<double2>(), c->wbuf.as<double>(), zbase ? zbase : c->hbuf.as<double2>(),
+                      c->scratch.as<double>(), dinfo + ch.first, v));
         CK(cudaEventRecord(c->ev[3], c->stream));
         CK(cudaEventSynchronize(c->ev[3]));
         CK(cudaEventElapsedTime(&ms[v], c->ev[2], c->ev[3]));
@@ -2077,9 +2134,9 @@ void solve_multi(pmx_ctx* c, const pmx::dev::CrystalDev* table, std::vector<Solv
     const Chunk& ch = chunks[ci];
     cap = pmx::dev::launch_assemble(table, dit + ch.first, ch.cnt, ch.max_npw, c->hbuf.as<double2>(), c->stream);
     if (cap != cudaSuccess) break;
-    cap = pmx::dev::launch_heev(dit + ch.first, ch.cnt, ch.max_n, ch.max_nval, c->hbuf.as<double2>(),
-                                c->wbuf.as<double>(), zbase ? zbase : c->hbuf.as<double2>(), c->scratch.as<double>(),
-                                dinfo + ch.first, c->stream, variant[ci]);
+    cap = eig_launch(c, dit + ch.first, ch.cnt, ch.max_n, ch.max_nval, zbase ? ch.max_nvec : 0,
+                     c->hbuf.as<double2>(), c->wbuf.as<double>(), zbase ? zbase : c->hbuf.as<double2>(),
+                     c->scratch.as<double>(), dinfo + ch.first, variant[ci]);
     if (cap != cudaSuccess) break;
   }
   const cudaError_t end = cudaStreamEndCapture(c->stream, &graph);
