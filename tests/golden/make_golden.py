@@ -79,7 +79,87 @@ CASES = {
 }
 
 
-def run_case(name, binary, argv, grid, tmp):
+def _strip_kfile(argv):
+    """argv without -kpoint / -kpointfile (the fixture carries its k list)."""
+    out, i = [], 0
+    while i < len(argv):
+        if argv[i] in ("-kpoint", "-kpointfile"):
+            i += 2
+            continue
+        out.append(argv[i])
+        i += 1
+    return out
+
+
+def _subset(K, count, skip=None):
+    """`count` points of the grid K taken at an even stride (deterministic),
+    leaving out the points `skip` rejects."""
+    idx = [i for i in range(len(K)) if skip is None or not skip(K[i])]
+    step = max(1, len(idx) // count)
+    return K[np.array(idx[::step][:count])]
+
+
+def _on_gamma_l(k):
+    """k on the Gamma-L line (|kx| = |ky| = |kz| != 0): NBAND 16 of Si cuts the
+    Lambda_3 pair there, and chi then depends on the eigensolver's basis."""
+    a = np.abs(k)
+    return a[0] > 1e-9 and abs(a[0] - a[1]) < 1e-9 and abs(a[0] - a[2]) < 1e-9
+
+
+def _is_gamma(k):
+    """Gamma: with the wurtzite seed the states nvalence-1 and nvalence are
+    degenerate there, so E_ref sits on both and their occupation is decided by
+    rounding (no implementation can reproduce another's)."""
+    return bool(np.all(np.abs(k) < 1e-12))
+
+
+def config_cases():
+    """The benchmark configurations at their own shape (encut / N_G, NEPS,
+    frequencies, broadening, SOC, preset, form-factor seeds) on a subset of
+    each configuration's own Gamma-centred k grid, sized so that the
+    reference finishes in seconds to a few minutes."""
+    from picomax_b200.workloads import workload
+    with tempfile.TemporaryDirectory() as tmp:
+        si, _, _ = workload("si_epsLL", tmp)
+        ga, _, _ = workload("gaas_epsij", tmp)
+        wz, _, _ = workload("wz_epsLL", tmp)
+        teb, _, _ = workload("te_band", tmp)
+        tel, _, _ = workload("te_epsLL", tmp)
+    Ksi, _ = gamma_grid("zb", 8, 8, 8)
+    Kga, _ = gamma_grid("zb", 16, 16, 16)
+    Kwz, _ = gamma_grid("wz", 24, 24, 16, 1.626)
+    Kte, _ = gamma_grid("te", 10, 10, 8, 1.33)
+    return {
+        # config 1: Si epsLL, N_G 113, NEPS 15, 1000 w, Gaussian 0.1 eV, KK
+        "cfg1_si_epsLL": ("picomax_ref_ll", _strip_kfile(si), ("list", _subset(Ksi, 32, _on_gamma_l))),
+        # config 2: GaAs + SOC epsij, n 274, NEPS 27, 2000 w, Lorentzian 0.05 eV, KK;
+        # 128 k-points give > 2048 transitions per 256-wide frequency tile, so
+        # the mixed path's periodic FP64 flush of the TMEM accumulator runs
+        "cfg2_gaas_epsij": ("picomax_ref_guard", _strip_kfile(ga), ("list", _subset(Kga, 128))),
+        # config 3: wurtzite epsLL, N_G 401, NEPS 59, 2000 w, Gaussian 0.1 eV, KK
+        "cfg3_wz_epsLL": ("picomax_ref_ll", _strip_kfile(wz), ("list", _subset(Kwz, 4, _is_gamma))),
+        # config 5: trigonal Te + SOC (n 570): 121-point band path and epsLL
+        "cfg5_te_band": ("picomax_ref", teb, None),
+        "cfg5_te_epsLL": ("picomax_ref_ll", _strip_kfile(tel), ("list", _subset(Kte, 16))),
+    }
+
+
+def _reduce_chi(dat, argv, nk_rows=None):
+    """Fixture form of a large chi .dat ([re|im][3][3][nq][pairs][nf]): every
+    row (re/im, i, j, q, pair) at a stride of frequencies, the rows of the
+    first three pairs ((0,0), (1,0), (1,1): the head and its neighbours) at
+    every frequency, every row's sum over frequencies, and max |value|."""
+    neps = int(argv[argv.index("-neps") + 1])
+    nf = int(argv[argv.index("-nfreq") + 1])
+    npairs = neps * (neps + 1) // 2
+    rows = dat.reshape(-1, npairs, nf)
+    fstride = max(1, (rows.shape[0] * npairs * nf) // 150000)
+    fsel = np.arange(0, nf, fstride)
+    return {"dat_absmax": np.abs(dat).max(), "dat_size": np.int64(dat.size), "fsel": fsel,
+            "dat_fsel": rows[:, :, fsel], "dat_head": rows[:, :3, :], "dat_rowsum": rows.sum(axis=2)}
+
+
+def run_case(name, binary, argv, grid, tmp, reduce=False):
     args = list(argv)
     K = None
     if grid is not None and grid[0] == "list":
@@ -101,10 +181,14 @@ def run_case(name, binary, argv, grid, tmp):
     dt = time.time() - t0
     if r.returncode != 0:
         raise RuntimeError(f"{name}: reference exited {r.returncode}\n{r.stdout[-2000:]}")
-    out = {"argv": np.array(argv), "binary": binary, "seconds": dt,
-           "dat": np.fromfile(os.path.join(tmp, name + ".dat"), np.float64)}
+    dat = np.fromfile(os.path.join(tmp, name + ".dat"), np.float64)
+    out = {"argv": np.array(argv), "binary": binary, "seconds": dt}
+    if reduce and "-neps" in argv:
+        out.update(_reduce_chi(dat, argv))
+    else:
+        out["dat"] = dat
     gpt = os.path.join(tmp, name + ".gpt")
-    if os.path.exists(gpt):
+    if os.path.exists(gpt) and not reduce:
         out["gpt"] = np.fromfile(gpt, np.float64)
     if K is not None:
         out["kpts"] = K
@@ -112,7 +196,7 @@ def run_case(name, binary, argv, grid, tmp):
             out["kgrid"] = np.array(grid[1:], np.int64)
             out["kcrystal"] = grid[0]
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
-    print(f"{name}: {out['dat'].size} values, {dt:.2f} s")
+    print(f"{name}: {dat.size} values, {dt:.2f} s")
 
 
 # -debug 3 dumps: the reference prints its G list, k list and q list
@@ -154,6 +238,10 @@ def main(names=None):
             if names and name not in names:
                 continue
             run_case(name, binary, argv, grid, tmp)
+        # configuration-shape cases only when named (minutes of host time)
+        for name, (binary, argv, grid) in config_cases().items():
+            if names and name in names:
+                run_case(name, binary, argv, grid, tmp, reduce=True)
     for name, argv in DUMPS.items():
         if names and name not in names:
             continue
