@@ -674,11 +674,16 @@ __global__ void __launch_bounds__(kS2Thr, 1) sbtrd_kernel(const EigItem* __restr
 }
 
 // --------------------------------------------------------- tridiagonal stage
+// 256 threads per matrix (one CTA): multisection bisection probes 256 / nval
+// points per eigenvalue at once; the inverse iteration runs one thread per
+// eigenvalue cluster (128-thread CTAs measured slower: 1.29 vs 1.16 ms)
+constexpr int kTriThr = 256;
+
 __host__ __device__ inline size_t tri_smem_bytes(int n, int nval, int nvec) {
-  return sizeof(double) * ((size_t)3 * n + 8 + 3 * nval + kThr) + sizeof(int) * ((size_t)kThr + nvec + 1 + 4);
+  return sizeof(double) * ((size_t)3 * n + 8 + 3 * nval + kTriThr) + sizeof(int) * ((size_t)kTriThr + nvec + 1 + 4);
 }
 
-__global__ void __launch_bounds__(kThr) tri_eig_kernel(const EigItem* __restrict__ items,
+__global__ void __launch_bounds__(kTriThr) tri_eig_kernel(const EigItem* __restrict__ items,
                                                      const double2* __restrict__ rbuf, double* __restrict__ wbuf,
                                                      double2* __restrict__ zbuf, double* __restrict__ scratch,
                                                      int* __restrict__ info) {
@@ -694,11 +699,11 @@ __global__ void __launch_bounds__(kThr) tri_eig_kernel(const EigItem* __restrict
   double* lo = lam + nval;
   double* hi = lo + nval;
   double* xs = hi + nval;
-  int* cnt = reinterpret_cast<int*>(xs + kThr);
-  int* clus = cnt + kThr;
+  int* cnt = reinterpret_cast<int*>(xs + kTriThr);
+  int* clus = cnt + kTriThr;
   int* misc = clus + nvec + 1;
   const double* de = reinterpret_cast<const double*>(rbuf + it.r_off + ceil_sum(ld - 1) * kNB);
-  for (int c = tid; c < n; c += kThr) {
+  for (int c = tid; c < n; c += kTriThr) {
     d[c] = de[c];
     e[c] = c + 1 < n ? de[ld + c] : 0.0;
   }
@@ -710,22 +715,23 @@ __global__ void __launch_bounds__(kThr) tri_eig_kernel(const EigItem* __restrict
 }
 
 // ----------------------------------------------------------- back-transform
-constexpr int kChunk = 64;  // panel rows per staged chunk of the stage-1 back-transform
+constexpr int kChunk = 32;  // panel rows per staged chunk of the stage-1 back-transform
 
 __host__ __device__ inline size_t back_smem_bytes(int ld, int vb) {
   // Z [ld][vb], one sweep's reflectors [2][ceil(ld/16)][16], panel chunks
-  // [2][64][16], W [16][vb], T [16][17]
+  // [2][kChunk][16], W [16][vb], T [16][17]
   return sizeof(double2) *
          ((size_t)ld * vb + 2 * ((ld + kNB - 1) / kNB) * kNB + 2 * kChunk * kNB + kNB * vb + kNB * 17);
 }
-// eigenvectors per back-transform CTA: up to kVecBlock, as many as fit
+// eigenvectors per back-transform CTA: up to kVecBlock, and few enough that
+// two CTAs share an SM (the stage is latency-bound)
 inline int back_vec_block(int ld, int max_nvec) {
   int vb = std::min(kVecBlock, std::max(max_nvec, 1));
-  while (vb > 1 && back_smem_bytes(ld, vb) > (size_t)227 * 1024) --vb;
+  while (vb > 1 && back_smem_bytes(ld, vb) > (size_t)112 * 1024) --vb;
   return vb;
 }
 
-__global__ void __launch_bounds__(kThr) eig2_back_kernel(const EigItem* __restrict__ items,
+__global__ void __launch_bounds__(kThr, 2) eig2_back_kernel(const EigItem* __restrict__ items,
                                                        const double2* __restrict__ hbuf,
                                                        const double2* __restrict__ rbuf, double2* __restrict__ zbuf,
                                                        const int* __restrict__ info, int vb) {
@@ -913,7 +919,7 @@ cudaError_t launch_heev2(const EigItem* items, int nitems, int max_n, int max_nv
   const size_t s3 = tri_smem_bytes(max_n, max_nval, max_nvec);
   e = cudaFuncSetAttribute(tri_eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s3);
   if (e != cudaSuccess) return e;
-  tri_eig_kernel<<<nitems, kThr, s3, st>>>(items, rbuf, wbuf, zbuf, scratch, info);
+  tri_eig_kernel<<<nitems, kTriThr, s3, st>>>(items, rbuf, wbuf, zbuf, scratch, info);
   if (max_nvec > 0) {
     const int vb = back_vec_block(ld, max_nvec);
     const size_t s4 = back_smem_bytes(ld, vb);
