@@ -93,6 +93,21 @@ int pmx_problem_write_gpt(const pmx_problem* p);
 
 /* ---------------------------------------------------------------- context */
 
+/* Limit in nanoseconds of every bounded mbarrier wait of the mixed-precision
+ * contraction (0: 2 s). A wait that runs out makes its CTA record the error,
+ * wait for its own copies and MMAs in flight, free its tensor memory and
+ * return; the call then fails with PMX_ERR_TIMEOUT and the context stays
+ * usable. No reference counterpart (the reference has no device waits). */
+int pmx_ctx_set_wait_limit(pmx_ctx* ctx, long long ns);
+
+/* Test hooks, no reference counterpart: fault 1 makes the producer warps of
+ * the mixed contraction withhold their first A-full arrival, so that the
+ * control warp's bounded wait runs out and the timeout path above runs
+ * (combine with a short pmx_ctx_set_wait_limit); fault 2 stops the
+ * eigensolver's bisection after one round, so that its status reports
+ * non-convergence (PMX_ERR_NOCONV). 0 restores normal operation. */
+int pmx_ctx_set_fault(pmx_ctx* ctx, int fault);
+
 int pmx_ctx_create(int device, pmx_ctx** out);
 void pmx_ctx_destroy(pmx_ctx* ctx);
 /* Message of the last failing call on this context (NUL-terminated). */
@@ -172,9 +187,12 @@ int pmx_heev_batched(pmx_ctx* ctx, int n, int batch, const double* A, int nev, d
  * when z is given). batch > 1024, n > 832, or 32 n nev batch bytes above
  * 16 MiB - 80 KiB (with z) return PMX_ERR_LIMIT. The first call on a device
  * looks the array up (set-up, once per device): make that first call before
- * any stream capture. Every call on a device shares the array and rewrites
- * what it reads; calls that overlap on the GPU (different streams or threads)
- * race on it. No counterpart in the reference (added entry point). */
+ * any stream capture. The address found then is kept for the life of the
+ * process, so do not call this entry point again after cudaDeviceReset on
+ * that device (the reset makes a new context and the kept address stale).
+ * Every call on a device shares the array and rewrites what it reads; calls
+ * that overlap on the GPU (different streams or threads) race on it. No
+ * counterpart in the reference (added entry point). */
 int pmx_heev_batched_noalloc(void* stream, int n, int batch, double* A, int nev, double* w, double* z, int* info);
 
 /* Energy reference: midpoint of eigenvalues nvalence-1 and nvalence at

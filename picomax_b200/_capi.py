@@ -43,7 +43,7 @@ EXPORTS = (
     "pmx_problem_params",
     "pmx_problem_set_params",
     "pmx_band_vjp",
-    "pmx_epsm_vjp",
+    "pmx_epsm_vjp", "pmx_ctx_set_wait_limit", "pmx_ctx_set_fault",
     "pmx_band_batch",
     "pmx_chi_batch",
     "pmx_ctx_occupation_ties",
@@ -117,6 +117,8 @@ def load() -> ctypes.CDLL:
         "pmx_problem_set_params": (c_int, [c_void_p, dp, c_int]),
         "pmx_band_vjp": (c_int, [c_void_p, c_void_p, dp, dp]),
         "pmx_epsm_vjp": (c_int, [c_void_p, c_void_p, dp, dp, dp, dp]),
+        "pmx_ctx_set_wait_limit": (c_int, [c_void_p, c_longlong]),
+        "pmx_ctx_set_fault": (c_int, [c_void_p, c_int]),
         "pmx_band_batch": (c_int, [c_void_p, c_int, POINTER(c_void_p), POINTER(dp)]),
         "pmx_chi_batch": (c_int, [c_void_p, c_int, POINTER(c_void_p), c_int, c_int, POINTER(dp), POINTER(dp),
                                   POINTER(dp)]),
@@ -314,6 +316,14 @@ class Context:
         v = c_longlong()
         self._check(self._lib.pmx_ctx_mixed_mmas(self.handle, ctypes.byref(v)), "mixed_mmas")
         return int(v.value)
+
+    def set_wait_limit(self, ns: int):
+        """Limit (ns) of the mixed contraction's bounded device waits (0: 2 s)."""
+        self._check(self._lib.pmx_ctx_set_wait_limit(self.handle, int(ns)), "set_wait_limit")
+
+    def set_fault(self, fault: int):
+        """Test hook: 1 = the mixed contraction's producers withhold one arrival (its wait runs out)."""
+        self._check(self._lib.pmx_ctx_set_fault(self.handle, int(fault)), "set_fault")
 
     def set_schedule(self, schedule: int):
         """Fix the eigensolver schedule for later batches (-1: autotuner)."""

@@ -709,7 +709,7 @@ __global__ void __launch_bounds__(kTriThr) tri_eig_kernel(const EigItem* __restr
   }
   __syncthreads();
   const TriWork tw{d, e, e2, red, lam, lo, hi, xs, cnt, clus, misc};
-  const int status = tri_eigvals(tw, n, nval, wbuf + it.w_off);
+  const int status = tri_eigvals(tw, n, nval, wbuf + it.w_off, it.bisect_cap);
   if (nvec > 0 && status == 0) tri_eigvecs(tw, n, nvec, zbuf + it.z_off, scratch + it.s_off, blockIdx.x);
   if (tid == 0) info[blockIdx.x] = status;
 }

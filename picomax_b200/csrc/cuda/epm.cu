@@ -436,7 +436,7 @@ __global__ void __launch_bounds__(kHeevThreads, OCC > 0 ? OCC : ((RING >= 2 || M
 
   // ------------------------------------------------------------- eigenvalues
   const TriWork tw{d, e, e2, red, lam, lo, hi, xs, cnt, clus, misc};
-  const int status = tri_eigvals(tw, n, nev, wbuf + it.w_off);
+  const int status = tri_eigvals(tw, n, nev, wbuf + it.w_off, it.bisect_cap);
   if (tri_out) {
     // H = Q T Q^H for the adjoint: T (d, e after deflation), the reflector
     // scalars tau, and (resident path) the reflectors back into hbuf

@@ -25,7 +25,7 @@
 //              arrive on the stage's A-full mbarrier; warps 0-3 move the FP32
 //              accumulator to the FP64 tile after every 64 chunks.
 // Every mbarrier wait is bounded; on expiry the CTA records an error code,
-// drains its own MMAs (bounded), frees its TMEM and returns. The producers
+// drains its own MMAs and W copies (bounded), frees its TMEM and returns. The producers
 // leave their loop together: the decision is an OR over a named barrier.
 #include <cuda_bf16.h>
 
@@ -52,7 +52,7 @@ constexpr int kThreads = kProducers + 32;    // + the control warp (W copies, MM
 constexpr int kFlushChunks = 64;  // chunks (2048 transitions) per FP32 accumulation before the FP64 flush
 constexpr int kTargetCtas = 4 * 148;  // K-split so that the grid covers the SMs a few times
 constexpr unsigned kWaitLimit = 1u << 26;
-constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s
+constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s, unless the caller sets a limit
 
 // canonical K-major, no-swizzle layout: core matrices of 8 rows x 16 bytes;
 // rows of a core matrix 16 B apart, row groups SBO = 128 B apart, 8-element
@@ -88,13 +88,13 @@ __device__ __forceinline__ uint64_t global_ns() {
   return t;
 }
 
-// Bounded wait on an mbarrier phase: gives up after kWaitNs nanoseconds (a
+// Bounded wait on an mbarrier phase: gives up after limit_ns nanoseconds (a
 // healthy wait takes microseconds) or kWaitLimit polls, whichever is first.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
   const uint32_t a = smem_u32(bar);
   const uint64_t t0 = global_ns();
   for (unsigned it = 0; it < kWaitLimit; ++it) {
-    if ((it & 1023u) == 1023u && global_ns() - t0 > kWaitNs) return false;
+    if ((it & 63u) == 63u && global_ns() - t0 > limit_ns) return false;
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -207,6 +207,8 @@ struct Plan {
   uint8_t* wbuf;     // [nchunk][32 KB]
   double* part;      // [nitem][ntile] FP64 partial tiles of 128 x 256, see part_index
   int* err;          // error flag
+  uint64_t wait_ns;  // limit of every bounded wait
+  int fault;         // tests only: 1 = the producers withhold their first A-full arrival
 };
 
 // Layout of a 128 x 256 partial tile: four 32-row blocks (one per TMEM lane
@@ -312,7 +314,7 @@ __global__ void __launch_bounds__(kThreads, 2) mixed_kernel(Plan pl, ContractArg
   // a bounded wait that gives up at once when the CTA already aborted
   auto wait = [&](uint64_t* bar, uint32_t parity, int code) {
     if (*(volatile int*)s_abort) return false;
-    if (mbar_wait(bar, parity)) return true;
+    if (mbar_wait(bar, parity, pl.wait_ns)) return true;
     atomicExch(pl.err, code);
     *(volatile int*)s_abort = 1;
     return false;
@@ -321,11 +323,17 @@ __global__ void __launch_bounds__(kThreads, 2) mixed_kernel(Plan pl, ContractArg
   if (wid == kProducers / 32) {
     // ------------------------------------------------------------ control
     if (lane == 0) {
-      for (int n = 0; n < 2 && n < nch; ++n)
+      // W chunks whose bulk copy was issued / has landed: on an abort the
+      // copies still in flight are waited for before the CTA frees anything
+      int issued = -1, landed = -1;
+      for (int n = 0; n < 2 && n < nch; ++n) {
         bulk_load(stage(n) + 2 * kABytes, pl.wbuf + (size_t)(c_begin + n) * kWChunkBytes, kWChunkBytes, &wfull[n]);
+        issued = n;
+      }
       for (int n = 0; n < nch; ++n) {
         const int s = n & 1, g = n % kFlushChunks;
         if (!wait(&afull[s], (n >> 1) & 1, 5) || !wait(&wfull[s], (n >> 1) & 1, 2)) break;
+        landed = n;
         tc_fence_after();
         const uint32_t sa = smem_u32(stage(s));
         const uint32_t sb = sa + 2 * kABytes;
@@ -349,8 +357,16 @@ __global__ void __launch_bounds__(kThreads, 2) mixed_kernel(Plan pl, ContractArg
           if (!wait(&mdone[s ^ 1], ((n - 1) >> 1) & 1, 1)) break;
           bulk_load(stage(s ^ 1) + 2 * kABytes, pl.wbuf + (size_t)(c_begin + n + 1) * kWChunkBytes, kWChunkBytes,
                     &wfull[s ^ 1]);
+          issued = n + 1;
         }
       }
+      // drain (after an abort): every issued W copy lands before the stages
+      // are released; chunk c completes phase (c >> 1) & 1 of wfull[c & 1]
+      for (int c = landed + 1; c <= issued; ++c)
+        if (!mbar_wait(&wfull[c & 1], (c >> 1) & 1, pl.wait_ns)) {
+          atomicExch(pl.err, 6);
+          break;
+        }
     }
     __syncwarp();
   } else {
@@ -466,7 +482,7 @@ __global__ void __launch_bounds__(kThreads, 2) mixed_kernel(Plan pl, ContractArg
         *reinterpret_cast<uint4*>(st + kABytes + o2) = l2;
       }
       async_proxy_fence();
-      mbar_arrive(&afull[s]);
+      if (!(pl.fault == 1 && n == 0)) mbar_arrive(&afull[s]);
       // warps 0-3 (TMEM lanes 0-127) move the FP32 accumulator into the FP64
       // tile after the group's last chunk: 32 columns at a time through this
       // warp's 8 KB of the stage of chunk n (free until chunk n + 2, which
@@ -522,7 +538,8 @@ __global__ void __launch_bounds__(kThreads, 2) mixed_kernel(Plan pl, ContractArg
   // drain: the last commit completes after every earlier MMA of the control
   // thread; it is waited for on every path before TMEM is freed
   const int nlast = *(volatile int*)s_last;
-  if (tid == kProducers && nlast >= 0 && !mbar_wait(&mdone[nlast & 1], (nlast >> 1) & 1)) atomicExch(pl.err, 3);
+  if (tid == kProducers && nlast >= 0 && !mbar_wait(&mdone[nlast & 1], (nlast >> 1) & 1, pl.wait_ns))
+    atomicExch(pl.err, 3);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -721,6 +738,8 @@ cudaError_t launch_contract_mixed(const ContractArgs& a, long long T, void* ws, 
   pl.wbuf = take((size_t)kWChunkBytes * std::max(1, pl.nchunk));
   pl.part = reinterpret_cast<double*>(take(sizeof(double) * (size_t)std::max(1, pl.nitem) * pl.ntile * kM * kN));
   pl.err = reinterpret_cast<int*>(take(sizeof(int) * 4));
+  pl.wait_ns = a.wait_ns > 0 ? (uint64_t)a.wait_ns : kWaitNs;
+  pl.fault = a.fault;
   float2* M32 = reinterpret_cast<float2*>(take(sizeof(float2) * (size_t)(T + 1) * A * a.nch));
   if ((size_t)(p - reinterpret_cast<uint8_t*>(ws)) > mixed_workspace_bytes(a, T)) return cudaErrorInvalidValue;
   cudaError_t e;

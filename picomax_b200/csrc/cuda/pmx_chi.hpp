@@ -52,6 +52,9 @@ struct ContractArgs {
   double* acc_pv;       // principal-value accumulators (epsLL, kk = 0) or null
   double* stats;        // mixed path only, optional (device, 2 doubles): max ||M32|^2 - |M|^2|, max |M|^2
   int pvclass;          // principal-value function: 0 by (i, j) block (epsLL), 3 = 1/dE/(dE^2-w^2) for all (epsxyz)
+  long long wait_ns;    // mixed path: limit of every bounded mbarrier wait (0: 2 s)
+  int fault;            // mixed path, tests only: 1 = the producers withhold their first A-full arrival,
+                        // so that the control thread's wait runs out (the timeout path is exercised)
 };
 
 struct ScaleArgs {

@@ -41,7 +41,8 @@ struct EigItem {
   long long s_off;    // double offset of the item's scratch (heev_scratch_doubles)
   int ld;             // leading dimension of the matrix (0: n); rows n..ld-1 and columns
                       // n..ld-1 of the workspace are zero when ld > n
-  long long r_off;    // double2 offset of the two-stage path's band reflectors (heev2_reflector_count)
+  long long r_off;    // double2 offset of the two-stage path's band reflectors (heev2_rbuf_double2)
+  int bisect_cap;     // rounds of the eigenvalue bisection at most (0: the default cap; tests set 1)
 };
 
 // Fills H(k) of every item (full Hermitian storage, leading dimension

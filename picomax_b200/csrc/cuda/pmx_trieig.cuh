@@ -52,7 +52,7 @@ struct TriWork {
   double* d;     // [n] diagonal
   double* e;     // [n] off-diagonal (e[n-1] unused); negligible entries are zeroed
   double* e2;    // [n] squares of e
-  double* red;   // [4+] Gershgorin interval, pivmin, |T|
+  double* red;   // [5+] Gershgorin interval, pivmin, |T|, T finite
   double* lam;   // [nval] eigenvalues
   double* lo;    // [nval] bisection brackets
   double* hi;    // [nval]
@@ -65,15 +65,19 @@ struct TriWork {
 // Lowest nval eigenvalues of T into lam[] and wout[]. Returns 0, 1 (bisection
 // did not converge) or 2 (non-finite eigenvalue). Every thread of the block
 // calls it; contains block barriers.
-__device__ inline int tri_eigvals(const TriWork& W, int n, int nval, double* __restrict__ wout) {
+__device__ inline int tri_eigvals(const TriWork& W, int n, int nval, double* __restrict__ wout, int cap = 0) {
+  const int iters = cap > 0 ? cap : kTriBisectIters;
   const int tid = threadIdx.x, nthr = blockDim.x;
   double *d = W.d, *e = W.e, *e2 = W.e2, *red = W.red, *lo = W.lo, *hi = W.hi, *xs = W.xs, *lam = W.lam;
   int* cnt = W.cnt;
-  // Gershgorin interval, pivmin, and negligible off-diagonals set to zero.
+  // Gershgorin interval, pivmin, and negligible off-diagonals set to zero;
+  // a non-finite entry of T (fmin/fmax would skip it) fails the matrix
   if (tid == 0) {
     double glo = d[0], ghi = d[0], emax2 = 0.0, tnorm = 0.0;
+    int fin = 1;
     for (int i = 0; i < n; ++i) {
       const double el = i > 0 ? fabs(e[i - 1]) : 0.0, er = i < n - 1 ? fabs(e[i]) : 0.0;
+      fin &= (isfinite(d[i]) && isfinite(el) && isfinite(er)) ? 1 : 0;
       glo = fmin(glo, d[i] - el - er);
       ghi = fmax(ghi, d[i] + el + er);
       tnorm = fmax(tnorm, fabs(d[i]) + el + er);
@@ -88,9 +92,11 @@ __device__ inline int tri_eigvals(const TriWork& W, int n, int nval, double* __r
     red[1] = ghi + pad;
     red[2] = DBL_MIN * fmax(1.0, emax2);
     red[3] = tnorm;
+    red[4] = fin;
   }
   __syncthreads();
   const double pivmin = red[2];
+  const bool finite_t = red[4] != 0.0;
   for (int k = tid; k < nval; k += nthr) {
     lo[k] = red[0];
     hi[k] = red[1];
@@ -102,7 +108,7 @@ __device__ inline int tri_eigvals(const TriWork& W, int n, int nval, double* __r
   if (nval > nthr) {
     // more eigenvalues than threads: plain bisection, each thread owns the
     // eigenvalues tid, tid + nthr, ...
-    for (int iter = 0; iter < kTriBisectIters; ++iter) {
+    for (int iter = 0; iter < iters; ++iter) {
       int done = 1;
       for (int k = tid; k < nval; k += nthr) {
         double l = lo[k], h = hi[k];
@@ -125,7 +131,7 @@ __device__ inline int tri_eigvals(const TriWork& W, int n, int nval, double* __r
       }
     }
   }
-  for (int iter = 0; iter < kTriBisectIters && !converged && nval <= nthr; ++iter) {
+  for (int iter = 0; iter < iters && !converged && nval <= nthr; ++iter) {
     const int k = tid / G, g = tid % G;
     if (k < nval) {
       const double l = lo[k], h = hi[k];
@@ -165,7 +171,7 @@ __device__ inline int tri_eigvals(const TriWork& W, int n, int nval, double* __r
     finite &= isfinite(lam[k]) ? 1 : 0;
   }
   finite = __syncthreads_and(finite);
-  return !finite ? 2 : (!converged ? 1 : 0);
+  return !(finite && finite_t) ? 2 : (!converged ? 1 : 0);
 }
 
 // Lowest nvec eigenvectors of T (after tri_eigvals) as real vectors in the

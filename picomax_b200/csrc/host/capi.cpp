@@ -249,6 +249,8 @@ struct pmx_ctx {
   // device times measured when it was chosen
   bool autotune = true;
   int fixed_schedule = -1;  // >= 0: this eigensolver schedule on every batch (clamped to the last one)
+  long long wait_ns = 0;    // limit of the mixed contraction's bounded device waits (0: the kernel's 2 s)
+  int fault = 0;            // tests only: fault injected into the mixed contraction (see pmx_ctx_set_fault)
   std::map<long long, int> heev_choice;
   std::map<long long, std::vector<float>> heev_trials;
   // named workspaces
@@ -468,6 +470,7 @@ void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int 
       it.s_off = per_item ? (long long)(i * sstride) : 0;
       it.ld = ld;
       it.r_off = (long long)(i * rstride);
+      it.bisect_cap = c->fault == 2 ? 1 : 0;
     }
     h2d(c, c->items, items.data(), sizeof(pmx::dev::EigItem) * cnt);
     {
@@ -646,6 +649,7 @@ extern "C" int pmx_heev_batched(pmx_ctx* ctx, int n, int batch, const double* A,
       items[i].s_off = (long long)(i * sstride);
       items[i].ld = ld;
       items[i].r_off = (long long)(i * rstride);
+      items[i].bisect_cap = ctx->fault == 2 ? 1 : 0;
     }
     if (batch == 0) return (int)PMX_OK;
     if (ld == n) {
@@ -1122,6 +1126,8 @@ void chi_process_q(pmx_ctx* ctx, const Problem& p, const ChiPlan& pl, const DevC
     ca.acc = ctx->acc.as<double>();
     ca.acc_pv = pv ? ctx->accpv.as<double>() : nullptr;
     ca.pvclass = mode == 2 ? 3 : 0;
+    ca.wait_ns = ctx->wait_ns;
+    ca.fault = ctx->fault;
     if (precision == PMX_PREC_FP64 || pv) {
       KTime kt(ctx, "contract_f64");
       CK(pmx::dev::launch_contract_f64(ca, st));
@@ -1134,7 +1140,10 @@ void chi_process_q(pmx_ctx* ctx, const Problem& p, const ChiPlan& pl, const DevC
       {
         KTime kt(ctx, "contract_mixed");
         long long mm = 0;
-        CK(pmx::dev::launch_contract_mixed(ca, (long long)T.T, ctx->mixws.ptr, nl, st, &mm));
+        const cudaError_t e = pmx::dev::launch_contract_mixed(ca, (long long)T.T, ctx->mixws.ptr, nl, st, &mm);
+        if (e == cudaErrorTimeout)
+          throw CudaFail("mixed contraction: a bounded device wait ran out (the CTAs returned)", PMX_ERR_TIMEOUT);
+        CK(e);
         ctx->mixed_mmas += mm;
       }
       ctx->launches += nl;
@@ -1296,6 +1305,18 @@ extern "C" int pmx_ctx_mixed_mmas(const pmx_ctx* c, long long* mmas) {
 extern "C" int pmx_ctx_set_autotune(pmx_ctx* c, int on) {
   if (!c) return PMX_ERR_INVALID;
   c->autotune = on != 0;
+  return PMX_OK;
+}
+
+extern "C" int pmx_ctx_set_wait_limit(pmx_ctx* c, long long ns) {
+  if (!c || ns < 0) return PMX_ERR_INVALID;
+  c->wait_ns = ns;
+  return PMX_OK;
+}
+
+extern "C" int pmx_ctx_set_fault(pmx_ctx* c, int fault) {
+  if (!c || fault < 0 || fault > 2) return PMX_ERR_INVALID;
+  c->fault = fault;
   return PMX_OK;
 }
 
@@ -2071,6 +2092,7 @@ void solve_multi(pmx_ctx* c, const pmx::dev::CrystalDev* table, std::vector<Solv
       it.s_off = sc;
       it.ld = eig_ld(r.n, max_n, false);
       it.r_off = rb;
+      it.bisect_cap = c->fault == 2 ? 1 : 0;
       h += (long long)it.ld * it.ld;
       rb += (long long)eig_rstride(r.n, max_n, false);
       ch.max_nvec = std::max(ch.max_nvec, r.nvec);

@@ -372,6 +372,10 @@ void generate_loci(Problem& p) {
 
 // ------------------------------------------------------------------- k-points
 // src/pmx_basis.cpp:200-245
+// Reads the kpointfile format of import_kpt (src/pmx_basis.cpp:200-245):
+// total count, listed count, then "kx ky kz w" per point. The reference
+// leaves the points a short or malformed file does not list at k = 0 with
+// weight 0 and divides by a zero total; this build rejects such files.
 void import_kpoints(Problem& p) {
   std::ifstream in(p.kpointfile);
   if (!in.is_open()) fail("cannot open kpointfile '" + p.kpointfile + "'");
@@ -380,20 +384,24 @@ void import_kpoints(Problem& p) {
   while (std::getline(in, line)) {
     if (line.empty() || line[0] == '#') continue;
     if (i == 0) {
-      std::stringstream(line) >> nk0;
+      if (!(std::stringstream(line) >> nk0) || nk0 <= 0) fail("kpointfile: the first line must be the total k count");
       ++i;
     } else if (i == 1) {
-      std::stringstream(line) >> nk;
-      if (nk < 0) fail("negative k-point count in kpointfile");
+      if (!(std::stringstream(line) >> nk) || nk < 0) fail("kpointfile: the second line must be the listed k count");
       p.K.assign(nk, Vec3{});
       p.KW.assign(nk, 0.0);
       ++i;
     } else if (i - 2 < nk) {
-      std::stringstream(line) >> p.K[i - 2].x >> p.K[i - 2].y >> p.K[i - 2].z >> p.KW[i - 2];
+      if (!(std::stringstream(line) >> p.K[i - 2].x >> p.K[i - 2].y >> p.K[i - 2].z >> p.KW[i - 2]))
+        fail("kpointfile: point " + std::to_string(i - 2) + " is not 'kx ky kz w'");
       p.KW[i - 2] /= nk0;
       ++i;
     }
   }
+  if (i < 2) fail("kpointfile '" + p.kpointfile + "' has no k counts");
+  if (i - 2 < nk)
+    fail("kpointfile '" + p.kpointfile + "' declares " + std::to_string(nk) + " points but lists " +
+         std::to_string(i - 2));
 }
 
 static bool inbz_fcc(const Vec3& K) {

@@ -74,3 +74,18 @@ def test_noalloc_rejects_sizes_beyond_limit(ctx):
     # 4 n nev batch doubles of inverse-iteration vectors above the scratch
     assert lib.pmx_heev_batched_noalloc(None, 832, 1000, d, 512, d, d, d) == _capi.PMX_ERR_LIMIT
     assert lib.pmx_heev_batched_noalloc(None, 64, 2, d, 65, d, d, d) == _capi.PMX_ERR_INVALID
+
+
+def test_noalloc_values_only_and_largest_sizes(ctx):
+    """Eigenvalues only (no vectors: the scratch array is not touched), then the
+    largest matrices the entry point takes (n 800, partial sums next to the
+    scratch limit in shared memory), two calls in a row."""
+    from picomax_b200 import _capi
+    rng = np.random.default_rng(7)
+    A = np.stack([_random_hermitian(rng, 226) for _ in range(3)])
+    w0, _ = ctx.heev(A, 12, vectors=False)
+    w1, _ = _noalloc(_capi.load(), A, 12, vectors=False)
+    scale = max(np.max(np.abs(np.linalg.eigvalsh(a))) for a in A)
+    assert np.max(np.abs(w1 - w0)) < 1e-12 * scale * 226
+    B = np.stack([_random_hermitian(rng, 800) for _ in range(2)])
+    _check(ctx, B, 16)
