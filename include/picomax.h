@@ -232,6 +232,17 @@ int pmx_chi_epsm(pmx_ctx* ctx, const pmx_problem* p, int sw, int precision, doub
 int pmx_eps_macroscopic(pmx_ctx* ctx, int neps, int nq, int nfreq, const double* chi_re, const double* chi_im,
                         double* epsm);
 
+/* Electron energy-loss spectrum from eps_M [nq][nfreq][2] (as pmx_chi_epsm
+ * returns it): loss [nq][nfreq] = -Im(1 / eps_M(q, w)), and per q the loss
+ * peak plasmon [nq][2] = (energy in eV, height): the largest loss at
+ * w >= wmin (eV; excludes the low-frequency edge), refined by the vertex of
+ * the parabola through the peak and its neighbours. Along a q line (-qpath,
+ * or several -qvec) plasmon[:, 0] is the plasmon dispersion. Post-processing
+ * of macroscopic.m (include/matlab_wrapper/+picomax/+eps/macroscopic.m:13-29,
+ * :79), which computes eps_M; the C++ reference has no counterpart. */
+int pmx_eels(pmx_ctx* ctx, int nq, int nfreq, double dfreq, double wmin, const double* epsm, double* loss,
+             double* plasmon);
+
 /* Kramers-Kronig transform of nrows spectra in place, re/im [nrows][nfreq],
  * w_f = dfreq f (kramerskronigtransform, src/pmx_chi.cpp:272-309). */
 int pmx_kk(pmx_ctx* ctx, int nrows, int nfreq, double dfreq, double* re, double* im);

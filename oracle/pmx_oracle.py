@@ -463,6 +463,28 @@ def eps_macroscopic(chi_ll_re: np.ndarray, chi_ll_im: np.ndarray, neps: int) -> 
     return out
 
 
+def loss_function(epsm: np.ndarray) -> np.ndarray:
+    """EELS loss -Im(1 / eps_M) of eps_M (macroscopic.m:79 gives eps_M; the
+    loss is its standard use, the reference's C++ has no counterpart)."""
+    return -np.imag(1.0 / np.asarray(epsm, complex))
+
+
+def plasmon_peak(loss: np.ndarray, dfreq: float, fmin: int = 0):
+    """(energy, height) of the largest loss at frequency index >= fmin (lowest
+    index on ties), refined by the vertex of the parabola through the peak and
+    its two neighbours when they bracket a strict maximum."""
+    L = np.asarray(loss, float)
+    i = fmin + int(np.argmax(L[fmin:]))
+    w, h = i * dfreq, L[i]
+    if 0 < i < len(L) - 1:
+        ym, y0, yp = L[i - 1], L[i], L[i + 1]
+        den = ym - 2.0 * y0 + yp
+        if den < 0:
+            t = 0.5 * (ym - yp) / den
+            w, h = (i + t) * dfreq, y0 - 0.25 * (ym - yp) * t
+    return w, h
+
+
 # ----------------------------------------------------------------- inputs
 def gvectors(cr: Crystal, gcut: float, first=None):
     """G list of generate_gpt (src/pmx_basis.cpp:29-81): every integer

@@ -43,7 +43,7 @@ EXPORTS = (
     "pmx_problem_params",
     "pmx_problem_set_params",
     "pmx_band_vjp",
-    "pmx_epsm_vjp", "pmx_ctx_set_wait_limit", "pmx_ctx_set_fault",
+    "pmx_epsm_vjp", "pmx_ctx_set_wait_limit", "pmx_ctx_set_fault", "pmx_eels",
     "pmx_band_batch",
     "pmx_chi_batch",
     "pmx_ctx_occupation_ties",
@@ -119,6 +119,7 @@ def load() -> ctypes.CDLL:
         "pmx_epsm_vjp": (c_int, [c_void_p, c_void_p, dp, dp, dp, dp]),
         "pmx_ctx_set_wait_limit": (c_int, [c_void_p, c_longlong]),
         "pmx_ctx_set_fault": (c_int, [c_void_p, c_int]),
+        "pmx_eels": (c_int, [c_void_p, c_int, c_int, c_double, c_double, dp, dp, dp]),
         "pmx_band_batch": (c_int, [c_void_p, c_int, POINTER(c_void_p), POINTER(dp)]),
         "pmx_chi_batch": (c_int, [c_void_p, c_int, POINTER(c_void_p), c_int, c_int, POINTER(dp), POINTER(dp),
                                   POINTER(dp)]),
@@ -402,6 +403,19 @@ class Context:
         st = self._lib.pmx_chi_device(self.handle, prob.handle, switch, precision, c_void_p(re_ptr),
                                       c_void_p(im_ptr), c_void_p(epsm_ptr) if epsm_ptr else None)
         self._check(st, "chi_device")
+
+    def eels(self, epsm, dfreq: float, wmin: float = 0.0):
+        """Loss function -Im(1/eps_M) [nq, nf] and plasmon peaks [nq, 2] (eV,
+        height) from eps_M [nq, nf] (complex)."""
+        e = np.asarray(epsm, np.complex128)
+        e = e.reshape(-1, e.shape[-1])
+        nq, nf = e.shape
+        buf = np.ascontiguousarray(np.stack([e.real, e.imag], -1))
+        loss = np.zeros((nq, nf), np.float64)
+        peak = np.zeros((nq, 2), np.float64)
+        self._check(self._lib.pmx_eels(self.handle, nq, nf, float(dfreq), float(wmin), _dptr(buf), _dptr(loss),
+                                       _dptr(peak)), "eels")
+        return loss, peak
 
     def eps_macroscopic(self, neps: int, chi_re, chi_im):
         """eps_M [nq, nf] from the LL block [nq, npairs, nf] of a chi spectrum."""

@@ -633,5 +633,62 @@ cudaError_t launch_epsm(const double* re, const double* im, int neps, int nq, in
   return cudaGetLastError();
 }
 
+// Electron energy-loss function L(q, w) = -Im(1 / eps_M(q, w)) (the quantity
+// the macroscopic dielectric function of macroscopic.m, :13-29 and :79, is
+// taken for in EELS), and per q the loss peak: the plasmon. One warp per q:
+// argmax of L over frequencies f >= fmin (ties to the lower f), then the
+// vertex of the parabola through the peak and its two neighbours.
+__global__ void __launch_bounds__(128) loss_kernel(const double2* __restrict__ epsm, int nq, int nf, int fmin,
+                                                   double dfreq, double* __restrict__ loss,
+                                                   double* __restrict__ peak) {
+  const int lane = threadIdx.x & 31;
+  const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (q >= nq) return;
+  const double2* e = epsm + (size_t)q * nf;
+  double* L = loss + (size_t)q * nf;
+  double best = -1.0;
+  int bi = -1;
+  for (int f = lane; f < nf; f += 32) {
+    const double2 v = e[f];
+    const double d = v.x * v.x + v.y * v.y;
+    const double l = d > 0.0 ? v.y / d : 0.0;  // -Im(1/eps) = Im(eps) / |eps|^2
+    L[f] = l;
+    if (f >= fmin && (l > best || bi < 0)) {
+      best = l;
+      bi = f;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (oi >= 0 && (bi < 0 || ob > best || (ob == best && oi < bi))) {
+      best = ob;
+      bi = oi;
+    }
+  }
+  __syncwarp();
+  if (lane == 0) {
+    double w = bi >= 0 ? bi * dfreq : 0.0, h = bi >= 0 ? best : 0.0;
+    if (bi > 0 && bi + 1 < nf) {
+      const double ym = L[bi - 1], y0 = L[bi], yp = L[bi + 1];
+      const double den = ym - 2.0 * y0 + yp;
+      if (den < 0.0) {
+        const double t = 0.5 * (ym - yp) / den;  // in (-1/2, 1/2) at a strict maximum
+        w = (bi + t) * dfreq;
+        h = y0 - 0.25 * (ym - yp) * t;
+      }
+    }
+    peak[2 * q] = w;
+    peak[2 * q + 1] = h;
+  }
+}
+
+cudaError_t launch_loss(const double2* epsm, int nq, int nf, int fmin, double dfreq, double* loss, double* peak,
+                        cudaStream_t st) {
+  if (nq <= 0 || nf <= 0) return cudaSuccess;
+  loss_kernel<<<(nq + 3) / 4, 128, 0, st>>>(epsm, nq, nf, fmin, dfreq, loss, peak);
+  return cudaGetLastError();
+}
+
 }  // namespace dev
 }  // namespace pmx

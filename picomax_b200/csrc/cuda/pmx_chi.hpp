@@ -87,5 +87,9 @@ namespace dev {
 // eps_M per (q, w) from the chi LL block laid out [q][pair][f] (re, im);
 // out [nq][nf] complex. neps <= 64.
 cudaError_t launch_epsm(const double* re, const double* im, int neps, int nq, int nf, double2* out, cudaStream_t st);
+// loss [nq][nf] = -Im(1/eps_M); peak [nq][2] = (frequency, height) of the
+// largest loss at f >= fmin, refined by a parabola through its neighbours.
+cudaError_t launch_loss(const double2* epsm, int nq, int nf, int fmin, double dfreq, double* loss, double* peak,
+                        cudaStream_t st);
 }  // namespace dev
 }  // namespace pmx

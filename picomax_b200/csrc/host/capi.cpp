@@ -1268,6 +1268,31 @@ extern "C" int pmx_chi_epsm(pmx_ctx* ctx, const pmx_problem* P, int sw, int prec
   return run_chi(ctx, P, sw, precision, re, im, false, epsm);
 }
 
+extern "C" int pmx_eels(pmx_ctx* ctx, int nq, int nfreq, double dfreq, double wmin, const double* epsm,
+                        double* loss, double* plasmon) {
+  if (nq <= 0 || nfreq <= 0 || !(dfreq > 0) || !epsm || !loss || !plasmon) return PMX_ERR_INVALID;
+  return guarded(ctx, [&]() {
+    const size_t ne = (size_t)nq * nfreq;
+    CK(ctx->epsm.ensure(sizeof(double2) * ne + sizeof(double) * (ne + 2 * (size_t)nq)));
+    double2* de = ctx->epsm.as<double2>();
+    double* dl = reinterpret_cast<double*>(de + ne);
+    double* dp = dl + ne;
+    CK(cudaMemcpyAsync(de, epsm, sizeof(double2) * ne, cudaMemcpyHostToDevice, ctx->stream));
+    ctx->h2d += (long long)(sizeof(double2) * ne);
+    const int fmin = std::max(0, (int)std::ceil(wmin / dfreq - 1e-9));
+    {
+      KTime kt(ctx, "loss");
+      CK(pmx::dev::launch_loss(de, nq, nfreq, fmin, dfreq, dl, dp, ctx->stream));
+    }
+    ctx->launches += 1;
+    CK(cudaMemcpyAsync(loss, dl, sizeof(double) * ne, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(plasmon, dp, sizeof(double) * 2 * nq, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->d2h += (long long)(sizeof(double) * (ne + 2 * (size_t)nq));
+    return (int)PMX_OK;
+  });
+}
+
 extern "C" void* pmx_ctx_stream(const pmx_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
 extern "C" int pmx_ctx_kernel_time(const pmx_ctx* c, const char* family, double* ms, long long* launches) {
