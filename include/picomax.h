@@ -93,11 +93,14 @@ int pmx_problem_write_gpt(const pmx_problem* p);
 
 /* ---------------------------------------------------------------- context */
 
-/* Limit in nanoseconds of every bounded mbarrier wait of the mixed-precision
- * contraction (0: 2 s). A wait that runs out makes its CTA record the error,
- * wait for its own copies and MMAs in flight, free its tensor memory and
- * return; the call then fails with PMX_ERR_TIMEOUT and the context stays
- * usable. No reference counterpart (the reference has no device waits). */
+/* Limit in nanoseconds of every bounded device wait (0: 2 s): the mbarrier
+ * waits of the mixed-precision contraction and the waits of the two-stage
+ * eigensolver's bulge chase on the previous sweep. A contraction wait that
+ * runs out makes its CTA record the error, wait for its own copies and MMAs
+ * in flight, free its tensor memory and return; a bulge-chase wait that runs
+ * out fails its matrix. The call then fails with PMX_ERR_TIMEOUT and the
+ * context stays usable. No reference counterpart (the reference has no device
+ * waits). */
 int pmx_ctx_set_wait_limit(pmx_ctx* ctx, long long ns);
 
 /* Test hooks, no reference counterpart: fault 1 makes the producer warps of
@@ -105,7 +108,10 @@ int pmx_ctx_set_wait_limit(pmx_ctx* ctx, long long ns);
  * control warp's bounded wait runs out and the timeout path above runs
  * (combine with a short pmx_ctx_set_wait_limit); fault 2 stops the
  * eigensolver's bisection after one round, so that its status reports
- * non-convergence (PMX_ERR_NOCONV). 0 restores normal operation. */
+ * non-convergence (PMX_ERR_NOCONV); fault 3 makes the second sweep of the
+ * two-stage eigensolver's bulge chase wait for progress that never comes, so
+ * that its bounded wait gives up (PMX_ERR_TIMEOUT; combine with a short
+ * pmx_ctx_set_wait_limit). 0 restores normal operation. */
 int pmx_ctx_set_fault(pmx_ctx* ctx, int fault);
 
 int pmx_ctx_create(int device, pmx_ctx** out);

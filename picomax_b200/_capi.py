@@ -323,7 +323,10 @@ class Context:
         self._check(self._lib.pmx_ctx_set_wait_limit(self.handle, int(ns)), "set_wait_limit")
 
     def set_fault(self, fault: int):
-        """Test hook: 1 = the mixed contraction's producers withhold one arrival (its wait runs out)."""
+        """Test hooks: 1 = the mixed contraction's producers withhold one arrival
+        (its wait runs out), 2 = the eigenvalue bisection stops after one round,
+        3 = the two-stage bulge chase's second sweep waits for progress that
+        never comes (its wait runs out); 0 = normal operation."""
         self._check(self._lib.pmx_ctx_set_fault(self.handle, int(fault)), "set_fault")
 
     def set_schedule(self, schedule: int):

@@ -20,9 +20,10 @@
 //     below the band (LAPACK layout); T goes into the free upper tile.
 //  2. sbtrd_kernel (one CTA per matrix): the band (16 sub-diagonals plus 16
 //     for the bulge) lives in shared memory; sweeps chase their bulges down
-//     the band, each sweep three time steps behind the previous one so that
-//     the tasks of one time step touch disjoint rows (one warp per task, one
-//     barrier per time step). Reflectors go to global memory.
+//     the band, eight at a time (a pair of warps per sweep), each step of a
+//     sweep waiting only for the previous sweep to leave its rows (progress
+//     words in shared memory, no block-wide barrier). Reflectors go to
+//     global memory.
 //  3. tri_eig_kernel: bisection and inverse iteration on the tridiagonal
 //     matrix (pmx_trieig.cuh), one CTA per matrix with small shared memory,
 //     so that many matrices share an SM.
@@ -36,6 +37,7 @@
 // exactly) and the eigenvectors are exactly zero in the padding.
 #include <algorithm>
 #include <cfloat>
+#include <climits>
 #include <cmath>
 
 #include "pmx_common.cuh"
@@ -50,7 +52,6 @@ namespace {
 constexpr int kNB = 16;        // panel width = band width
 constexpr int kThr = 256;      // threads per CTA of every stage
 constexpr int kNW = kThr / 32;
-constexpr int kLag = 3;        // time steps between consecutive sweeps
 constexpr int kMaxLd = 416;    // largest padded dimension (shared memory of both stages)
 constexpr int kVecBlock = 32;  // eigenvectors per back-transform CTA
 
@@ -136,7 +137,7 @@ struct SbSmem {
   double2* P;     // [16 * 17] T^H M
   double2* taus;  // [16]
   // panel QR work arrays, inside Y (free until Y = A V is formed)
-  double2* part;  // [2][16][16] partial sums of the panel QR
+  double2* part;  // [2][8][16] partial sums of the panel QR
   double2* rowj;  // [2][16] the current row of the panel QR
   double2* pvw;   // [8][2][MR] per-warp pivot buffers of the panel QR
 };
@@ -154,25 +155,28 @@ __host__ __device__ inline size_t sb_smem_bytes(int ld) {
 // layout: R on and above the diagonal, v below it) and the explicit V (unit
 // diagonal, zeros above) in shared memory. Thread (column c = tid % 16,
 // row group g = tid / 16) holds rows g, g + 16, ... of column c in registers.
-// Per column j one CTA-wide reduction of one value per thread: for c > j the
-// dot conj(a_j)^T a_c (which gives v^H a_c once the reflector's scale is
-// known), for c = j the norm |x|^2, for c < j the dot v_c^H a_j (which gives
-// the T column, zlarft). The pivot column reaches the threads of a row group
-// through the warp's own shared-memory buffer (the group's 16 threads share
-// a warp). red/rowj: [2][16][16] / [2][16]; pvw [8][2][MR]; dsm [16][16];
-// tsm [16]; T [16][17].
+// Per column j one CTA-wide reduction of one value per thread, the same
+// product for every column, sum_{r > j} conj(a_j[r]) a_c[r]: for c > j it
+// gives v^H a_c once the reflector's scale is known, for c = j the norm
+// |x|^2, for c < j (conjugated) the dot v_c^H v_j of the T column (zlarft).
+// The two row groups of a warp are summed with one shuffle, the eight warps'
+// sums in shared memory. The update of the columns has one form for every
+// column, a_c[r] -= a_j[r] s_c (s_c = scal w_c for c > j, 1 - scal for c = j,
+// 0 for c < j), so that the lanes of a warp do not diverge. T column j - 1 is
+// formed in iteration j by all warps, two rows each. The pivot column reaches
+// the threads of a row group through the warp's own shared-memory buffer (the
+// group's 16 threads share a warp). red/rowj: [2][8][16] / [2][16]; pvw
+// [8][2][MR]; dsm [16][16]; tsm [16]; T [16][17].
 template <int MR>
 __device__ void panel_qr(double2* __restrict__ A, int ld, int c0, int r0, int m, double2* V, double2* T,
                          double2* red, double2* rowj, double2* pvw, double2* dsm, double2* tsm) {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int c = tid & 15, g = tid >> 4;
+  const int Mt = m / kNB;  // m is a multiple of 16: row slots t < Mt are inside the panel
   double2* pv = pvw + (size_t)wid * 2 * MR + (g & 1) * MR;  // this group's pivot buffer
   double2 col[MR];
 #pragma unroll
-  for (int t = 0; t < MR; ++t) {
-    const int r = g + 16 * t;
-    col[t] = r < m ? A[(size_t)(c0 + c) * ld + r0 + r] : make_double2(0, 0);
-  }
+  for (int t = 0; t < MR; ++t) col[t] = t < Mt ? A[(size_t)(c0 + c) * ld + r0 + g + 16 * t] : make_double2(0, 0);
   // the group's rows of column 0 become the first pivot
   if (c == 0) {
 #pragma unroll
@@ -181,65 +185,59 @@ __device__ void panel_qr(double2* __restrict__ A, int ld, int c0, int r0, int m,
   __syncwarp();
   for (int j = 0; j < kNB; ++j) {
     const int buf = j & 1;
-    // ---- partial sums over this thread's rows r > j
-    double2 acc = make_double2(0, 0);
+    // ---- partial sums over this thread's rows r > j (two chains)
+    double2 acc0 = make_double2(0, 0), acc1 = make_double2(0, 0);
+    if (g > j) {
+      const double2 aj = pv[0];
+      acc0.x = aj.x * col[0].x + aj.y * col[0].y;
+      acc0.y = aj.x * col[0].y - aj.y * col[0].x;
+    }
 #pragma unroll
-    for (int t = 0; t < MR; ++t) {
-      const int r = g + 16 * t;
-      if (r > j && r < m) {
+    for (int t = 1; t < MR; ++t) {
+      if (t < Mt) {
         const double2 aj = pv[t];
-        if (c > j)
-          acc = cadd(acc, cmulc(aj, col[t]));
-        else if (c < j)
-          acc = cadd(acc, cmulc(col[t], aj));
-        else
-          acc.x += aj.x * aj.x + aj.y * aj.y;
+        double2& a = (t & 1) ? acc1 : acc0;
+        a.x = fma(aj.x, col[t].x, fma(aj.y, col[t].y, a.x));
+        a.y = fma(aj.x, col[t].y, fma(-aj.y, col[t].x, a.y));
       }
     }
-    red[(buf * 16 + g) * 16 + c] = acc;
+    double2 acc = cadd(acc0, acc1);
+    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 16);
+    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 16);
+    if (lane < 16) red[(buf * 8 + wid) * 16 + c] = acc;
     if (g == j) rowj[buf * 16 + c] = col[0];  // row j = row group j, slot 0
     __syncthreads();
-    double2 tot = make_double2(0, 0);
-    double xn = 0.0;
+    double2 tq[8];
+    double xq[8];
 #pragma unroll
-    for (int q = 0; q < 16; ++q) {
-      tot = cadd(tot, red[(buf * 16 + q) * 16 + c]);
-      xn += red[(buf * 16 + q) * 16 + j].x;
+    for (int q = 0; q < 8; ++q) {
+      tq[q] = red[(buf * 8 + q) * 16 + c];
+      xq[q] = red[(buf * 8 + q) * 16 + j].x;
     }
+    const double2 tot = cadd(cadd(cadd(tq[0], tq[1]), cadd(tq[2], tq[3])), cadd(cadd(tq[4], tq[5]), cadd(tq[6], tq[7])));
+    const double xn = ((xq[0] + xq[1]) + (xq[2] + xq[3])) + ((xq[4] + xq[5]) + (xq[6] + xq[7]));
     const double2 alpha = rowj[buf * 16 + j], rj = rowj[buf * 16 + c];
-    const Refl R = make_refl(alpha, xn);
-    if (c > j) {
-      // w_c = conj(tau) v^H a_c; a_c -= v w_c with v = (1; scal a_j)
-      const double2 w = cmul(cconj(R.tau), cadd(rj, cmulc(R.scal, tot)));
-      const double2 sw = cmul(R.scal, w);
-#pragma unroll
-      for (int t = 0; t < MR; ++t) {
-        const int r = g + 16 * t;
-        if (r > j && r < m) col[t] = csub(col[t], cmul(pv[t], sw));
-      }
-      if (g == j) col[0] = csub(col[0], w);
-    } else if (c == j) {
-#pragma unroll
-      for (int t = 0; t < MR; ++t) {
-        const int r = g + 16 * t;
-        if (r > j && r < m) col[t] = cmul(col[t], R.scal);
-      }
-      if (g == j) col[0] = make_double2(R.beta, 0.0);
-    } else if (g == 0) {
-      dsm[j * 16 + c] = cadd(cconj(rj), cmul(R.scal, tot));  // v_c^H v_j
-    }
-    if (tid == 0) tsm[j] = R.tau;
-    // T column j - 1 (its dots are complete now): T[0:j-1, j-1] = -tau T d
-    if (wid == 0 && j >= 1) {
-      const int jj = j - 1;
-      double2 sacc = make_double2(0, 0);
-      if (lane < jj)
-        for (int q = lane; q < jj; ++q) sacc = cadd(sacc, cmul(T[lane * 17 + q], dsm[jj * 16 + q]));
+    // T column j - 1 (its dots are complete now): T[0:j-1, j-1] = -tau T d,
+    // rows 2 wid and 2 wid + 1
+    if (j >= 1) {
+      const int jj = j - 1, l = 2 * wid + (lane >> 4);
+      double2 p = c >= l && c < jj ? cmul(T[l * 17 + c], dsm[jj * 16 + c]) : make_double2(0, 0);
+      p.x = sum16(p.x);
+      p.y = sum16(p.y);
       const double2 tj = tsm[jj];
-      if (lane < jj) T[lane * 17 + jj] = cmul(make_double2(-tj.x, -tj.y), sacc);
-      if (lane == jj) T[jj * 17 + jj] = tj;
-      if (lane > jj && lane < kNB) T[lane * 17 + jj] = make_double2(0, 0);
+      if (c == 0) T[l * 17 + jj] = l < jj ? cmul(make_double2(-tj.x, -tj.y), p) : (l == jj ? tj : make_double2(0, 0));
     }
+    const Refl R = make_refl(alpha, xn);
+    // w_c = conj(tau) v^H a_c (v = (1; scal a_j)); a_c -= v w_c
+    const double2 w = cmul(cconj(R.tau), cadd(rj, cmulc(R.scal, tot)));
+    const double2 sw = c > j ? cmul(R.scal, w) : (c == j ? make_double2(1.0 - R.scal.x, -R.scal.y) : make_double2(0, 0));
+    if (g > j) col[0] = csub(col[0], cmul(pv[0], sw));
+#pragma unroll
+    for (int t = 1; t < MR; ++t)
+      if (t < Mt) col[t] = csub(col[t], cmul(pv[t], sw));
+    if (g == j) col[0] = c > j ? csub(col[0], w) : (c == j ? make_double2(R.beta, 0.0) : col[0]);
+    if (g == 0 && c < j) dsm[j * 16 + c] = cadd(cconj(rj), cmul(R.scal, cconj(tot)));  // v_c^H v_j
+    if (tid == 0) tsm[j] = R.tau;
     // the next pivot column reaches the group through the warp's buffer
     __syncwarp();
     if (j + 1 < kNB && c == j + 1) {
@@ -263,7 +261,7 @@ __device__ void panel_qr(double2* __restrict__ A, int ld, int c0, int r0, int m,
 #pragma unroll
   for (int t = 0; t < MR; ++t) {
     const int r = g + 16 * t;
-    if (r < m) {
+    if (t < Mt) {
       A[(size_t)(c0 + c) * ld + r0 + r] = col[t];
       V[pidx(r, c)] = r < c ? make_double2(0, 0) : (r == c ? make_double2(1, 0) : col[t]);
     }
@@ -410,8 +408,8 @@ __global__ void __launch_bounds__(kThr, 1) sb_kernel(const EigItem* __restrict__
   S.M = S.T + kNB * 17;
   S.P = S.M + kNB * 17;
   S.taus = S.P + kNB * 17;
-  S.part = S.Y;  // 512 + 32 + 16 MR <= 16 mmax double2 for ld >= 96
-  S.rowj = S.part + 2 * 16 * 16;
+  S.part = S.Y;  // 256 + 32 + 16 MR <= 16 mmax double2 for ld >= 96
+  S.rowj = S.part + 2 * 8 * 16;
   S.pvw = S.rowj + 2 * 16;
 
   for (int c0 = 0; c0 + kNB < ld; c0 += kNB) {
@@ -480,24 +478,59 @@ __global__ void __launch_bounds__(kThr, 1) sb_kernel(const EigItem* __restrict__
 // bulge (a task reaches d = len + 15 <= 31 at most). kBandLd is even, so reads
 // along a row of the band (stride kBandLd - 1) and down a column (stride 1)
 // are both free of bank conflicts.
+//
+// Task (s, j) (sweep s, step j, first row p = s + 1 + 16 j) reads and writes
+// exactly the elements (r, c) with p <= c < p + 16 and c <= r < p + 32 (its
+// diagonal block D and the block E below it), plus column s when j = 0. Two
+// tasks of different sweeps commute unless those sets meet, and task (s, j)
+// meets sweep s - 1 only in its steps j' <= j + 1. So sweep s may run step j
+// as soon as sweep s - 1 has finished min(j + 2, its step count) steps: each
+// pair of warps runs its sweeps s = pair, pair + 8, ... and publishes its
+// progress in a shared-memory word (release), which the next sweep's pair
+// waits for (acquire, bounded by a time limit). No block-wide barrier runs
+// between steps.
 constexpr int kBandLd = 2 * kNB;
-constexpr int kSlots = 10;          // sweeps in flight: at most ceil(26 / 3) = 9 for ld 416
-constexpr int kS2Thr = 512;         // 8 tasks x (D warp + E warp)
+constexpr int kPairs = 8;                // sweeps in flight: one per pair of warps
+constexpr int kS2Thr = 64 * kPairs;      // a D warp and an E warp per pair
 constexpr int kS2W = kS2Thr / 32;
+constexpr int kProgStride = 64;          // progress word: sweep * 64 + steps done (<= 26)
+constexpr long long kWaitNs = 2000000000LL;  // default limit of one wait
 
 __host__ __device__ inline size_t sbtrd_smem_bytes(int ld) {
-  return sizeof(double2) * ((size_t)ld * kBandLd + kSlots * 17 + kSlots * kNB + kS2W * 2 * kNB) +
-         sizeof(double) * kSlots;
+  return sizeof(double2) * ((size_t)ld * kBandLd + kPairs * 2 * 17 + kS2W * 2 * kNB) + sizeof(int) * (kPairs + 4);
 }
 
-// Reflector of a 16-vector held as x_i on lanes i (both 16-lane halves hold
-// the same values): v_i on lane i (v_0 = 1, zero beyond len), tau, beta.
-__device__ __forceinline__ Refl refl16(double2 x, int i, int len, double2& v) {
-  const double xn = sum16(i >= 1 && i < len ? x.x * x.x + x.y * x.y : 0.0);
-  const double2 a0 = make_double2(__shfl_sync(0xffffffffu, x.x, 0), __shfl_sync(0xffffffffu, x.y, 0));
-  const Refl R = make_refl(a0, xn);
-  v = i == 0 ? make_double2(1, 0) : (i < len ? cmul(x, R.scal) : make_double2(0, 0));
-  return R;
+__device__ __forceinline__ int ld_acquire_shared(const int* p) {
+  int v;
+  asm volatile("ld.acquire.cta.shared::cta.b32 %0, [%1];"
+               : "=r"(v)
+               : "r"((unsigned)__cvta_generic_to_shared(p))
+               : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_shared(int* p, int v) {
+  asm volatile("st.release.cta.shared::cta.b32 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(p)), "r"(v)
+               : "memory");
+}
+__device__ __forceinline__ long long global_ns() {
+  long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Waits until *flag >= need. Gives up, and sets *err, after limit_ns, after
+// 2^28 polls, or at once when another warp has given up already.
+__device__ __forceinline__ void wait_progress(const int* flag, int need, int* err, long long limit_ns) {
+  if (ld_acquire_shared(flag) >= need) return;
+  const long long t0 = global_ns();
+  for (int k = 1; k < (1 << 28); ++k) {
+    if (ld_acquire_shared(flag) >= need) return;
+    if ((k & 255) == 0) {
+      if (*reinterpret_cast<volatile int*>(err)) return;
+      if (global_ns() - t0 > limit_ns) break;
+    }
+  }
+  atomicExch(err, 1);
 }
 
 __global__ void __launch_bounds__(kS2Thr, 1) sbtrd_kernel(const EigItem* __restrict__ items,
@@ -509,56 +542,68 @@ __global__ void __launch_bounds__(kS2Thr, 1) sbtrd_kernel(const EigItem* __restr
   double2* R = rbuf + it.r_off;
   extern __shared__ __align__(16) unsigned char smraw[];
   double2* Bd = reinterpret_cast<double2*>(smraw);
-  double2* slot = Bd + (size_t)ld * kBandLd;  // [kSlots][17]: v[16], tau of the sweeps in flight
-  double2* v2s = slot + kSlots * 17;          // [kSlots][16]: new reflectors (tau in place of v_0)
-  double2* wsm = v2s + kSlots * kNB;          // [16 warps][32]: vectors a warp broadcasts to its lanes
-  double* bst = reinterpret_cast<double*>(wsm + kS2W * 2 * kNB);  // [kSlots]: beta of a sweep's column
+  double2* slots = Bd + (size_t)ld * kBandLd;  // [pair][2][17]: v (v_0 = 1), tau of the pair's next steps
+  double2* wsm = slots + kPairs * 2 * 17;       // [warp][32]: [0, 16) v, [16, 32) vectors broadcast in a warp
+  int* prog = reinterpret_cast<int*>(wsm + kS2W * 2 * kNB);  // [pair]: progress words
+  int* err = prog + kPairs;                                  // a wait gave up
   for (int idx = tid; idx < ld * kBandLd; idx += kS2Thr) {
     const int c = idx / kBandLd, d = idx % kBandLd;
     Bd[idx] = (d <= kNB && c + d < ld) ? A[(size_t)c * ld + c + d] : make_double2(0, 0);
   }
+  if (tid < kPairs) prog[tid] = -1;
+  if (tid == 0) *err = 0;
   __syncthreads();
   // A(r, c) for 0 <= r - c <= 31 (int arithmetic, never a negative offset)
   auto at = [&](int r, int c) -> double2& { return Bd[c * kBandLd + (r - c)]; };
   const int i = lane & 15, h = lane >> 4;
-  const int pair = wid >> 1;          // task slot of this warp
+  const int pair = wid >> 1;
   const bool ewarp = (wid & 1) != 0;  // E (bulge) warp, else D (diagonal block) warp
-  double2* wv = wsm + wid * 2 * kNB;  // [0..15] first vector, [16..31] second
-  const int tmax = kLag * (ld - 2);
-  for (int t = 0; t <= tmax; ++t) {
-    const int smax = min(t / kLag, ld - 2);
-    int smin = smax;
-    while (smin - 1 >= 0 && t - kLag * (smin - 1) < sweep_steps(ld, smin - 1)) --smin;
-    if (t - kLag * smax >= sweep_steps(ld, smax)) smin = smax + 1;  // nothing active
-    for (int s = smax - pair; s >= smin; s -= 8) {
-      const int j = t - kLag * s;
+  double2* wv = wsm + wid * 2 * kNB;
+  double2* sl = slots + pair * 2 * 17;
+  const long long limit = it.wait_ns > 0 ? it.wait_ns : kWaitNs;
+  for (int s = pair; s <= ld - 2; s += kPairs) {
+    const int ns = sweep_steps(ld, s), nprev = s > 0 ? sweep_steps(ld, s - 1) : 0;
+    const long long ridx = sweep_first(ld, s);
+    for (int j = 0; j < ns; ++j) {
       const int p = s + 1 + kNB * j, len = min(kNB, ld - p), q = p + len;
-      const long long ridx = sweep_first(ld, s);
-      // this task's reflector v (16, zero beyond len) and tau into wv[0..15]
-      double2 tau;
-      const double2* vv;
-      if (j == 0) {
-        // from column s, rows s+1 .. s+len (both warps; the D warp stages beta
-        // and records the reflector)
-        double2 v;
-        const double2 x = i < len ? at(p + i, s) : make_double2(0, 0);
-        const Refl Rf = refl16(x, i, len, v);
-        tau = Rf.tau;
-        if (h == 0) wv[i] = v;
-        if (!ewarp && h == 0) {
-          if (i == 0) bst[s % kSlots] = Rf.beta;
-          R[ridx * kNB + i] = i == 0 ? tau : v;
-        }
+      if (s > 0) {  // sweep s - 1 has left the rows of this task
+        const int need = (it.wait_fault && s == 1) ? INT_MAX : (s - 1) * kProgStride + min(j + 2, nprev);
+        wait_progress(&prog[(s - 1) % kPairs], need, err, limit);
         __syncwarp();
-        vv = wv;
-      } else {
-        vv = slot + (s % kSlots) * 17;
-        tau = vv[16];
       }
-      const double2 vi = vv[i];
+      // this step's reflector: tau, v (all 16 entries at vsrc, v_0 = 1, zero
+      // beyond len), v_i and v at this lane's columns 8h .. 8h + 7
+      double2 tau, vi, vc[8];
+      double beta = 0.0;
+      const double2* vsrc;
+      if (j == 0) {
+        // from column s, rows p .. p + len - 1 (both warps)
+        const double2* cs = Bd + (size_t)s * kBandLd + 1;  // A(p + k, s) = cs[k]
+        double xq[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int k = 1; k < kNB; ++k)
+          if (k < len) {
+            const double2 x = cs[k];
+            xq[k & 3] += x.x * x.x + x.y * x.y;
+          }
+        const Refl Rf = make_refl(cs[0], (xq[0] + xq[1]) + (xq[2] + xq[3]));
+        tau = Rf.tau;
+        beta = Rf.beta;
+        vi = i == 0 ? make_double2(1, 0) : (i < len ? cmul(cs[i], Rf.scal) : make_double2(0, 0));
+        if (h == 0) wv[i] = vi;
+        if (!ewarp && h == 0) R[ridx * kNB + i] = i == 0 ? tau : vi;
+        __syncwarp();
+        vsrc = wv;
+      } else {
+        vsrc = sl + (j & 1) * 17;
+        tau = vsrc[16];
+        vi = vsrc[i];
+      }
+#pragma unroll
+      for (int cc = 0; cc < 8; ++cc) vc[cc] = vsrc[8 * h + cc];
       if (!ewarp) {
         // ---- D <- H^H D H on D = A(p : p+len, p : p+len): lane (row i, half h)
-        double2 d[8], y = make_double2(0, 0);
+        double2 d[8];
 #pragma unroll
         for (int cc = 0; cc < 8; ++cc) {
           const int c = 8 * h + cc;
@@ -569,107 +614,128 @@ __global__ void __launch_bounds__(kS2Thr, 1) sbtrd_kernel(const EigItem* __restr
           if (c > i) val.y = -val.y;
           d[cc] = (i < len && c < len) ? val : make_double2(0, 0);
         }
+        double2 y0 = make_double2(0, 0), y1 = make_double2(0, 0);
 #pragma unroll
-        for (int cc = 0; cc < 8; ++cc) y = cadd(y, cmul(d[cc], vv[8 * h + cc]));
+        for (int cc = 0; cc < 8; cc += 2) {
+          y0 = cadd(y0, cmul(d[cc], vc[cc]));
+          y1 = cadd(y1, cmul(d[cc + 1], vc[cc + 1]));
+        }
+        double2 y = cadd(y0, y1);
         y.x += __shfl_xor_sync(0xffffffffu, y.x, 16);
         y.y += __shfl_xor_sync(0xffffffffu, y.y, 16);
-        const double vhy = sum16(i < len ? cmulc(vi, y).x : 0.0);
-        const double al = -0.5 * (tau.x * tau.x + tau.y * tau.y) * vhy;
-        const double2 w = cadd(cmul(tau, y), cscale(vi, al));
-        if (h == 0) wv[kNB + i] = w;
+        if (h == 0) wv[kNB + i] = y;
         __syncwarp();
+        // v^H y = v^H D v (real), w = tau y - 1/2 |tau|^2 (v^H y) v
+        double sq[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < kNB; ++k) {
+          const double2 yk = wv[kNB + k], vk = vsrc[k];
+          sq[k & 3] += vk.x * yk.x + vk.y * yk.y;
+        }
+        const double al = -0.5 * (tau.x * tau.x + tau.y * tau.y) * ((sq[0] + sq[1]) + (sq[2] + sq[3]));
+        const double2 w = cadd(cmul(tau, y), cscale(vi, al));
 #pragma unroll
         for (int cc = 0; cc < 8; ++cc) {
           const int c = 8 * h + cc;
-          if (i < len && c <= i)
-            at(p + i, p + c) = csub(d[cc], cadd(cmul(vi, cconj(wv[kNB + c])), cmul(w, cconj(vv[c]))));
+          const double2 wc = cadd(cmul(tau, wv[kNB + c]), cscale(vc[cc], al));
+          if (i < len && c <= i) at(p + i, p + c) = csub(d[cc], cadd(cmul(vi, cconj(wc)), cmul(w, cconj(vc[cc]))));
         }
       } else if (q < ld) {
         // ---- E = A(q : q+len2, p : p+len) <- E H, then the next reflector
         // from E's first column and E(:, 1:) <- H2^H E(:, 1:)
         const int len2 = min(kNB, ld - q);
-        double2 e[8], u = make_double2(0, 0);
+        double2 e[8];
 #pragma unroll
         for (int cc = 0; cc < 8; ++cc) {
           const int c = 8 * h + cc;
           e[cc] = (i < len2 && c < len) ? at(q + i, p + c) : make_double2(0, 0);
         }
+        double2 u0 = make_double2(0, 0), u1 = make_double2(0, 0);
 #pragma unroll
-        for (int cc = 0; cc < 8; ++cc) u = cadd(u, cmul(e[cc], vv[8 * h + cc]));
+        for (int cc = 0; cc < 8; cc += 2) {
+          u0 = cadd(u0, cmul(e[cc], vc[cc]));
+          u1 = cadd(u1, cmul(e[cc + 1], vc[cc + 1]));
+        }
+        double2 u = cadd(u0, u1);
         u.x += __shfl_xor_sync(0xffffffffu, u.x, 16);
         u.y += __shfl_xor_sync(0xffffffffu, u.y, 16);
         const double2 tu = cmul(tau, u);  // E(i, c) -= tau u_i conj(v_c)
 #pragma unroll
-        for (int cc = 0; cc < 8; ++cc) e[cc] = csub(e[cc], cmul(tu, cconj(vv[8 * h + cc])));
-        // E(i, 0) sits on lane (i, half 0); the rows go to shared memory
+        for (int cc = 0; cc < 8; ++cc) e[cc] = csub(e[cc], cmul(tu, cconj(vc[cc])));
+        // E's first column x (lane (i, half 0) holds x_i) to every lane
         if (h == 0) wv[kNB + i] = e[0];
         __syncwarp();
-        const double2 x = wv[kNB + i];
-        double2 v2;
-        const Refl Rf = refl16(x, i, len2, v2);
+        double xq[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int k = 1; k < kNB; ++k)
+          if (k < len2) {
+            const double2 x = wv[kNB + k];
+            xq[k & 3] += x.x * x.x + x.y * x.y;
+          }
+        const Refl Rf = make_refl(wv[kNB], (xq[0] + xq[1]) + (xq[2] + xq[3]));
         if (h == 0) e[0] = i == 0 ? make_double2(Rf.beta, 0) : make_double2(0, 0);
 #pragma unroll
         for (int cc = 0; cc < 8; ++cc) {
           const int c = 8 * h + cc;
           if (i < len2 && c < len) at(q + i, p + c) = e[cc];
         }
-        __syncwarp();  // every lane has read wv (x) and stored its row
-        if (h == 0) wv[i] = v2;  // (this warp's v was read into registers above)
         __syncwarp();
-        // E(:, 1:) <- H2^H E(:, 1:): lane (column c = i, rows of half h)
+        // E(:, 1:) <- H2^H E(:, 1:): lane (column c = i, rows of half h);
+        // v2_r = x_r scal (v2_0 = 1)
         const double2 t2 = cconj(Rf.tau);
         const int c = i;
-        double2 col[8], zc = make_double2(0, 0);
+        double2 col[8], v2r[8];
 #pragma unroll
         for (int rr = 0; rr < 8; ++rr) {
           const int r = 8 * h + rr;
           col[rr] = (c >= 1 && c < len && r < len2) ? at(q + r, p + c) : make_double2(0, 0);
+          v2r[rr] = r == 0 ? make_double2(1, 0) : (r < len2 ? cmul(wv[kNB + r], Rf.scal) : make_double2(0, 0));
         }
+        double2 z0 = make_double2(0, 0), z1 = make_double2(0, 0);
 #pragma unroll
-        for (int rr = 0; rr < 8; ++rr) zc = cadd(zc, cmulc(wv[8 * h + rr], col[rr]));
+        for (int rr = 0; rr < 8; rr += 2) {
+          z0 = cadd(z0, cmulc(v2r[rr], col[rr]));
+          z1 = cadd(z1, cmulc(v2r[rr + 1], col[rr + 1]));
+        }
+        double2 zc = cadd(z0, z1);
         zc.x += __shfl_xor_sync(0xffffffffu, zc.x, 16);
         zc.y += __shfl_xor_sync(0xffffffffu, zc.y, 16);
         const double2 tz = cmul(t2, zc);
 #pragma unroll
         for (int rr = 0; rr < 8; ++rr) {
           const int r = 8 * h + rr;
-          if (c >= 1 && c < len && r < len2) at(q + r, p + c) = csub(col[rr], cmul(wv[r], tz));
+          if (c >= 1 && c < len && r < len2) at(q + r, p + c) = csub(col[rr], cmul(v2r[rr], tz));
         }
         if (h == 0) {
-          // staged: the D warp of this task may still be reading the sweep's slot
-          v2s[(s % kSlots) * kNB + i] = i == 0 ? Rf.tau : v2;
+          // the pair's next step reads the other slot buffer
+          const double2 v2 = i == 0 ? make_double2(1, 0) : (i < len2 ? cmul(wv[kNB + i], Rf.scal) : make_double2(0, 0));
+          double2* nx = sl + ((j + 1) & 1) * 17;
+          nx[i] = v2;
+          if (i == 0) nx[16] = Rf.tau;
           R[(ridx + j + 1) * kNB + i] = i == 0 ? Rf.tau : v2;
         }
       }
-      __syncwarp();  // wv is rewritten by this warp's next task
-    }
-    __syncthreads();
-    // every task of this time step is done: the new reflectors move into
-    // their sweeps' slots, and the first task of the newest sweep writes its
-    // column (beta, zeros below), which no task of this step read after it
-    for (int s = smax - (tid >> 4); s >= smin; s -= kS2Thr / 16) {
-      const int j = t - kLag * s;
-      const int p = s + 1 + kNB * j, len = min(kNB, ld - p), q = p + len;
-      const int k = tid & 15;
-      double2* sl = slot + (s % kSlots) * 17;
-      if (q < ld) {
-        const double2 val = v2s[(s % kSlots) * kNB + k];
-        if (k == 0) {
-          sl[16] = val;
-          sl[0] = make_double2(1, 0);
-        } else {
-          sl[k] = val;
+      // both warps of the pair are done with this step
+      asm volatile("bar.sync %0, 64;" ::"r"(1 + pair) : "memory");
+      if (!ewarp) {
+        // column s after its reflector: beta, zeros below (nothing reads it
+        // before the tridiagonal is extracted)
+        if (j == 0 && lane < len) Bd[(size_t)s * kBandLd + 1 + lane] = lane == 0 ? make_double2(beta, 0) : make_double2(0, 0);
+        __syncwarp();
+        if (lane == 0) {
+          __threadfence_block();
+          st_release_shared(&prog[pair], s * kProgStride + j + 1);
         }
       }
-      if (j == 0 && k < len) at(p + k, s) = k == 0 ? make_double2(bst[s % kSlots], 0) : make_double2(0, 0);
     }
-    __syncthreads();
   }
-  // tridiagonal T after the reflectors above: d real, e real (beta)
+  __syncthreads();
+  // tridiagonal T after the reflectors above: d real, e real (beta); the
+  // unused e[ld - 1] carries the wait status (1: a wait gave up)
   double* de = reinterpret_cast<double*>(R + ceil_sum(ld - 1) * kNB);
   for (int c = tid; c < ld; c += kS2Thr) {
     de[c] = Bd[(size_t)c * kBandLd].x;
-    de[ld + c] = c + 1 < ld ? Bd[(size_t)c * kBandLd + 1].x : 0.0;
+    de[ld + c] = c + 1 < ld ? Bd[(size_t)c * kBandLd + 1].x : (*err ? 1.0 : 0.0);
   }
 }
 
@@ -682,11 +748,17 @@ constexpr int kTriThr = 256;
 __host__ __device__ inline size_t tri_smem_bytes(int n, int nval, int nvec) {
   return sizeof(double) * ((size_t)3 * n + 8 + 3 * nval + kTriThr) + sizeof(int) * ((size_t)kTriThr + nvec + 1 + 4);
 }
+// with the inverse-iteration iterates in shared memory (n * nvec doubles after
+// the work arrays), when three CTAs still share an SM
+__host__ __device__ inline size_t tri_smem_xbytes(int n, int nval, int nvec) {
+  return (tri_smem_bytes(n, nval, nvec) + 7) / 8 * 8 + sizeof(double) * (size_t)n * nvec;
+}
+constexpr size_t kTriXsmMax = 72 * 1024;
 
 __global__ void __launch_bounds__(kTriThr) tri_eig_kernel(const EigItem* __restrict__ items,
                                                      const double2* __restrict__ rbuf, double* __restrict__ wbuf,
                                                      double2* __restrict__ zbuf, double* __restrict__ scratch,
-                                                     int* __restrict__ info) {
+                                                     int* __restrict__ info, int xsm_ok) {
   const EigItem it = items[blockIdx.x];
   const int n = it.n, ld = it.ld, nval = it.nval, nvec = it.want_vec ? it.nev : 0;
   const int tid = threadIdx.x;
@@ -708,9 +780,14 @@ __global__ void __launch_bounds__(kTriThr) tri_eig_kernel(const EigItem* __restr
     e[c] = c + 1 < n ? de[ld + c] : 0.0;
   }
   __syncthreads();
+  if (de[2 * ld - 1] != 0.0) {  // the bulge chase gave up a wait: T is incomplete
+    if (tid == 0) info[blockIdx.x] = 3;
+    return;
+  }
   const TriWork tw{d, e, e2, red, lam, lo, hi, xs, cnt, clus, misc};
   const int status = tri_eigvals(tw, n, nval, wbuf + it.w_off, it.bisect_cap);
-  if (nvec > 0 && status == 0) tri_eigvecs(tw, n, nvec, zbuf + it.z_off, scratch + it.s_off, blockIdx.x);
+  double* xsm = xsm_ok ? reinterpret_cast<double*>(smraw + (tri_smem_bytes(n, nval, nvec) + 7) / 8 * 8) : nullptr;
+  if (nvec > 0 && status == 0) tri_eigvecs(tw, n, nvec, zbuf + it.z_off, scratch + it.s_off, blockIdx.x, xsm);
   if (tid == 0) info[blockIdx.x] = status;
 }
 
@@ -916,10 +993,11 @@ cudaError_t launch_heev2(const EigItem* items, int nitems, int max_n, int max_nv
   e = cudaFuncSetAttribute(sbtrd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2);
   if (e != cudaSuccess) return e;
   sbtrd_kernel<<<nitems, kS2Thr, s2, st>>>(items, hbuf, rbuf);
-  const size_t s3 = tri_smem_bytes(max_n, max_nval, max_nvec);
+  const int xsm_ok = tri_smem_xbytes(max_n, max_nval, max_nvec) <= kTriXsmMax ? 1 : 0;
+  const size_t s3 = xsm_ok ? tri_smem_xbytes(max_n, max_nval, max_nvec) : tri_smem_bytes(max_n, max_nval, max_nvec);
   e = cudaFuncSetAttribute(tri_eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s3);
   if (e != cudaSuccess) return e;
-  tri_eig_kernel<<<nitems, kTriThr, s3, st>>>(items, rbuf, wbuf, zbuf, scratch, info);
+  tri_eig_kernel<<<nitems, kTriThr, s3, st>>>(items, rbuf, wbuf, zbuf, scratch, info, xsm_ok);
   if (max_nvec > 0) {
     const int vb = back_vec_block(ld, max_nvec);
     const size_t s4 = back_smem_bytes(ld, vb);

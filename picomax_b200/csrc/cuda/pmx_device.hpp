@@ -43,6 +43,8 @@ struct EigItem {
                       // n..ld-1 of the workspace are zero when ld > n
   long long r_off;    // double2 offset of the two-stage path's band reflectors (heev2_rbuf_double2)
   int bisect_cap;     // rounds of the eigenvalue bisection at most (0: the default cap; tests set 1)
+  long long wait_ns;  // limit of one bounded wait of the two-stage bulge chase (0: 2 s)
+  int wait_fault;     // tests only: 1 makes the bulge chase's sweep 1 wait for progress never made
 };
 
 // Fills H(k) of every item (full Hermitian storage, leading dimension

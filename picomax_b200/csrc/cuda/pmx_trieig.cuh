@@ -17,7 +17,6 @@
 #include <cuda_runtime.h>
 
 #include "pmx_common.cuh"
-#include "pmx_tri.cuh"
 
 namespace pmx {
 namespace dev {
@@ -174,15 +173,106 @@ __device__ inline int tri_eigvals(const TriWork& W, int n, int nval, double* __r
   return !(finite && finite_t) ? 2 : (!converged ? 1 : 0);
 }
 
+// LU factors of T - lam I with partial pivoting (the U factor has two
+// super-diagonals), for repeated solves: per row i the multiplier f (its
+// lowest mantissa bit set when rows i and i + 1 were swapped, a change of one
+// unit in the last place of f), 1 / pivot, and U's two super-diagonals, each
+// array at [i * st] (several threads' arrays interleaved).
+__device__ inline void tri_factor(const double* __restrict__ d, const double* __restrict__ e, int n, double lam,
+                                  double tiny, double* __restrict__ F, double* __restrict__ I0,
+                                  double* __restrict__ U1, double* __restrict__ U2, int st) {
+  double a = d[0] - lam;          // current pivot-row diagonal
+  double c = n > 1 ? e[0] : 0.0;  // current pivot-row super-diagonal
+  for (int i = 0; i < n - 1; ++i) {
+    const double b = e[i], dn = d[i + 1] - lam, en = i + 1 < n - 1 ? e[i + 1] : 0.0;
+    const size_t o = (size_t)i * st;
+    if (fabs(a) >= fabs(b)) {
+      if (a == 0.0) a = tiny;
+      const double ia = 1.0 / a, f = b * ia;
+      F[o] = __longlong_as_double(__double_as_longlong(f) & ~1ll);
+      I0[o] = ia;
+      U1[o] = c;
+      U2[o] = 0.0;
+      a = dn - f * c;
+      c = en;
+    } else {  // swap rows i and i + 1
+      const double ib = 1.0 / b, f = a * ib;
+      F[o] = __longlong_as_double(__double_as_longlong(f) | 1ll);
+      I0[o] = ib;
+      U1[o] = dn;
+      U2[o] = en;
+      a = c - f * dn;
+      c = -f * en;
+    }
+  }
+  if (a == 0.0 || fabs(a) < tiny) a = a < 0 ? -tiny : tiny;
+  I0[(size_t)(n - 1) * st] = 1.0 / a;
+}
+
+// Solves (T - lam I) x = b in place with the factors of tri_factor: x (b on
+// entry) at xb[i * xs]. Division-free; the loads run eight rows ahead of the
+// recurrences.
+__device__ inline void tri_factored_solve(const double* __restrict__ F, const double* __restrict__ I0,
+                                          const double* __restrict__ U1, const double* __restrict__ U2, int st, int n,
+                                          double* __restrict__ xb, int xs) {
+  constexpr int kB = 8;
+  double xc = xb[0];
+  for (int i0 = 0; i0 < n - 1; i0 += kB) {
+    double xv[kB], fv[kB];
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      const int i = i0 + u;
+      xv[u] = i + 1 < n ? xb[(size_t)(i + 1) * xs] : 0.0;
+      fv[u] = i + 1 < n ? F[(size_t)i * st] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      const int i = i0 + u;
+      if (i + 1 < n) {
+        const bool sw = (__double_as_longlong(fv[u]) & 1ll) != 0;
+        const double piv = sw ? xv[u] : xc, oth = sw ? xc : xv[u];
+        xb[(size_t)i * xs] = piv;
+        xc = oth - fv[u] * piv;
+      }
+    }
+  }
+  double x1 = xc * I0[(size_t)(n - 1) * st], x2 = 0.0;  // rows i + 1, i + 2
+  xb[(size_t)(n - 1) * xs] = x1;
+  for (int i0 = n - 2; i0 >= 0; i0 -= kB) {
+    double yv[kB], iv[kB], av[kB], bv[kB];
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      const int i = i0 - u;
+      yv[u] = i >= 0 ? xb[(size_t)i * xs] : 0.0;
+      iv[u] = i >= 0 ? I0[(size_t)i * st] : 0.0;
+      av[u] = i >= 0 ? U1[(size_t)i * st] : 0.0;
+      bv[u] = i >= 0 ? U2[(size_t)i * st] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      const int i = i0 - u;
+      if (i >= 0) {
+        const double xi = (yv[u] - av[u] * x1 - bv[u] * x2) * iv[u];
+        xb[(size_t)i * xs] = xi;
+        x2 = x1;
+        x1 = xi;
+      }
+    }
+  }
+}
+
 // Lowest nvec eigenvectors of T (after tri_eigvals) as real vectors in the
 // real parts of z[k * n + i] (imaginary parts zero). Clusters of eigenvalues
-// closer than 1e-5 |T| are reorthogonalised. One thread per cluster; the four
-// work arrays of the clusters are interleaved in `scratch` (element i of
-// cluster cl at [i * ncl + cl], 4 n nvec doubles at most) so that the threads
-// of a warp, which step through the rows together, read and write consecutive
-// addresses. `seed` makes the pseudo-random start vectors differ per matrix.
+// closer than 1e-5 |T| are reorthogonalised. One thread per cluster: per
+// eigenvalue one LU factorisation of T - lam I (tri_factor, its four arrays
+// interleaved by cluster in `scratch`, 4 n nvec doubles at most), then
+// kTriInvIters division-free solves from a pseudo-random start. The iterate
+// lives in shared memory when xsm is given (n * nvec doubles, interleaved by
+// cluster), else in the real parts of its z column. `seed` makes the start
+// vectors differ per matrix.
 __device__ inline void tri_eigvecs(const TriWork& W, int n, int nvec, double2* __restrict__ z,
-                                   double* __restrict__ scratch, unsigned long long seed) {
+                                   double* __restrict__ scratch, unsigned long long seed,
+                                   double* __restrict__ xsm = nullptr) {
   const int tid = threadIdx.x, nthr = blockDim.x;
   const double* d = W.d;
   const double* e = W.e;
@@ -200,27 +290,33 @@ __device__ inline void tri_eigvecs(const TriWork& W, int n, int nvec, double2* _
   const int ncl = W.misc[0];
   const double tiny = DBL_EPSILON * fmax(tnorm, DBL_MIN);
   for (int cl = tid; cl < ncl; cl += nthr) {
-    double* u0 = scratch + cl;
-    double* u1 = u0 + (size_t)n * ncl;
-    double* u2 = u1 + (size_t)n * ncl;
-    double* x = u2 + (size_t)n * ncl;
-    auto X = [&](int i) -> double& { return x[(size_t)i * ncl]; };
+    double* F = scratch + cl;
+    double* I0 = F + (size_t)n * ncl;
+    double* U1 = I0 + (size_t)n * ncl;
+    double* U2 = U1 + (size_t)n * ncl;
     for (int k = W.clus[cl]; k < W.clus[cl + 1]; ++k) {
+      double* xb = xsm ? xsm + cl : reinterpret_cast<double*>(z + (size_t)k * n);
+      const int xs = xsm ? ncl : 2;
+      auto X = [&](int i) -> double& { return xb[(size_t)i * xs]; };
+      tri_factor(d, e, n, lam[k], tiny, F, I0, U1, U2, ncl);
       for (int i = 0; i < n; ++i) X(i) = hash_uniform((seed << 20) + k, i);
       for (int iter = 0; iter < kTriInvIters; ++iter) {
-        tri_solve(d, e, n, lam[k], tiny, x, u0, u1, u2, ncl);
+        tri_factored_solve(F, I0, U1, U2, ncl, n, xb, xs);
         for (int kp = W.clus[cl]; kp < k; ++kp) {
           const double2* zp = z + (size_t)kp * n;
           double s = 0.0;
           for (int i = 0; i < n; ++i) s += zp[i].x * X(i);
           for (int i = 0; i < n; ++i) X(i) -= s * zp[i].x;
         }
-        double s = 0.0, mx = 0.0;
+        double mx = 0.0;
         for (int i = 0; i < n; ++i) mx = fmax(mx, fabs(X(i)));
         if (!(mx > 0.0) || !isfinite(mx)) mx = 1.0;
+        const double imx = 1.0 / mx;
+        double s = 0.0;
         for (int i = 0; i < n; ++i) {
-          X(i) /= mx;
-          s += X(i) * X(i);
+          const double v = X(i) * imx;
+          X(i) = v;
+          s += v * v;
         }
         s = 1.0 / sqrt(s);
         for (int i = 0; i < n; ++i) X(i) *= s;

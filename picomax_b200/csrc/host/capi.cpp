@@ -249,8 +249,8 @@ struct pmx_ctx {
   // device times measured when it was chosen
   bool autotune = true;
   int fixed_schedule = -1;  // >= 0: this eigensolver schedule on every batch (clamped to the last one)
-  long long wait_ns = 0;    // limit of the mixed contraction's bounded device waits (0: the kernel's 2 s)
-  int fault = 0;            // tests only: fault injected into the mixed contraction (see pmx_ctx_set_fault)
+  long long wait_ns = 0;    // limit of the bounded device waits (0: the kernels' 2 s)
+  int fault = 0;            // tests only: injected fault (see pmx_ctx_set_fault)
   std::map<long long, int> heev_choice;
   std::map<long long, std::vector<float>> heev_trials;
   // named workspaces
@@ -408,6 +408,14 @@ int eig_ld(int n, int max_n, bool tri) { return use_two_stage(max_n, tri) ? pmx:
 size_t eig_rstride(int n, int max_n, bool tri) {
   return use_two_stage(max_n, tri) ? pmx::dev::heev2_rbuf_double2(pmx::dev::heev2_ld(n)) : 0;
 }
+// the context's wait limit and test fault hooks on an eigensolver item
+void eig_hooks(const pmx_ctx* c, pmx::dev::EigItem& it) {
+  it.bisect_cap = c->fault == 2 ? 1 : 0;
+  it.wait_ns = c->wait_ns;
+  it.wait_fault = c->fault == 3 ? 1 : 0;
+}
+// status of a failed eigensolve: 3 = a bounded wait of the bulge chase gave up
+int eig_status_error(int status) { return status == 3 ? PMX_ERR_TIMEOUT : PMX_ERR_NOCONV; }
 cudaError_t eig_launch(pmx_ctx* c, const pmx::dev::EigItem* items, int nitems, int max_n, int max_nval,
                        int max_nvec, double2* hbuf, double* wbuf, double2* zbuf, double* scratch, int* info,
                        int variant, double* tri = nullptr) {
@@ -470,7 +478,7 @@ void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int 
       it.s_off = per_item ? (long long)(i * sstride) : 0;
       it.ld = ld;
       it.r_off = (long long)(i * rstride);
-      it.bisect_cap = c->fault == 2 ? 1 : 0;
+      eig_hooks(c, it);
     }
     h2d(c, c->items, items.data(), sizeof(pmx::dev::EigItem) * cnt);
     {
@@ -523,7 +531,7 @@ void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int 
       if (info[i] != 0)
         throw CudaFail("eigensolver failed (status " + std::to_string(info[i]) + ") at k-point " +
                            std::to_string(k0 + i),
-                       PMX_ERR_NOCONV);
+                       eig_status_error(info[i]));
   }
   CK(cudaMemcpyAsync(w.data(), c->wbuf.ptr, sizeof(double) * w.size(), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -649,7 +657,7 @@ extern "C" int pmx_heev_batched(pmx_ctx* ctx, int n, int batch, const double* A,
       items[i].s_off = (long long)(i * sstride);
       items[i].ld = ld;
       items[i].r_off = (long long)(i * rstride);
-      items[i].bisect_cap = ctx->fault == 2 ? 1 : 0;
+      eig_hooks(ctx, items[i]);
     }
     if (batch == 0) return (int)PMX_OK;
     if (ld == n) {
@@ -677,7 +685,9 @@ extern "C" int pmx_heev_batched(pmx_ctx* ctx, int n, int batch, const double* A,
                          ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     for (int i = 0; i < batch; ++i)
-      if (info[i]) throw CudaFail("eigensolver failed for matrix " + std::to_string(i), PMX_ERR_NOCONV);
+      if (info[i])
+        throw CudaFail("eigensolver failed (status " + std::to_string(info[i]) + ") for matrix " + std::to_string(i),
+                       eig_status_error(info[i]));
     return (int)PMX_OK;
   });
 }
@@ -1340,7 +1350,7 @@ extern "C" int pmx_ctx_set_wait_limit(pmx_ctx* c, long long ns) {
 }
 
 extern "C" int pmx_ctx_set_fault(pmx_ctx* c, int fault) {
-  if (!c || fault < 0 || fault > 2) return PMX_ERR_INVALID;
+  if (!c || fault < 0 || fault > 3) return PMX_ERR_INVALID;
   c->fault = fault;
   return PMX_OK;
 }
@@ -2117,7 +2127,7 @@ void solve_multi(pmx_ctx* c, const pmx::dev::CrystalDev* table, std::vector<Solv
       it.s_off = sc;
       it.ld = eig_ld(r.n, max_n, false);
       it.r_off = rb;
-      it.bisect_cap = c->fault == 2 ? 1 : 0;
+      eig_hooks(c, it);
       h += (long long)it.ld * it.ld;
       rb += (long long)eig_rstride(r.n, max_n, false);
       ch.max_nvec = std::max(ch.max_nvec, r.nvec);
@@ -2215,7 +2225,7 @@ void solve_multi(pmx_ctx* c, const pmx::dev::CrystalDev* table, std::vector<Solv
   c->d2h += (long long)(sizeof(int) * nitems + sizeof(double) * wv.size());
   for (int i = 0; i < nitems; ++i) {
     if (info[i] != 0)
-      throw CudaFail("eigensolver failed (status " + std::to_string(info[i]) + ")", PMX_ERR_NOCONV);
+      throw CudaFail("eigensolver failed (status " + std::to_string(info[i]) + ")", eig_status_error(info[i]));
     const SolveReq& r = reqs[order[i]];
     std::copy(wv.begin() + items[i].w_off, wv.begin() + items[i].w_off + r.nval, r.w);
   }

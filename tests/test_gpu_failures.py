@@ -6,6 +6,10 @@
   tensor memory and return) and the context computes correctly afterwards;
 * eigensolver: a bisection capped at one round reports non-convergence
   (PMX_ERR_NOCONV, the reference's abort() at src/pmx_epm.cpp:233);
+* two-stage eigensolver: a test hook makes the bulge chase's second sweep wait
+  for progress that never comes; with a short limit the bounded wait gives up
+  and the call returns PMX_ERR_TIMEOUT, and the context solves correctly
+  afterwards;
 * non-finite form factors give non-finite eigenvalues: PMX_ERR_NOCONV;
 * the CLI exits non-zero when it cannot write its output.
 """
@@ -54,6 +58,26 @@ def test_bisection_cap_returns_noconv(name, tmp_path):
     assert np.max(np.abs(c.band(p).ravel() - g["dat"])) < 1e-9
     c.close()
     p.close()
+
+
+def test_bulge_chase_wait_timeout_returns_status():
+    rng = np.random.default_rng(5)
+    n, b, nev = 274, 4, 17
+    A = rng.standard_normal((b, n, n)) + 1j * rng.standard_normal((b, n, n))
+    A = (A + A.conj().transpose(0, 2, 1)) / 2
+    c = pm.Context(0)
+    c.set_schedule(0)  # the two-stage solver
+    c.set_wait_limit(1_000_000)  # 1 ms
+    c.set_fault(3)
+    with pytest.raises(pm.PicomaxError) as e:
+        c.heev(A, nev)
+    assert e.value.status == pm.PMX_ERR_TIMEOUT
+    c.set_fault(0)
+    c.set_wait_limit(0)
+    w, _ = c.heev(A, nev)
+    for i in range(b):
+        assert np.abs(w[i] - np.linalg.eigvalsh(A[i])[:nev]).max() < 1e-10 * np.abs(A[i]).max() * n
+    c.close()
 
 
 def test_nonfinite_form_factor_returns_noconv():
