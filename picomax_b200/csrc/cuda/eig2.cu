@@ -792,14 +792,14 @@ __global__ void __launch_bounds__(kTriThr) tri_eig_kernel(const EigItem* __restr
 }
 
 // ----------------------------------------------------------- back-transform
-constexpr int kChunk = 32;  // panel rows per staged chunk of the stage-1 back-transform
+constexpr int kPfSweeps = 4;  // the band reflectors are prefetched into L2 this many sweeps ahead
 
 __host__ __device__ inline size_t back_smem_bytes(int ld, int vb) {
-  // Z [ld][vb], one sweep's reflectors [2][ceil(ld/16)][16], panel chunks
-  // [2][kChunk][16], W [16][vb], T [16][17]
-  return sizeof(double2) *
-         ((size_t)ld * vb + 2 * ((ld + kNB - 1) / kNB) * kNB + 2 * kChunk * kNB + kNB * vb + kNB * 17);
+  // Z [ld][vb], one sweep's reflectors [2][ceil(ld/16)][16], W [16][vb], T [16][17]
+  return sizeof(double2) * ((size_t)ld * vb + 2 * ((ld + kNB - 1) / kNB) * kNB + kNB * vb + kNB * 17);
 }
+// reflector entries of a sweep that one thread stages (ceil(416 / 16) * 16 / 256)
+constexpr int kBackStage = 2;
 // eigenvectors per back-transform CTA: up to kVecBlock, and few enough that
 // two CTAs share an SM (the stage is latency-bound)
 inline int back_vec_block(int ld, int max_nvec) {
@@ -808,6 +808,18 @@ inline int back_vec_block(int ld, int max_nvec) {
   return vb;
 }
 
+// element r of column i of a panel's explicit V (unit diagonal, zeros above;
+// below the diagonal the reflectors that stage 1 left in place)
+__device__ __forceinline__ double2 panel_v(const double2* __restrict__ vcol, int r, int i) {
+  return r > i ? __ldg(vcol + r) : make_double2(r == i ? 1.0 : 0.0, 0.0);
+}
+
+// Z (the eigenvectors of T, in shared memory) -> eigenvectors of H. The band
+// reflectors of a sweep are prefetched into L2 kPfSweeps sweeps earlier and
+// loaded into registers while the previous sweep is applied, then stored to
+// shared memory (one barrier per sweep); the panels' reflectors are read
+// straight from global memory (the vectors of a CTA all use the same ones,
+// so they come from L1 after the first thread).
 __global__ void __launch_bounds__(kThr, 2) eig2_back_kernel(const EigItem* __restrict__ items,
                                                        const double2* __restrict__ hbuf,
                                                        const double2* __restrict__ rbuf, double2* __restrict__ zbuf,
@@ -825,33 +837,50 @@ __global__ void __launch_bounds__(kThr, 2) eig2_back_kernel(const EigItem* __res
   const int maxsteps = (ld + kNB - 1) / kNB;
   double2* Z = reinterpret_cast<double2*>(smraw);  // Z[r * nv + k]
   double2* RB = Z + (size_t)ld * nv;               // [2][maxsteps * 16]
-  double2* VC = RB + 2 * maxsteps * kNB;           // [2][64][16]
-  double2* W = VC + 2 * kChunk * kNB;              // [16][nv]
+  double2* W = RB + 2 * maxsteps * kNB;            // [16][nv]
   double2* T = W + kNB * nv;                       // [16][17]
   for (int idx = tid; idx < ld * nv; idx += kThr) {
     const int r = idx / nv, k = idx % nv;
     Z[idx] = r < n ? zg[(size_t)(k0 + k) * n + r] : make_double2(0, 0);
   }
-  // ---- band reflectors, sweeps in reverse; one sweep's reflectors act on
-  // disjoint rows and are applied together (one thread per reflector and
-  // vector); the next sweep's reflectors stream in (cp.async) meanwhile
-  auto prefetch = [&](int s, double2* dst) {
-    const int ns = sweep_steps(ld, s);
-    const double2* src = R + sweep_first(ld, s) * kNB;
-    for (int idx = tid; idx < ns * kNB; idx += kThr) cp_async16(dst + idx, src + idx);
-    cp_async_commit();
+  auto prefetch_sweep = [&](int s) {  // one 128-byte line per thread
+    const int lines = sweep_steps(ld, s) * kNB * (int)sizeof(double2) / 128;
+    if (tid < lines)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(R + sweep_first(ld, s) * kNB + tid * (128 / sizeof(double2))));
   };
-  prefetch(ld - 2, RB);
-  cp_async_wait<0>();
+  for (int s = ld - 2; s > ld - 2 - kPfSweeps && s >= 0; --s) prefetch_sweep(s);
+  auto load_sweep = [&](int s, double2 (&st)[kBackStage]) {
+    const int cnt = sweep_steps(ld, s) * kNB;
+    const double2* src = R + sweep_first(ld, s) * kNB;
+#pragma unroll
+    for (int u = 0; u < kBackStage; ++u) {
+      const int idx = tid + u * kThr;
+      st[u] = idx < cnt ? __ldg(src + idx) : make_double2(0, 0);
+    }
+  };
+  auto store_sweep = [&](double2* dst, const double2 (&st)[kBackStage]) {
+#pragma unroll
+    for (int u = 0; u < kBackStage; ++u)
+      if (tid + u * kThr < maxsteps * kNB) dst[tid + u * kThr] = st[u];
+  };
+  {
+    double2 st[kBackStage];
+    load_sweep(ld - 2, st);
+    store_sweep(RB, st);
+  }
   __syncthreads();
+  // ---- band reflectors, sweeps in reverse; one sweep's reflectors act on
+  // disjoint rows and are applied together (one thread per reflector and vector)
   for (int s = ld - 2; s >= 0; --s) {
-    const double2* cur = RB + ((ld - 2 - s) & 1) * maxsteps * kNB;
-    if (s > 0) prefetch(s - 1, RB + ((ld - 1 - s) & 1) * maxsteps * kNB);
+    if (s - kPfSweeps >= 0) prefetch_sweep(s - kPfSweeps);
+    double2 st[kBackStage];
+    if (s > 0) load_sweep(s - 1, st);  // lands while this sweep is applied
     const int ns = sweep_steps(ld, s);
+    const double2* Rs = RB + ((ld - 2 - s) & 1) * maxsteps * kNB;
     for (int task = tid; task < ns * nv; task += kThr) {
       const int j = task / nv, k = task % nv;
       const int p = s + 1 + kNB * j, len = min(kNB, ld - p);
-      const double2* v = cur + j * kNB;
+      const double2* v = Rs + j * kNB;
       const double2 tau = v[0];
       if (tau.x == 0.0 && tau.y == 0.0) continue;
       double2* zc = Z + (size_t)p * nv + k;
@@ -870,61 +899,34 @@ __global__ void __launch_bounds__(kThr, 2) eig2_back_kernel(const EigItem* __res
       for (int q = 1; q < kNB; ++q)
         if (q < len) zc[(size_t)q * nv] = csub(zr[q], cmul(v[q], dot));
     }
-    cp_async_wait<0>();
+    if (s > 0) store_sweep(RB + ((ld - 1 - s) & 1) * maxsteps * kNB, st);
     __syncthreads();
   }
-  // ---- panels in reverse: Z[r0:] -= V (T (V^H Z[r0:])); V streams in
-  // 64-row chunks (cp.async, double-buffered), explicit unit diagonal
-  auto load_chunk = [&](int c0, int r0, int rc, int m, double2* dst) {
-    const int rows = min(kChunk, m - rc);
-    for (int idx = tid; idx < rows * kNB; idx += kThr) {
-      const int r = idx % rows, c = idx / rows;
-      cp_async16(dst + r * kNB + c, A + (size_t)(c0 + c) * ld + r0 + rc + r);
-    }
-    cp_async_commit();
-  };
-  auto fix_chunk = [&](int rc, int rows, double2* dst) {  // rows < 16 of the panel: unit diagonal, zeros above
-    if (rc > 0) return;
-    for (int idx = tid; idx < kNB * kNB; idx += kThr) {
-      const int r = idx / kNB, c = idx % kNB;
-      if (r < rows && r <= c) dst[r * kNB + c] = make_double2(r == c ? 1.0 : 0.0, 0.0);
-    }
-  };
+  // ---- panels in reverse: Z[r0:] -= V (T (V^H Z[r0:]))
   for (int c0 = ld - 2 * kNB; c0 >= 0; c0 -= kNB) {
-    const int r0 = c0 + kNB, m = ld - r0, nch = (m + kChunk - 1) / kChunk;
+    const int r0 = c0 + kNB, m = ld - r0;
     for (int idx = tid; idx < kNB * kNB; idx += kThr) {
       const int i = idx % kNB, j = idx / kNB;
-      T[i * 17 + j] = A[(size_t)(r0 + j) * ld + c0 + i];
+      T[i * 17 + j] = __ldg(A + (size_t)(r0 + j) * ld + c0 + i);
     }
-    // W = V^H Z[r0:]: thread (i, k) over the chunks
-    double2 wacc[2][2] = {{make_double2(0, 0), make_double2(0, 0)}, {make_double2(0, 0), make_double2(0, 0)}};
-    load_chunk(c0, r0, 0, m, VC);
-    for (int ch = 0; ch < nch; ++ch) {
-      double2* cur = VC + (ch & 1) * kChunk * kNB;
-      if (ch + 1 < nch) load_chunk(c0, r0, (ch + 1) * kChunk, m, VC + ((ch + 1) & 1) * kChunk * kNB);
-      if (ch + 1 < nch) cp_async_wait<1>(); else cp_async_wait<0>();
-      __syncthreads();
-      const int rows = min(kChunk, m - ch * kChunk);
-      fix_chunk(ch * kChunk, rows, cur);
-      __syncthreads();
-#pragma unroll
-      for (int o = 0; o < 2; ++o) {
-        const int idx = tid + o * kThr;
-        if (idx < kNB * nv) {
-          const int i = idx / nv, k = idx % nv;
-          const double2* zc = Z + (size_t)(r0 + ch * kChunk) * nv + k;
-          for (int r = 0; r < rows; r += 2) {
-            wacc[o][0] = cadd(wacc[o][0], cmulc(cur[r * kNB + i], zc[(size_t)r * nv]));
-            if (r + 1 < rows) wacc[o][1] = cadd(wacc[o][1], cmulc(cur[(r + 1) * kNB + i], zc[(size_t)(r + 1) * nv]));
-          }
-        }
-      }
-      __syncthreads();
-    }
+    // W = V^H Z[r0:]: thread (i, k), two chains over the rows
 #pragma unroll
     for (int o = 0; o < 2; ++o) {
       const int idx = tid + o * kThr;
-      if (idx < kNB * nv) W[idx] = cadd(wacc[o][0], wacc[o][1]);
+      if (idx < kNB * nv) {
+        const int i = idx / nv, k = idx % nv;
+        const double2* vcol = A + (size_t)(c0 + i) * ld + r0;
+        const double2* zc = Z + (size_t)r0 * nv + k;
+        double2 a0 = make_double2(0, 0), a1 = make_double2(0, 0);
+        int r = i;  // V is zero above its diagonal
+#pragma unroll 4
+        for (; r + 1 < m; r += 2) {
+          a0 = cadd(a0, cmulc(panel_v(vcol, r, i), zc[(size_t)r * nv]));
+          a1 = cadd(a1, cmulc(panel_v(vcol, r + 1, i), zc[(size_t)(r + 1) * nv]));
+        }
+        if (r < m) a0 = cadd(a0, cmulc(panel_v(vcol, r, i), zc[(size_t)r * nv]));
+        W[idx] = cadd(a0, a1);
+      }
     }
     __syncthreads();
     // W <- T W (T upper triangular): thread per column k
@@ -934,35 +936,26 @@ __global__ void __launch_bounds__(kThr, 2) eig2_back_kernel(const EigItem* __res
       for (int i = 0; i < kNB; ++i) w[i] = W[i * nv + k];
 #pragma unroll
       for (int i = 0; i < kNB; ++i) {
-        double2 s = make_double2(0, 0);
+        double2 sacc = make_double2(0, 0);
 #pragma unroll
-        for (int q = i; q < kNB; ++q) s = cadd(s, cmul(T[i * 17 + q], w[q]));
-        W[i * nv + k] = s;
+        for (int q = i; q < kNB; ++q) sacc = cadd(sacc, cmul(T[i * 17 + q], w[q]));
+        W[i * nv + k] = sacc;
       }
     }
-    // Z[r0:] -= V W
-    load_chunk(c0, r0, 0, m, VC);
-    for (int ch = 0; ch < nch; ++ch) {
-      double2* cur = VC + (ch & 1) * kChunk * kNB;
-      if (ch + 1 < nch) load_chunk(c0, r0, (ch + 1) * kChunk, m, VC + ((ch + 1) & 1) * kChunk * kNB);
-      if (ch + 1 < nch) cp_async_wait<1>(); else cp_async_wait<0>();
-      __syncthreads();
-      const int rows = min(kChunk, m - ch * kChunk);
-      fix_chunk(ch * kChunk, rows, cur);
-      __syncthreads();
-      for (int idx = tid; idx < rows * nv; idx += kThr) {
-        const int r = idx / nv, k = idx % nv;
-        double2 s0 = make_double2(0, 0), s1 = make_double2(0, 0);
+    __syncthreads();
+    // Z[r0:] -= V W: thread (row, k)
+    for (int idx = tid; idx < m * nv; idx += kThr) {
+      const int r = idx / nv, k = idx % nv;
+      double2 s0 = make_double2(0, 0), s1 = make_double2(0, 0);
 #pragma unroll
-        for (int i = 0; i < kNB; i += 2) {
-          s0 = cadd(s0, cmul(cur[r * kNB + i], W[i * nv + k]));
-          s1 = cadd(s1, cmul(cur[r * kNB + i + 1], W[(i + 1) * nv + k]));
-        }
-        double2* z = Z + (size_t)(r0 + ch * kChunk + r) * nv + k;
-        *z = csub(*z, cadd(s0, s1));
+      for (int i = 0; i < kNB; i += 2) {
+        s0 = cadd(s0, cmul(panel_v(A + (size_t)(c0 + i) * ld + r0, r, i), W[i * nv + k]));
+        s1 = cadd(s1, cmul(panel_v(A + (size_t)(c0 + i + 1) * ld + r0, r, i + 1), W[(i + 1) * nv + k]));
       }
-      __syncthreads();
+      double2* z = Z + (size_t)(r0 + r) * nv + k;
+      *z = csub(*z, cadd(s0, s1));
     }
+    __syncthreads();
   }
   for (int idx = tid; idx < n * nv; idx += kThr) {
     const int k = idx / n, r = idx % n;
