@@ -249,6 +249,36 @@ int pmx_eps_macroscopic(pmx_ctx* ctx, int neps, int nq, int nfreq, const double*
 int pmx_eels(pmx_ctx* ctx, int nq, int nfreq, double dfreq, double wmin, const double* epsm, double* loss,
              double* plasmon);
 
+/* ------------------------------------------------------------ k-point grids
+ * Symmetry reduction of a Gamma-centred k grid. The reference reads
+ * irreducible point lists with weights from files (import_kpt,
+ * src/pmx_basis.cpp:200-245; include/kpoints/autoGR and kpLib hold lists made
+ * by outside tools) and generates only full grids itself
+ * (src/pmx_basis.cpp:256-650).
+ *
+ * pmx_problem_symmetry (host only): the point-group operations of the
+ * problem's Hamiltonian as integer matrices in the reciprocal basis
+ * (hkl' = M hkl, reduced k coordinates alike), row-major [nops][9], identity
+ * first; ops may be NULL to query nops (at most 96). A lattice operation is
+ * kept when, with some translation, the local and spin-orbit form factors of
+ * every G difference transform as a potential does and the G list maps onto
+ * itself, so that H(k) and H(Rk) have the same spectrum.
+ * PMX_KGRID_TIME_REVERSAL adds -M for every M (E(-k) = E(k));
+ * PMX_KGRID_LITTLE_GROUP_Q keeps the operations that leave the problem's first
+ * q unchanged.
+ *
+ * pmx_kgrid_reduce (device): the irreducible points of the grid
+ * k = sum_j i_j / n_j b_j, 0 <= i_j < n_j, under those operations that map
+ * the grid onto itself. nirr receives their count; idx [nirr][3] their grid
+ * indices (the smallest linear index i0 + n0 (i1 + n1 i2) of each orbit, in
+ * that order) and weight [nirr] the orbit sizes (summing to n0 n1 n2). Pass
+ * idx = weight = NULL to query nirr. */
+#define PMX_KGRID_TIME_REVERSAL 1
+#define PMX_KGRID_LITTLE_GROUP_Q 2
+int pmx_problem_symmetry(const pmx_problem* p, int flags, int* nops, int* ops);
+int pmx_kgrid_reduce(pmx_ctx* ctx, const pmx_problem* p, const int* n, int flags, int* nirr, int* idx,
+                     int* weight);
+
 /* Kramers-Kronig transform of nrows spectra in place, re/im [nrows][nfreq],
  * w_f = dfreq f (kramerskronigtransform, src/pmx_chi.cpp:272-309). */
 int pmx_kk(pmx_ctx* ctx, int nrows, int nfreq, double dfreq, double* re, double* im);

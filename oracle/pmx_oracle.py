@@ -485,6 +485,74 @@ def plasmon_peak(loss: np.ndarray, dfreq: float, fmin: int = 0):
     return w, h
 
 
+# ------------------------------------------------------- symmetry of k grids
+def point_group_ops(cr: Crystal, species, time_reversal: bool = True) -> np.ndarray:
+    """Operations M (integer, reciprocal basis: hkl' = M hkl) of the crystal's
+    point group found by mapping atoms: a lattice operation R = B M B^-1
+    (|M_ij| <= 1, R orthogonal) is kept when some translation t sends every
+    atom tau_s to an atom of the same species modulo the lattice. With time
+    reversal -M is added for every M. Restated independently of the library's
+    search, which tests the form-factor tables instead (equal results for
+    Hamiltonians without spin-orbit coupling). Returns [nops, 3, 3], sorted."""
+    Bm = cr.recip.T                       # columns b_j
+    Bi = np.linalg.inv(Bm)
+    atoms = np.asarray(cr.atoms, float)
+    species = list(species)
+    out = []
+    vals = (-1, 0, 1)
+    for code in range(3 ** 9):
+        M = np.array([vals[(code // 3 ** e) % 3] for e in range(9)], float).reshape(3, 3)
+        R = Bm @ M @ Bi
+        if not np.allclose(R.T @ R, np.eye(3), atol=1e-9):
+            continue
+        found = False
+        for j in range(len(atoms)):
+            t = atoms[j] - R @ atoms[0]
+            ok = True
+            for s_ in range(len(atoms)):
+                img = R @ atoms[s_] + t
+                hit = False
+                for s2 in range(len(atoms)):
+                    if species[s2] != species[s_]:
+                        continue
+                    frac = (img - atoms[s2]) @ cr.recip.T   # coordinates along a_i (a_i . b_j = delta_ij)
+                    if np.allclose(frac, np.round(frac), atol=1e-9):
+                        hit = True
+                        break
+                if not hit:
+                    ok = False
+                    break
+            if ok:
+                found = True
+                break
+        if found:
+            out.append(M.astype(int))
+    if time_reversal:
+        out = out + [-m for m in out]
+    uniq = sorted({tuple(m.ravel()) for m in out})
+    return np.array(uniq, int).reshape(-1, 3, 3)
+
+
+def ibz_reduce(ops, n):
+    """Irreducible points of the Gamma-centred grid k = sum_j i_j / n_j b_j
+    under the operations `ops` ([nops, 3, 3] integer, a group that maps the
+    grid onto itself): each point's representative is the smallest linear
+    index i0 + n0 (i1 + n1 i2) of its orbit. Returns (idx [nirr, 3] in index
+    order, orbit sizes [nirr])."""
+    n = np.asarray(n, np.int64)
+    N = int(n.prod())
+    L = np.arange(N, dtype=np.int64)
+    i = np.stack([L % n[0], (L // n[0]) % n[1], L // (n[0] * n[1])])
+    rep = L.copy()
+    for M in np.asarray(ops, np.int64):
+        j = np.mod(M @ i, n[:, None])
+        rep = np.minimum(rep, j[0] + n[0] * (j[1] + n[1] * j[2]))
+    w = np.bincount(rep, minlength=N)
+    reps = np.nonzero(rep == L)[0]
+    idx = np.stack([reps % n[0], (reps // n[0]) % n[1], reps // (n[0] * n[1])], 1)
+    return idx.astype(np.int32), w[reps].astype(np.int32)
+
+
 # ----------------------------------------------------------------- inputs
 def gvectors(cr: Crystal, gcut: float, first=None):
     """G list of generate_gpt (src/pmx_basis.cpp:29-81): every integer

@@ -6,6 +6,7 @@ The compute path is the in-tree shared library ``lib/libpicomax_b200.so``
 the torch autograd wrapper. There is no CPU implementation of the GPU stages.
 """
 from ._capi import (  # noqa: F401
+    KGRID_TIME_REVERSAL, KGRID_LITTLE_GROUP_Q,
     PREC_FP64, PREC_MIXED, SWITCH_BAND, SWITCH_EPSIJ, SWITCH_EPSLL, SWITCH_EPSXYZ, CLI_PATH, LIB_PATH, Context,
     PicomaxError, Problem, load, run_main, PMX_OK, PMX_ERR_INVALID, PMX_ERR_CUDA, PMX_ERR_NOCONV, PMX_ERR_TIMEOUT,
     PMX_ERR_NO_DEVICE, PMX_ERR_UNSUPPORTED, PMX_ERR_LIMIT)

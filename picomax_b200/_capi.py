@@ -47,7 +47,11 @@ EXPORTS = (
     "pmx_band_batch",
     "pmx_chi_batch",
     "pmx_ctx_occupation_ties",
+    "pmx_problem_symmetry",
+    "pmx_kgrid_reduce",
 )
+
+KGRID_TIME_REVERSAL, KGRID_LITTLE_GROUP_Q = 1, 2
 
 
 class ProblemInfo(ctypes.Structure):
@@ -124,6 +128,8 @@ def load() -> ctypes.CDLL:
         "pmx_chi_batch": (c_int, [c_void_p, c_int, POINTER(c_void_p), c_int, c_int, POINTER(dp), POINTER(dp),
                                   POINTER(dp)]),
         "pmx_ctx_tuning": (c_int, [c_void_p, c_char_p, c_size_t, POINTER(c_size_t)]),
+        "pmx_problem_symmetry": (c_int, [c_void_p, c_int, ip, ip]),
+        "pmx_kgrid_reduce": (c_int, [c_void_p, c_void_p, ip, c_int, ip, ip, ip]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -188,6 +194,16 @@ class Problem:
         W = np.zeros(self.info.nk, np.float64)
         self._lib.pmx_problem_kpoints(self.handle, _dptr(K), _dptr(W))
         return K, W
+
+    def symmetry_ops(self, flags: int = KGRID_TIME_REVERSAL) -> np.ndarray:
+        """Point-group operations [nops, 3, 3] (integer, reciprocal basis; identity first)."""
+        n = c_int()
+        st = self._lib.pmx_problem_symmetry(self.handle, int(flags), ctypes.byref(n), None)
+        if st != PMX_OK:
+            raise PicomaxError(st, "pmx_problem_symmetry failed")
+        ops = np.zeros((n.value, 9), np.int32)
+        self._lib.pmx_problem_symmetry(self.handle, int(flags), ctypes.byref(n), _iptr(ops))
+        return ops.reshape(-1, 3, 3)
 
     def qpoints(self):
         Q = np.zeros((self.info.nq, 3), np.float64)
@@ -406,6 +422,19 @@ class Context:
         st = self._lib.pmx_chi_device(self.handle, prob.handle, switch, precision, c_void_p(re_ptr),
                                       c_void_p(im_ptr), c_void_p(epsm_ptr) if epsm_ptr else None)
         self._check(st, "chi_device")
+
+    def kgrid_reduce(self, problem, n, flags: int = KGRID_TIME_REVERSAL):
+        """Irreducible points of the Gamma-centred grid n = (n1, n2, n3) of the
+        problem's reciprocal basis: grid indices [nirr, 3] and orbit sizes [nirr]."""
+        nn = np.ascontiguousarray(n, np.int32)
+        cnt = c_int()
+        self._check(self._lib.pmx_kgrid_reduce(self.handle, problem.handle, _iptr(nn), int(flags),
+                                               ctypes.byref(cnt), None, None), "kgrid_reduce")
+        idx = np.zeros((cnt.value, 3), np.int32)
+        w = np.zeros(cnt.value, np.int32)
+        self._check(self._lib.pmx_kgrid_reduce(self.handle, problem.handle, _iptr(nn), int(flags),
+                                               ctypes.byref(cnt), _iptr(idx), _iptr(w)), "kgrid_reduce")
+        return idx, w
 
     def eels(self, epsm, dfreq: float, wmin: float = 0.0):
         """Loss function -Im(1/eps_M) [nq, nf] and plasmon peaks [nq, 2] (eV,

@@ -518,14 +518,18 @@ __device__ __forceinline__ long long global_ns() {
   return t;
 }
 
-// Waits until *flag >= need. Gives up, and sets *err, after limit_ns, after
-// 2^28 polls, or at once when another warp has given up already.
+// Waits until *flag >= need, polling every ~kPollNs so that a waiting warp
+// leaves the issue slots to the warps that work. Gives up, and sets *err,
+// after limit_ns, after 2^28 polls, or at once when another warp has given
+// up already.
+constexpr unsigned kPollNs = 40;
 __device__ __forceinline__ void wait_progress(const int* flag, int need, int* err, long long limit_ns) {
   if (ld_acquire_shared(flag) >= need) return;
   const long long t0 = global_ns();
   for (int k = 1; k < (1 << 28); ++k) {
+    __nanosleep(kPollNs);
     if (ld_acquire_shared(flag) >= need) return;
-    if ((k & 255) == 0) {
+    if ((k & 63) == 0) {
       if (*reinterpret_cast<volatile int*>(err)) return;
       if (global_ns() - t0 > limit_ns) break;
     }

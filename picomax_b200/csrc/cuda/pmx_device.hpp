@@ -87,5 +87,19 @@ size_t heev2_rbuf_double2(int ld);
 cudaError_t launch_heev2(const EigItem* items, int nitems, int max_n, int max_nval, int max_nvec, double2* hbuf,
                          double* wbuf, double2* zbuf, double* scratch, double2* rbuf, int* info, cudaStream_t st);
 
+// Symmetry reduction of a Gamma-centred n[0] x n[1] x n[2] grid (kgrid.cu):
+// ops are integer matrices in the reciprocal basis (a group, identity
+// included) that map the grid onto itself. rep/cnt: device scratch of
+// n0 n1 n2 ints each; idx [nirr][3] (may be null) and w [nirr] receive the
+// representatives (smallest linear index of each orbit, index order) and
+// their orbit sizes; nirr (device) their count.
+constexpr int kKgridMaxOps = 96;
+struct KgridOps {
+  int n;
+  int m[kKgridMaxOps][9];
+};
+cudaError_t launch_kgrid_reduce(const KgridOps& ops, const int* n, int* rep, int* cnt, int* idx, int* w, int* nirr,
+                                cudaStream_t st);
+
 }  // namespace dev
 }  // namespace pmx

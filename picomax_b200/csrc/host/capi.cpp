@@ -254,7 +254,7 @@ struct pmx_ctx {
   std::map<long long, int> heev_choice;
   std::map<long long, std::vector<float>> heev_trials;
   // named workspaces
-  DevBuf crystal, g, hkl, vloc, vso, items, hbuf, wbuf, zk, zq, scratch, info, rbuf;
+  DevBuf crystal, g, hkl, vloc, vso, items, hbuf, wbuf, zk, zq, scratch, info, rbuf, kgrid;
   DevBuf loci, kpts, uvec, ssoc, qgn, ncd, nvd, cbase, vbase, cidx, vidx, blkoff, dest;
   DevBuf M, dE, wgt, f0, trange, acc, accpv, chi, chi2, mixws, epsm, stats;
   // adjoint workspaces
@@ -1299,6 +1299,71 @@ extern "C" int pmx_eels(pmx_ctx* ctx, int nq, int nfreq, double dfreq, double wm
     CK(cudaMemcpyAsync(plasmon, dp, sizeof(double) * 2 * nq, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->d2h += (long long)(sizeof(double) * (ne + 2 * (size_t)nq));
+    return (int)PMX_OK;
+  });
+}
+
+namespace {
+std::vector<std::array<int, 9>> problem_ops(const pmx_problem* P, int flags) {
+  const pmx::Problem& p = P->p;
+  if ((flags & PMX_KGRID_LITTLE_GROUP_Q) && p.nq() < 1) throw std::runtime_error("the little group of q needs a q point");
+  const pmx::Vec3* q = (flags & PMX_KGRID_LITTLE_GROUP_Q) ? &p.lat.Q[0] : nullptr;
+  return pmx::symmetry_ops(p, (flags & PMX_KGRID_TIME_REVERSAL) != 0, q);
+}
+}  // namespace
+
+extern "C" int pmx_problem_symmetry(const pmx_problem* P, int flags, int* nops, int* ops) {
+  if (!P || !nops) return PMX_ERR_INVALID;
+  try {
+    const auto v = problem_ops(P, flags);
+    *nops = (int)v.size();
+    if (ops)
+      for (size_t o = 0; o < v.size(); ++o)
+        for (int e = 0; e < 9; ++e) ops[9 * o + e] = v[o][e];
+    return PMX_OK;
+  } catch (const std::exception&) {
+    return PMX_ERR_INVALID;
+  }
+}
+
+extern "C" int pmx_kgrid_reduce(pmx_ctx* ctx, const pmx_problem* P, const int* n, int flags, int* nirr, int* idx,
+                                int* weight) {
+  if (!P || !n || !nirr || n[0] <= 0 || n[1] <= 0 || n[2] <= 0 || (idx && !weight) || (!idx && weight))
+    return PMX_ERR_INVALID;
+  const long long N = (long long)n[0] * n[1] * n[2];
+  if (N > (1LL << 28)) return PMX_ERR_LIMIT;
+  return guarded(ctx, [&]() {
+    const auto all = problem_ops(P, flags);
+    // the operations that map this grid onto itself: M_ab != 0 only where n_a = n_b
+    pmx::dev::KgridOps ops{};
+    for (const auto& m : all) {
+      bool ok = true;
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) ok &= m[3 * a + b] == 0 || n[a] == n[b];
+      if (ok && ops.n < pmx::dev::kKgridMaxOps) {
+        for (int e = 0; e < 9; ++e) ops.m[ops.n][e] = m[e];
+        ++ops.n;
+      }
+    }
+    CK(ctx->kgrid.ensure(sizeof(int) * (size_t)(2 * N + 4 * N + 1)));
+    int* rep = ctx->kgrid.as<int>();
+    int* cnt = rep + N;
+    int* didx = cnt + N;
+    int* dw = didx + 3 * N;
+    int* dn = dw + N;
+    {
+      KTime kt(ctx, "kgrid");
+      CK(pmx::dev::launch_kgrid_reduce(ops, n, rep, cnt, didx, dw, dn, ctx->stream));
+    }
+    ctx->launches += 2;
+    CK(cudaMemcpyAsync(nirr, dn, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (idx) {
+      CK(cudaMemcpyAsync(idx, didx, sizeof(int) * 3 * (size_t)*nirr, cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaMemcpyAsync(weight, dw, sizeof(int) * (size_t)*nirr, cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+    }
+    ctx->d2h += (long long)sizeof(int) * (1 + (idx ? 4LL * *nirr : 0));
     return (int)PMX_OK;
   });
 }

@@ -3,6 +3,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <complex>
 #include <cstring>
 #include <filesystem>
 #include <fstream>
@@ -662,6 +664,143 @@ void soc_scalar(const Problem& p, const Vec3& q, double& re, double& im) {
   }
   re = ls * cs;
   im = la * sn;
+}
+
+std::vector<std::array<int, 9>> symmetry_ops(const Problem& p, bool time_reversal, const Vec3* little_q) {
+  if (p.lat.dim != 3 || p.lat.reciprocal.size() != 3)
+    throw std::runtime_error("symmetry operations need a 3D crystal");
+  // columns of Bm are the reciprocal basis vectors: G = Bm hkl
+  double Bm[3][3], Bi[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) Bm[r][c] = p.lat.reciprocal[c][r];
+  {
+    const double det = Bm[0][0] * (Bm[1][1] * Bm[2][2] - Bm[1][2] * Bm[2][1]) -
+                       Bm[0][1] * (Bm[1][0] * Bm[2][2] - Bm[1][2] * Bm[2][0]) +
+                       Bm[0][2] * (Bm[1][0] * Bm[2][1] - Bm[1][1] * Bm[2][0]);
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) {
+        const int r1 = (c + 1) % 3, r2 = (c + 2) % 3, c1 = (r + 1) % 3, c2 = (r + 2) % 3;
+        Bi[r][c] = (Bm[r1][c1] * Bm[r2][c2] - Bm[r1][c2] * Bm[r2][c1]) / det;
+      }
+  }
+  auto gvec = [&](const std::array<int, 3>& h) {
+    Vec3 g;
+    for (int r = 0; r < 3; ++r) g[r] = Bm[r][0] * h[0] + Bm[r][1] * h[1] + Bm[r][2] * h[2];
+    return g;
+  };
+  // the G list (hkl) and its distinct differences
+  std::set<std::array<int, 3>> gset(p.hkl.begin(), p.hkl.end());
+  std::set<std::array<int, 3>> dset;
+  for (const auto& a : p.hkl)
+    for (const auto& b : p.hkl) dset.insert({a[0] - b[0], a[1] - b[1], a[2] - b[2]});
+  std::vector<std::array<int, 3>> diffs(dset.begin(), dset.end());
+  std::vector<std::complex<double>> V(diffs.size()), S(diffs.size());
+  const bool soc = soc_active(p);
+  double vmax = 0, smax = 0;
+  for (size_t d = 0; d < diffs.size(); ++d) {
+    double re, im;
+    const Vec3 dg = gvec(diffs[d]);
+    local_potential(p, dg, re, im);
+    V[d] = {re, im};
+    vmax = std::max(vmax, std::abs(V[d]));
+    if (soc) {
+      soc_scalar(p, (-1.0) * dg, re, im);
+      S[d] = {re, im};
+      smax = std::max(smax, std::abs(S[d]));
+    }
+  }
+  std::map<std::array<int, 3>, size_t> dindex;
+  for (size_t d = 0; d < diffs.size(); ++d) dindex[diffs[d]] = d;
+  auto mat_apply = [](const std::array<int, 9>& M, const std::array<int, 3>& h) {
+    return std::array<int, 3>{M[0] * h[0] + M[1] * h[1] + M[2] * h[2], M[3] * h[0] + M[4] * h[1] + M[5] * h[2],
+                              M[6] * h[0] + M[7] * h[1] + M[8] * h[2]};
+  };
+  std::vector<std::array<int, 9>> ops;
+  std::array<int, 9> M;
+  for (int code = 0; code < 19683; ++code) {
+    int c = code;
+    for (int e = 0; e < 9; ++e) {
+      M[e] = c % 3 - 1;
+      c /= 3;
+    }
+    // R = Bm M Bm^-1 must be orthogonal
+    double R[3][3];
+    for (int r = 0; r < 3; ++r)
+      for (int cc = 0; cc < 3; ++cc) {
+        double acc = 0;
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) acc += Bm[r][a] * M[3 * a + b] * Bi[b][cc];
+        R[r][cc] = acc;
+      }
+    bool orth = true;
+    for (int a = 0; a < 3 && orth; ++a)
+      for (int b = 0; b < 3 && orth; ++b) {
+        double acc = 0;
+        for (int r = 0; r < 3; ++r) acc += R[r][a] * R[r][b];
+        orth = std::abs(acc - (a == b ? 1.0 : 0.0)) < 1e-9;
+      }
+    if (!orth) continue;
+    bool gok = true;
+    for (const auto& h : p.hkl)
+      if (!gset.count(mat_apply(M, h))) {
+        gok = false;
+        break;
+      }
+    if (!gok) continue;
+    // translations: t = tau_j - R tau_0
+    auto rot = [&](const Vec3& v) {
+      Vec3 o;
+      for (int r = 0; r < 3; ++r) o[r] = R[r][0] * v[0] + R[r][1] * v[1] + R[r][2] * v[2];
+      return o;
+    };
+    bool found = false;
+    const int na = std::max(1, (int)p.lat.atomic.size());
+    for (int j = 0; j < na && !found; ++j) {
+      const Vec3 t = p.lat.atomic.empty() ? Vec3{} : p.lat.atomic[j] - rot(p.lat.atomic[0]);
+      bool ok = true;
+      for (size_t d = 0; d < diffs.size() && ok; ++d) {
+        const auto hr = mat_apply(M, diffs[d]);
+        const auto it = dindex.find(hr);
+        if (it == dindex.end()) {
+          ok = false;
+          break;
+        }
+        const double ph = -2.0 * kPi * dot(gvec(hr), t);
+        const std::complex<double> e(std::cos(ph), std::sin(ph));
+        ok = std::abs(V[it->second] - V[d] * e) <= 1e-9 * std::max(vmax, 1e-300) &&
+             (!soc || std::abs(S[it->second] - S[d] * e) <= 1e-9 * std::max(smax, 1e-300));
+      }
+      found = ok;
+    }
+    if (!found) continue;
+    ops.push_back(M);
+  }
+  if (time_reversal) {
+    std::set<std::array<int, 9>> all(ops.begin(), ops.end());
+    for (const auto& m : std::vector<std::array<int, 9>>(ops)) {
+      std::array<int, 9> n;
+      for (int e = 0; e < 9; ++e) n[e] = -m[e];
+      all.insert(n);
+    }
+    ops.assign(all.begin(), all.end());
+  }
+  if (little_q) {  // keep the operations with M kq = kq (kq: reduced coordinates of q)
+    double kq[3];
+    for (int r = 0; r < 3; ++r) kq[r] = Bi[r][0] * little_q->x + Bi[r][1] * little_q->y + Bi[r][2] * little_q->z;
+    std::vector<std::array<int, 9>> keep;
+    for (const auto& m : ops) {
+      double dev = 0;
+      for (int r = 0; r < 3; ++r) dev += std::abs(m[3 * r] * kq[0] + m[3 * r + 1] * kq[1] + m[3 * r + 2] * kq[2] - kq[r]);
+      if (dev <= 1e-9) keep.push_back(m);
+    }
+    ops.swap(keep);
+  }
+  // the identity first, then the order of the codes
+  const std::array<int, 9> id{1, 0, 0, 0, 1, 0, 0, 0, 1};
+  auto itid = std::find(ops.begin(), ops.end(), id);
+  if (itid == ops.end()) throw std::runtime_error("symmetry search lost the identity");
+  std::rotate(ops.begin(), itid, itid + 1);
+  return ops;
 }
 
 bool soc_active(const Problem& p) {

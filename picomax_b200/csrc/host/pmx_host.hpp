@@ -149,6 +149,17 @@ void local_potential(const Problem& p, const Vec3& dG, double& re, double& im);
 void soc_scalar(const Problem& p, const Vec3& q, double& re, double& im);
 bool soc_active(const Problem& p);
 
+// Point-group operations of the problem's Hamiltonian, as integer matrices M
+// in the reciprocal basis (hkl' = M hkl; reduced k coordinates transform the
+// same way), row-major. A lattice operation R (|M_ij| <= 1, R orthogonal) is
+// kept when some translation t (a difference of atomic positions after R)
+// makes the local and spin-orbit form factors over every G difference of the
+// basis satisfy V(R dG) = V(dG) exp(-2 pi i R dG . t), and R maps the G list
+// onto itself: then H(k) and H(Rk) have the same spectrum. time_reversal adds
+// -R for every R (E(-k) = E(k)); little_q keeps only the operations that
+// leave q unchanged. The identity comes first.
+std::vector<std::array<int, 9>> symmetry_ops(const Problem& p, bool time_reversal, const Vec3* little_q);
+
 // Polarisation vectors [L, (T+iP)/sqrt2, (T-iP)/sqrt2] (src/pmx_basis.cpp:798-874),
 // returned as 3 complex 3-vectors: out[i][x] = (re, im).
 void uvec_LT(const Vec3& v, double out[3][3][2]);

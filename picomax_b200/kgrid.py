@@ -37,32 +37,40 @@ def _in_bz(crystal: str, k, f: float) -> bool:
     return not (z > 0.5 / f + tol or y > 1 / s3 + tol or x + y / s3 > 1 / s3 + tol)
 
 
+def _fold_point(crystal: str, b: np.ndarray, i, n, f: float) -> np.ndarray:
+    """Cartesian k of grid index i (indices folded into (-N/2, N/2], then the
+    point moved into the first zone with the 27 lattice shifts)."""
+    j = [ii if ii <= nn // 2 else ii - nn for ii, nn in zip(i, n)]
+    k = (j[0] / n[0]) * b[0] + (j[1] / n[1]) * b[1] + (j[2] / n[2]) * b[2]
+    if not _in_bz(crystal, k, f):
+        for s1 in (-1, 0, 1):
+            for s2 in (-1, 0, 1):
+                for s3_ in (-1, 0, 1):
+                    kk = k + s1 * b[0] + s2 * b[1] + s3_ * b[2]
+                    if _in_bz(crystal, kk, f):
+                        return kk
+    return k
+
+
 def gamma_grid(crystal: str, n1: int, n2: int, n3: int, f: float = math.sqrt(8.0 / 3.0)):
     """Returns (K [N,3], W [N]) of the folded Gamma-centred grid, first index fastest."""
     b = reciprocal(crystal, f)
-    pts = []
-    for i3 in range(n3):
-        for i2 in range(n2):
-            for i1 in range(n1):
-                j = [i if i <= n // 2 else i - n for i, n in ((i1, n1), (i2, n2), (i3, n3))]
-                k = (j[0] / n1) * b[0] + (j[1] / n2) * b[1] + (j[2] / n3) * b[2]
-                if not _in_bz(crystal, k, f):
-                    for s1 in (-1, 0, 1):
-                        done = False
-                        for s2 in (-1, 0, 1):
-                            for s3_ in (-1, 0, 1):
-                                kk = k + s1 * b[0] + s2 * b[1] + s3_ * b[2]
-                                if _in_bz(crystal, kk, f):
-                                    k = kk
-                                    done = True
-                                    break
-                            if done:
-                                break
-                        if done:
-                            break
-                pts.append(k)
+    pts = [_fold_point(crystal, b, (i1, i2, i3), (n1, n2, n3), f)
+           for i3 in range(n3) for i2 in range(n2) for i1 in range(n1)]
     K = np.array(pts, np.float64)
     return K, np.ones(len(K), np.float64)
+
+
+def ibz_grid(ctx, problem, crystal: str, n1: int, n2: int, n3: int, f: float = math.sqrt(8.0 / 3.0),
+             flags: int = 1):
+    """Irreducible wedge of the Gamma-centred grid under the problem's point
+    group (with time reversal by default; flags as pmx_kgrid_reduce), reduced
+    on the device: (K [nirr, 3] folded like gamma_grid, W [nirr] orbit sizes,
+    N = n1 n2 n3 for the kpointfile's first line)."""
+    idx, w = ctx.kgrid_reduce(problem, (n1, n2, n3), flags)
+    b = reciprocal(crystal, f)
+    K = np.array([_fold_point(crystal, b, tuple(int(x) for x in i), (n1, n2, n3), f) for i in idx], np.float64)
+    return K.reshape(-1, 3), w.astype(np.float64), n1 * n2 * n3
 
 
 def write_kfile(path: str, K, W, ntotal: int | None = None) -> None:
