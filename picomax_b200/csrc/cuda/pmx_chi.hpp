@@ -38,6 +38,46 @@ struct OverlapArgs {
   double2* M;             // [T][3 neps][nch]
 };
 
+// Device transition list of one q (trans.cu).
+constexpr int kTransMaxNB = 512;  // NBAND limit (per-thread state lists)
+struct TransSummary {
+  long long T;     // transitions
+  long long nblk;  // (k, c, v) slots of dest
+  int ncd_max, nvd_max;
+  int cuts, ties;  // degenerate NBAND cuts, states within 1e-8 eV of E_ref
+  int f0_lo, f0_hi;
+};
+struct TransArgs {
+  const double* wk;  // [nk][nval] eigenvalues at k (spatial states without SOC)
+  const double* wq;  // [nk][nval] at k+q
+  const double* kw;  // [nk] k-point weights
+  int nk, nval, nband, nh, soc, xyz;
+  double off, w0, df;
+  // per k
+  int *ncd, *nvd, *cbase, *vbase, *cidx, *vidx, *ntr, *nblk;  // cidx/vidx [nk][nband]
+  long long *blkoff, *toff;
+  // transitions in k order
+  long long* rsrc;
+  double *rde, *rw;
+  int* rf0;
+  // sorted by window start
+  long long* dest;  // [nblk] sorted index of (k, c, v), -1 if unused
+  double *de, *wgt;
+  int* f0;
+  int2* trange;     // [nft] transition range of every frequency tile
+  int *cnt, *btot;  // sort scratch (transitions_sort_ints)
+  TransSummary* sum;
+};
+// occupations, counts and offsets; the summary (device) is complete when the
+// stream reaches it
+cudaError_t launch_transitions_count(const TransArgs& a, cudaStream_t st);
+// the list, sorted by window start when asked, and the frequency-tile ranges
+// (window < 0: every tile takes all transitions)
+cudaError_t launch_transitions_fill(const TransArgs& a, const TransSummary& s, bool sort, int nft, int ftile, int nf,
+                                    int window, cudaStream_t st);
+size_t transitions_sort_ints(const TransSummary& s);
+bool transitions_sortable(const TransSummary& s);
+
 struct ContractArgs {
   const double2* M;     // [T][3 neps][nch]
   const double* dE;     // [T]

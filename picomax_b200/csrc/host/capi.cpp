@@ -257,6 +257,7 @@ struct pmx_ctx {
   DevBuf crystal, g, hkl, vloc, vso, items, hbuf, wbuf, zk, zq, scratch, info, rbuf, kgrid;
   DevBuf loci, kpts, uvec, ssoc, qgn, ncd, nvd, cbase, vbase, cidx, vidx, blkoff, dest;
   DevBuf M, dE, wgt, f0, trange, acc, accpv, chi, chi2, mixws, epsm, stats;
+  DevBuf t_wk, t_wq, t_kw, t_ntr, t_nblk, t_toff, t_rsrc, t_rde, t_rw, t_rf0, t_cnt, t_sum;  // device transition list
   // adjoint workspaces
   DevBuf a_chi, a_g, a_gx, a_kk, a_f1, a_f2, a_obar, a_debar, a_mbar, a_zbk, a_zbq, a_lbk, a_lbq;
   DevBuf a_lamk, a_lamq, a_C, a_X, a_R, a_SV, a_SSO, a_kp, a_linv, a_hk, a_trik, a_triq, a_work;
@@ -1018,8 +1019,90 @@ void chi_process_q(pmx_ctx* ctx, const Problem& p, const ChiPlan& pl, const DevC
   const bool pv = pl.pv;
   pmx::dev::ScaleArgs sa = pl.sa;
   const Vec3 Q = p.lat.Q[q];
-  const Transitions& T = build_transitions(p, dc.soc, nval, wk, wq, off, mode == 0, ctx->degenerate_cuts, 0, -1,
-                                    &ctx->occupation_ties, mode == 2);
+  // transition list on the device (trans.cu): occupations and counts, one
+  // read-back of the summary, then the list, its sort by window start and
+  // the frequency-tile ranges
+  pmx::dev::TransArgs ta{};
+  pmx::dev::TransSummary tsum{};
+  {
+    KTime kt(ctx, "transitions");
+    h2d(ctx, ctx->t_wk, wk.data(), sizeof(double) * (size_t)nk * nval);
+    h2d(ctx, ctx->t_wq, wq.data(), sizeof(double) * (size_t)nk * nval);
+    h2d(ctx, ctx->t_kw, p.KW.data(), sizeof(double) * (size_t)nk);
+    const int NB = p.nband;
+    CK(ctx->ncd.ensure(sizeof(int) * nk));
+    CK(ctx->nvd.ensure(sizeof(int) * nk));
+    CK(ctx->cbase.ensure(sizeof(int) * nk));
+    CK(ctx->vbase.ensure(sizeof(int) * nk));
+    CK(ctx->cidx.ensure(sizeof(int) * (size_t)nk * NB));
+    CK(ctx->vidx.ensure(sizeof(int) * (size_t)nk * NB));
+    CK(ctx->t_ntr.ensure(sizeof(int) * nk));
+    CK(ctx->t_nblk.ensure(sizeof(int) * nk));
+    CK(ctx->blkoff.ensure(sizeof(long long) * nk));
+    CK(ctx->t_toff.ensure(sizeof(long long) * nk));
+    CK(ctx->t_sum.ensure(sizeof(pmx::dev::TransSummary)));
+    ta.wk = ctx->t_wk.as<double>();
+    ta.wq = ctx->t_wq.as<double>();
+    ta.kw = ctx->t_kw.as<double>();
+    ta.nk = nk;
+    ta.nval = nval;
+    ta.nband = NB;
+    ta.nh = 2 * p.npw();
+    ta.soc = dc.soc;
+    ta.xyz = mode == 2 ? 1 : 0;
+    ta.off = off;
+    ta.w0 = p.freq.empty() ? 0.0 : p.freq[0];
+    ta.df = p.dfreq;
+    ta.ncd = ctx->ncd.as<int>();
+    ta.nvd = ctx->nvd.as<int>();
+    ta.cbase = ctx->cbase.as<int>();
+    ta.vbase = ctx->vbase.as<int>();
+    ta.cidx = ctx->cidx.as<int>();
+    ta.vidx = ctx->vidx.as<int>();
+    ta.ntr = ctx->t_ntr.as<int>();
+    ta.nblk = ctx->t_nblk.as<int>();
+    ta.blkoff = ctx->blkoff.as<long long>();
+    ta.toff = ctx->t_toff.as<long long>();
+    ta.sum = ctx->t_sum.as<pmx::dev::TransSummary>();
+    CK(pmx::dev::launch_transitions_count(ta, st));
+    CK(cudaMemcpyAsync(&tsum, ta.sum, sizeof(tsum), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    ctx->d2h += (long long)sizeof(tsum);
+    ctx->launches += 2;
+    ctx->degenerate_cuts += tsum.cuts;
+    ctx->occupation_ties += tsum.ties;
+    const bool sort = mode == 0;
+    if (sort && !pmx::dev::transitions_sortable(tsum))
+      throw CudaFail("transition energies span too many frequency steps for the device sort", PMX_ERR_LIMIT);
+    const size_t T0 = (size_t)std::max<long long>(tsum.T, 1);
+    CK(ctx->dest.ensure(sizeof(long long) * (size_t)std::max<long long>(tsum.nblk, 1)));
+    CK(ctx->dE.ensure(sizeof(double) * T0));
+    CK(ctx->wgt.ensure(sizeof(double) * T0));
+    CK(ctx->f0.ensure(sizeof(int) * T0));
+    CK(ctx->t_rsrc.ensure(sizeof(long long) * T0));
+    CK(ctx->t_rde.ensure(sizeof(double) * T0));
+    CK(ctx->t_rw.ensure(sizeof(double) * T0));
+    CK(ctx->t_rf0.ensure(sizeof(int) * T0));
+    CK(ctx->trange.ensure(sizeof(int2) * std::max(nft, 1)));
+    if (sort) CK(ctx->t_cnt.ensure(sizeof(int) * pmx::dev::transitions_sort_ints(tsum)));
+    ta.rsrc = ctx->t_rsrc.as<long long>();
+    ta.rde = ctx->t_rde.as<double>();
+    ta.rw = ctx->t_rw.as<double>();
+    ta.rf0 = ctx->t_rf0.as<int>();
+    ta.dest = ctx->dest.as<long long>();
+    ta.de = ctx->dE.as<double>();
+    ta.wgt = ctx->wgt.as<double>();
+    ta.f0 = ctx->f0.as<int>();
+    ta.trange = ctx->trange.as<int2>();
+    if (sort) {
+      ta.cnt = ctx->t_cnt.as<int>();
+      const long long nb = (long long)tsum.f0_hi - tsum.f0_lo + 1;
+      ta.btot = ta.cnt + (pmx::dev::transitions_sort_ints(tsum) - (size_t)std::max<long long>(nb, 1));
+    }
+    CK(pmx::dev::launch_transitions_fill(ta, tsum, sort, nft, FT, nf, W, st));
+    ctx->launches += tsum.T > 0 ? (sort ? 6 : 2) : 1;
+  }
+  const long long Tn = tsum.T;
   // per-m polarisation and SOC-current tables
   std::vector<double2> uv((size_t)neps * 9), ss((size_t)neps * 3);
   std::vector<double> qg(neps);
@@ -1049,34 +1132,10 @@ void chi_process_q(pmx_ctx* ctx, const Problem& p, const ChiPlan& pl, const DevC
   h2d(ctx, ctx->uvec, uv.data(), sizeof(double2) * uv.size());
   h2d(ctx, ctx->ssoc, ss.data(), sizeof(double2) * ss.size());
   h2d(ctx, ctx->qgn, qg.data(), sizeof(double) * qg.size());
-  h2d(ctx, ctx->ncd, T.ncd.data(), sizeof(int) * T.ncd.size());
-  h2d(ctx, ctx->nvd, T.nvd.data(), sizeof(int) * T.nvd.size());
-  h2d(ctx, ctx->cbase, T.cbase.data(), sizeof(int) * T.cbase.size());
-  h2d(ctx, ctx->vbase, T.vbase.data(), sizeof(int) * T.vbase.size());
-  h2d(ctx, ctx->cidx, T.cidx.data(), sizeof(int) * T.cidx.size());
-  h2d(ctx, ctx->vidx, T.vidx.data(), sizeof(int) * T.vidx.size());
-  h2d(ctx, ctx->blkoff, T.blkoff.data(), sizeof(long long) * T.blkoff.size());
-  h2d(ctx, ctx->dest, T.dest.data(), sizeof(long long) * T.dest.size());
-  h2d(ctx, ctx->dE, T.dE.data(), sizeof(double) * T.dE.size());
-  h2d(ctx, ctx->wgt, T.wgt.data(), sizeof(double) * T.wgt.size());
-  h2d(ctx, ctx->f0, T.f0.data(), sizeof(int) * T.f0.size());
-  // frequency-tile transition ranges
-  std::vector<int2> tr(nft);
-  for (int ft = 0; ft < nft; ++ft) {
-    if (W < 0) {
-      tr[ft] = make_int2(0, (int)T.T);
-    } else {
-      const int flo = ft * FT, fhi = std::min(nf, flo + FT) - 1;
-      const auto b = std::lower_bound(T.f0.begin(), T.f0.end(), flo - W);
-      const auto e = std::upper_bound(T.f0.begin(), T.f0.end(), fhi + W);
-      tr[ft] = make_int2((int)(b - T.f0.begin()), (int)(e - T.f0.begin()));
-    }
-  }
-  h2d(ctx, ctx->trange, tr.data(), sizeof(int2) * tr.size());
   const int A = 3 * neps;
-  CK(ctx->M.ensure(std::max<size_t>(sizeof(double2) * (size_t)T.T * A * nch, 16)));
+  CK(ctx->M.ensure(std::max<size_t>(sizeof(double2) * (size_t)Tn * A * nch, 16)));
   // overlaps
-  if (T.T > 0) {
+  if (Tn > 0) {
     Timer tm(ctx, 1);
     pmx::dev::OverlapArgs oa{};
     oa.n = n;
@@ -1089,8 +1148,8 @@ void chi_process_q(pmx_ctx* ctx, const Problem& p, const ChiPlan& pl, const DevC
     oa.neps = neps;
     oa.nch = nch;
     oa.mode = mode == 2 ? 0 : mode;  // epsxyz: orbital current along x, y, z
-    oa.ncd_max = *std::max_element(T.ncd.begin(), T.ncd.end());
-    oa.nvd_max = *std::max_element(T.nvd.begin(), T.nvd.end());
+    oa.ncd_max = tsum.ncd_max;
+    oa.nvd_max = tsum.nvd_max;
     if (!pmx::dev::overlap_tiles(oa.ncd_max, oa.nvd_max, n, dc.npw, oa.cchunk, oa.vchunk))
       throw CudaFail("overlap tile does not fit in shared memory", PMX_ERR_UNSUPPORTED);
     oa.zk = zk;
@@ -1144,13 +1203,13 @@ void chi_process_q(pmx_ctx* ctx, const Problem& p, const ChiPlan& pl, const DevC
       ctx->launches += 1;
     } else {
       int nl = 0;
-      CK(ctx->mixws.ensure(std::max<size_t>(pmx::dev::mixed_workspace_bytes(ca, (long long)T.T), 16)));
+      CK(ctx->mixws.ensure(std::max<size_t>(pmx::dev::mixed_workspace_bytes(ca, Tn), 16)));
       CK(ctx->stats.ensure(16));
       ca.stats = ctx->stats.as<double>();
       {
         KTime kt(ctx, "contract_mixed");
         long long mm = 0;
-        const cudaError_t e = pmx::dev::launch_contract_mixed(ca, (long long)T.T, ctx->mixws.ptr, nl, st, &mm);
+        const cudaError_t e = pmx::dev::launch_contract_mixed(ca, Tn, ctx->mixws.ptr, nl, st, &mm);
         if (e == cudaErrorTimeout)
           throw CudaFail("mixed contraction: a bounded device wait ran out (the CTAs returned)", PMX_ERR_TIMEOUT);
         CK(e);
