@@ -303,7 +303,8 @@ def measure(name, steps, warmup, fp64_steps, rank, world, dev, with_e2e=True, sc
     err_eps = ((epsm_d - ref_eps).abs().max() / ref_eps.abs().max()).item() if ref_eps is not None else None
     del ref_re, ref_im, ref_eps
     # kernel-family device times over the mixed timed region
-    fams = ["assemble", "heev", "overlap", "contract_mixed", "contract_f64", "scale", "kk", "epsm"]
+    fams = ["assemble", "heev", "transitions", "overlap", "overlap_tc", "contract_mixed", "contract_f64", "scale",
+            "kk", "epsm"]
     k0 = {f: ctx.kernel_time(f) for f in fams}
     l0 = ctx.kernel_launches()
     mma0 = ctx.mixed_mmas()

@@ -103,6 +103,13 @@ int pmx_problem_write_gpt(const pmx_problem* p);
  * waits). */
 int pmx_ctx_set_wait_limit(pmx_ctx* ctx, long long ns);
 
+/* Overlaps of the mixed-precision path (no reference counterpart): 1
+ * (default) on the tensor cores from split TF32 operands (tcgen05 kind::tf32,
+ * FP32 accumulation); 0 in FP64 on the CUDA cores, rounded to FP32; 2 both,
+ * the tensor-core results used and their error against the FP64 ones reported
+ * by pmx_ctx_overlap_error. The FP64 path always uses FP64 overlaps. */
+int pmx_ctx_set_overlap_mode(pmx_ctx* ctx, int mode);
+
 /* Test hooks, no reference counterpart: fault 1 makes the producer warps of
  * the mixed contraction withhold their first A-full arrival, so that the
  * control warp's bounded wait runs out and the timeout path above runs
@@ -111,7 +118,9 @@ int pmx_ctx_set_wait_limit(pmx_ctx* ctx, long long ns);
  * non-convergence (PMX_ERR_NOCONV); fault 3 makes the second sweep of the
  * two-stage eigensolver's bulge chase wait for progress that never comes, so
  * that its bounded wait gives up (PMX_ERR_TIMEOUT; combine with a short
- * pmx_ctx_set_wait_limit). 0 restores normal operation. */
+ * pmx_ctx_set_wait_limit); fault 4 leaves the first chunk of the tensor-core
+ * overlaps uncommitted, so that the wait for its stage runs out
+ * (PMX_ERR_TIMEOUT). 0 restores normal operation. */
 int pmx_ctx_set_fault(pmx_ctx* ctx, int fault);
 
 int pmx_ctx_create(int device, pmx_ctx** out);

@@ -49,6 +49,7 @@ EXPORTS = (
     "pmx_ctx_occupation_ties",
     "pmx_problem_symmetry",
     "pmx_kgrid_reduce",
+    "pmx_ctx_set_overlap_mode",
 )
 
 KGRID_TIME_REVERSAL, KGRID_LITTLE_GROUP_Q = 1, 2
@@ -130,6 +131,7 @@ def load() -> ctypes.CDLL:
         "pmx_ctx_tuning": (c_int, [c_void_p, c_char_p, c_size_t, POINTER(c_size_t)]),
         "pmx_problem_symmetry": (c_int, [c_void_p, c_int, ip, ip]),
         "pmx_kgrid_reduce": (c_int, [c_void_p, c_void_p, ip, c_int, ip, ip, ip]),
+        "pmx_ctx_set_overlap_mode": (c_int, [c_void_p, c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -342,8 +344,14 @@ class Context:
         """Test hooks: 1 = the mixed contraction's producers withhold one arrival
         (its wait runs out), 2 = the eigenvalue bisection stops after one round,
         3 = the two-stage bulge chase's second sweep waits for progress that
-        never comes (its wait runs out); 0 = normal operation."""
+        never comes (its wait runs out), 4 = the tensor-core overlaps leave
+        their first chunk uncommitted (a wait runs out); 0 = normal operation."""
         self._check(self._lib.pmx_ctx_set_fault(self.handle, int(fault)), "set_fault")
+
+    def set_overlap_mode(self, mode: int):
+        """Overlaps of the mixed path: 1 tensor cores (split TF32, default), 0
+        FP64 rounded to FP32, 2 both with the error reported by overlap_error."""
+        self._check(self._lib.pmx_ctx_set_overlap_mode(self.handle, int(mode)), "set_overlap_mode")
 
     def set_schedule(self, schedule: int):
         """Fix the eigensolver schedule for later batches (-1: autotuner)."""

@@ -37,6 +37,7 @@
 
 #include "pmx_common.cuh"
 #include "pmx_mixed.hpp"
+#include "pmx_tc.cuh"
 
 namespace pmx {
 namespace dev {
@@ -65,48 +66,22 @@ __host__ __device__ constexpr int core_off(int r, int k, int rows) {
   return ((k >> 3) * (rows >> 3) + (r >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2;
 }
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
+using tc::global_ns;
+using tc::mbar_arrive;
+using tc::mbar_init;
+using tc::mma_commit;
+using tc::smem_u32;
+using tc::umma_desc;
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
+  return tc::mbar_wait(bar, parity, limit_ns, kWaitLimit);
 }
-
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
-         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
-}
+__device__ __forceinline__ void tc_fence_after() { tc::fence_after(); }
+__device__ __forceinline__ void tc_fence_before() { tc::fence_before(); }
+__device__ __forceinline__ void async_proxy_fence() { tc::async_proxy_fence(); }
 
 // kind::f16 instruction descriptor: BF16 x BF16 -> F32, A and B K-major.
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kN >> 3) << 17) |
                             ((uint32_t)(kM >> 4) << 24);
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ uint64_t global_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Bounded wait on an mbarrier phase: gives up after limit_ns nanoseconds (a
-// healthy wait takes microseconds) or kWaitLimit polls, whichever is first.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
-  const uint32_t a = smem_u32(bar);
-  const uint64_t t0 = global_ns();
-  for (unsigned it = 0; it < kWaitLimit; ++it) {
-    if ((it & 63u) == 63u && global_ns() - t0 > limit_ns) return false;
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (ok) return true;
-  }
-  return false;
-}
 
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
@@ -127,10 +102,6 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t adesc, uint64_t
       : "memory");
 }
 
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
 // Named barrier 1 over the producer warps, returning the OR of v over them
 // (every producer gets the same answer).
 __device__ __forceinline__ bool producers_sync_or(bool v) {
@@ -145,21 +116,6 @@ __device__ __forceinline__ bool producers_sync_or(bool v) {
       : "memory");
   return r != 0;
 }
-
-__device__ __forceinline__ void mma_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                   smem_u32(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void async_proxy_fence() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
 
 // hi/lo split of 8 values into two 16-byte rows of a core matrix:
 // hi = bf16_rn(x), lo = bf16_rn(x - hi), two values per conversion.
@@ -684,8 +640,10 @@ __global__ void m32_error_kernel(const double2* __restrict__ M, const float2* __
 __global__ void m_to_f32_kernel(const double2* __restrict__ M, float2* __restrict__ M32, size_t n,
                                 const double* __restrict__ w, float* __restrict__ w32, long long T) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const double2 v = M[i];
-    M32[i] = make_float2((float)v.x, (float)v.y);
+    if (M) {
+      const double2 v = M[i];
+      M32[i] = make_float2((float)v.x, (float)v.y);
+    }
     if (i < (size_t)T) w32[i] = (float)w[i];
   }
 }
@@ -740,7 +698,8 @@ cudaError_t launch_contract_mixed(const ContractArgs& a, long long T, void* ws, 
   pl.err = reinterpret_cast<int*>(take(sizeof(int) * 4));
   pl.wait_ns = a.wait_ns > 0 ? (uint64_t)a.wait_ns : kWaitNs;
   pl.fault = a.fault;
-  float2* M32 = reinterpret_cast<float2*>(take(sizeof(float2) * (size_t)(T + 1) * A * a.nch));
+  float2* M32 = a.M32 ? const_cast<float2*>(a.M32)
+                      : reinterpret_cast<float2*>(take(sizeof(float2) * (size_t)(T + 1) * A * a.nch));
   if ((size_t)(p - reinterpret_cast<uint8_t*>(ws)) > mixed_workspace_bytes(a, T)) return cudaErrorInvalidValue;
   cudaError_t e;
 #define PMX_CP(dst, src, n)                                                                            \
@@ -761,9 +720,11 @@ cudaError_t launch_contract_mixed(const ContractArgs& a, long long T, void* ws, 
   e = cudaMemsetAsync(a.acc, 0, sizeof(double) * 2 * 9 * (size_t)a.np * a.nf, st);
   if (e != cudaSuccess) return e;
   if (T > 0) {
-    m_to_f32_kernel<<<1184, 256, 0, st>>>(a.M, M32, (size_t)T * A * a.nch, a.wgt, pl.wgt32, T);
+    // FP32 copies of the overlaps (unless they come in FP32) and of the weights
+    m_to_f32_kernel<<<1184, 256, 0, st>>>(a.M32 ? nullptr : a.M, M32, a.M32 ? (size_t)T : (size_t)T * A * a.nch,
+                                          a.wgt, pl.wgt32, T);
     ++nlaunch;
-    if (a.stats) {
+    if (a.stats && a.M) {
       e = cudaMemsetAsync(a.stats, 0, 2 * sizeof(double), st);
       if (e != cudaSuccess) return e;
       m32_error_kernel<<<592, 256, 0, st>>>(a.M, M32, (size_t)T * A * a.nch,

@@ -78,8 +78,22 @@ cudaError_t launch_transitions_fill(const TransArgs& a, const TransSummary& s, b
 size_t transitions_sort_ints(const TransSummary& s);
 bool transitions_sortable(const TransSummary& s);
 
+// Overlaps of the mixed path on the tensor cores (overlap_tc.cu): the same
+// moments as overlap_kernel from split TF32 operands, FP32 results M32[t][3 neps][nch].
+constexpr int kOvlTcMaxN = 128;  // GEMM columns (c, s, w) per CTA
+struct OverlapTcArgs {
+  OverlapArgs a;      // M unused
+  float2* M32;
+  long long wait_ns;  // limit of the bounded mbarrier waits (0: 2 s)
+  int* err;           // set to 1 when a wait ran out
+  int fault;          // tests only: 4 = the first chunk's MMAs are not committed, so that a wait runs out
+};
+cudaError_t launch_overlap_tc(const OverlapTcArgs& t, int nk, cudaStream_t st);
+size_t overlap_tc_smem_bytes(int npw, int neps);
+
 struct ContractArgs {
-  const double2* M;     // [T][3 neps][nch]
+  const double2* M;     // [T][3 neps][nch] (may be null on the mixed path when M32 is given)
+  const float2* M32;    // mixed path: overlaps already in FP32 (tensor-core overlaps), or null
   const double* dE;     // [T]
   const double* wgt;    // [T] k weight times spin multiplicity
   const int* f0;        // [T] window centre int((dE - w0)/dw)
@@ -91,6 +105,7 @@ struct ContractArgs {
   double* acc;          // [2][9][np][nf] Re then Im
   double* acc_pv;       // principal-value accumulators (epsLL, kk = 0) or null
   double* stats;        // mixed path only, optional (device, 2 doubles): max ||M32|^2 - |M|^2|, max |M|^2
+                       // (needs M)
   int pvclass;          // principal-value function: 0 by (i, j) block (epsLL), 3 = 1/dE/(dE^2-w^2) for all (epsxyz)
   long long wait_ns;    // mixed path: limit of every bounded mbarrier wait (0: 2 s)
   int fault;            // mixed path, tests only: 1 = the producers withhold their first A-full arrival,

@@ -251,6 +251,7 @@ struct pmx_ctx {
   int fixed_schedule = -1;  // >= 0: this eigensolver schedule on every batch (clamped to the last one)
   long long wait_ns = 0;    // limit of the bounded device waits (0: the kernels' 2 s)
   int fault = 0;            // tests only: injected fault (see pmx_ctx_set_fault)
+  int overlap_mode = 1;     // mixed path overlaps: 0 FP64 rounded to FP32, 1 tensor cores, 2 both (error check)
   std::map<long long, int> heev_choice;
   std::map<long long, std::vector<float>> heev_trials;
   // named workspaces
@@ -258,6 +259,7 @@ struct pmx_ctx {
   DevBuf loci, kpts, uvec, ssoc, qgn, ncd, nvd, cbase, vbase, cidx, vidx, blkoff, dest;
   DevBuf M, dE, wgt, f0, trange, acc, accpv, chi, chi2, mixws, epsm, stats;
   DevBuf t_wk, t_wq, t_kw, t_ntr, t_nblk, t_toff, t_rsrc, t_rde, t_rw, t_rf0, t_cnt, t_sum;  // device transition list
+  DevBuf m32, tcerr;  // tensor-core overlaps of the mixed path and their wait status
   // adjoint workspaces
   DevBuf a_chi, a_g, a_gx, a_kk, a_f1, a_f2, a_obar, a_debar, a_mbar, a_zbk, a_zbq, a_lbk, a_lbq;
   DevBuf a_lamk, a_lamq, a_C, a_X, a_R, a_SV, a_SSO, a_kp, a_linv, a_hk, a_trik, a_triq, a_work;
@@ -1133,8 +1135,16 @@ void chi_process_q(pmx_ctx* ctx, const Problem& p, const ChiPlan& pl, const DevC
   h2d(ctx, ctx->ssoc, ss.data(), sizeof(double2) * ss.size());
   h2d(ctx, ctx->qgn, qg.data(), sizeof(double) * qg.size());
   const int A = 3 * neps;
-  CK(ctx->M.ensure(std::max<size_t>(sizeof(double2) * (size_t)Tn * A * nch, 16)));
-  // overlaps
+  // overlaps: FP64 (overlap_kernel) for the FP64 contraction, on the tensor
+  // cores (overlap_tc_kernel, split TF32, FP32 results) for the mixed one
+  const bool tc_ovl = precision == PMX_PREC_MIXED && !pv && ctx->overlap_mode != 0;
+  const bool f64_ovl = !tc_ovl || ctx->overlap_mode == 2;
+  if (f64_ovl) CK(ctx->M.ensure(std::max<size_t>(sizeof(double2) * (size_t)Tn * A * nch, 16)));
+  if (tc_ovl) {
+    CK(ctx->m32.ensure(std::max<size_t>(sizeof(float2) * (size_t)Tn * A * nch, 16)));
+    CK(ctx->tcerr.ensure(16));
+    CK(cudaMemsetAsync(ctx->tcerr.ptr, 0, sizeof(int), st));
+  }
   if (Tn > 0) {
     Timer tm(ctx, 1);
     pmx::dev::OverlapArgs oa{};
@@ -1150,7 +1160,7 @@ void chi_process_q(pmx_ctx* ctx, const Problem& p, const ChiPlan& pl, const DevC
     oa.mode = mode == 2 ? 0 : mode;  // epsxyz: orbital current along x, y, z
     oa.ncd_max = tsum.ncd_max;
     oa.nvd_max = tsum.nvd_max;
-    if (!pmx::dev::overlap_tiles(oa.ncd_max, oa.nvd_max, n, dc.npw, oa.cchunk, oa.vchunk))
+    if (!pmx::dev::overlap_tiles(oa.ncd_max, oa.nvd_max, n, dc.npw, oa.cchunk, oa.vchunk) && f64_ovl)
       throw CudaFail("overlap tile does not fit in shared memory", PMX_ERR_UNSUPPORTED);
     oa.zk = zk;
     oa.zq = zq;
@@ -1170,16 +1180,31 @@ void chi_process_q(pmx_ctx* ctx, const Problem& p, const ChiPlan& pl, const DevC
     oa.q[2] = Q.z;
     oa.uvec = ctx->uvec.as<double2>();
     oa.ssoc = ctx->ssoc.as<double2>();
-    oa.M = ctx->M.as<double2>();
-    KTime kt(ctx, "overlap");
-    CK(pmx::dev::launch_overlap(oa, nk, st));
-    ctx->launches += 1;
+    if (f64_ovl) {
+      oa.M = ctx->M.as<double2>();
+      KTime kt(ctx, "overlap");
+      CK(pmx::dev::launch_overlap(oa, nk, st));
+      ctx->launches += 1;
+    }
+    if (tc_ovl) {
+      pmx::dev::OverlapTcArgs tca{};
+      tca.a = oa;
+      tca.a.M = nullptr;
+      tca.M32 = ctx->m32.as<float2>();
+      tca.wait_ns = ctx->wait_ns;
+      tca.err = ctx->tcerr.as<int>();
+      tca.fault = ctx->fault;
+      KTime kt(ctx, "overlap_tc");
+      CK(pmx::dev::launch_overlap_tc(tca, nk, st));
+      ctx->launches += 1;
+    }
   }
   // contraction
   {
     Timer tm(ctx, 2);
     pmx::dev::ContractArgs ca{};
-    ca.M = ctx->M.as<double2>();
+    ca.M = f64_ovl ? ctx->M.as<double2>() : nullptr;
+    ca.M32 = tc_ovl ? ctx->m32.as<float2>() : nullptr;
     ca.dE = ctx->dE.as<double>();
     ca.wgt = ctx->wgt.as<double>();
     ca.f0 = ctx->f0.as<int>();
@@ -1217,10 +1242,16 @@ void chi_process_q(pmx_ctx* ctx, const Problem& p, const ChiPlan& pl, const DevC
       }
       ctx->launches += nl;
       double sv[2] = {0, 0};
+      int oerr = 0;
       CK(cudaMemcpyAsync(sv, ctx->stats.ptr, sizeof(sv), cudaMemcpyDeviceToHost, st));
+      if (tc_ovl) CK(cudaMemcpyAsync(&oerr, ctx->tcerr.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
-      ctx->m2_err = std::max(ctx->m2_err, sv[0]);
-      ctx->m2_max = std::max(ctx->m2_max, sv[1]);
+      if (oerr)
+        throw CudaFail("tensor-core overlaps: a bounded device wait ran out (the CTAs returned)", PMX_ERR_TIMEOUT);
+      if (f64_ovl) {
+        ctx->m2_err = std::max(ctx->m2_err, sv[0]);
+        ctx->m2_max = std::max(ctx->m2_max, sv[1]);
+      }
     }
   }
   // scaling and Kramers-Kronig
@@ -1473,8 +1504,14 @@ extern "C" int pmx_ctx_set_wait_limit(pmx_ctx* c, long long ns) {
   return PMX_OK;
 }
 
+extern "C" int pmx_ctx_set_overlap_mode(pmx_ctx* c, int mode) {
+  if (!c || mode < 0 || mode > 2) return PMX_ERR_INVALID;
+  c->overlap_mode = mode;
+  return PMX_OK;
+}
+
 extern "C" int pmx_ctx_set_fault(pmx_ctx* c, int fault) {
-  if (!c || fault < 0 || fault > 3) return PMX_ERR_INVALID;
+  if (!c || fault < 0 || fault > 4) return PMX_ERR_INVALID;
   c->fault = fault;
   return PMX_OK;
 }
