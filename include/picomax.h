@@ -103,11 +103,13 @@ int pmx_problem_write_gpt(const pmx_problem* p);
  * waits). */
 int pmx_ctx_set_wait_limit(pmx_ctx* ctx, long long ns);
 
-/* Overlaps of the mixed-precision path (no reference counterpart): 1
- * (default) on the tensor cores from split TF32 operands (tcgen05 kind::tf32,
- * FP32 accumulation); 0 in FP64 on the CUDA cores, rounded to FP32; 2 both,
- * the tensor-core results used and their error against the FP64 ones reported
- * by pmx_ctx_overlap_error. The FP64 path always uses FP64 overlaps. */
+/* Overlaps of the mixed-precision path (no reference counterpart): 3 on the
+ * tensor cores from split TF32 operands (tcgen05 kind::tf32, FP32
+ * accumulation); 0 in FP64 on the CUDA cores, rounded to FP32; 1 (default)
+ * the faster of the two for the problem: the tensor cores without spin-orbit
+ * coupling, FP64 with it; 2 both, the tensor-core results used and their
+ * error against the FP64 ones reported by pmx_ctx_overlap_error. The FP64
+ * path always uses FP64 overlaps. */
 int pmx_ctx_set_overlap_mode(pmx_ctx* ctx, int mode);
 
 /* Test hooks, no reference counterpart: fault 1 makes the producer warps of

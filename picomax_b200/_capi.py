@@ -349,8 +349,10 @@ class Context:
         self._check(self._lib.pmx_ctx_set_fault(self.handle, int(fault)), "set_fault")
 
     def set_overlap_mode(self, mode: int):
-        """Overlaps of the mixed path: 1 tensor cores (split TF32, default), 0
-        FP64 rounded to FP32, 2 both with the error reported by overlap_error."""
+        """Overlaps of the mixed path: 3 tensor cores (split TF32), 0 FP64
+        rounded to FP32, 1 (default) the faster of the two for the problem
+        (tensor cores without spin-orbit coupling), 2 both with the error
+        reported by overlap_error."""
         self._check(self._lib.pmx_ctx_set_overlap_mode(self.handle, int(mode)), "set_overlap_mode")
 
     def set_schedule(self, schedule: int):

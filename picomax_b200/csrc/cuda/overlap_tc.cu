@@ -9,9 +9,9 @@
 // one k-point they are one complex GEMM D = A B with
 //   rows of A:    (m, v, s')         A[(m,v,s')][p] = v_s'(loci[m][p]) (gathered)
 //   columns of B: (c, s, w)          B[p][(c,s,w)]  = conj(c_s(p)) w(p)
-// which one CTA computes for one k-point, 128 rows at a time (the k+q
-// vectors that the rows gather from staged in shared memory when they fit):
-// the complex
+// which one CTA computes for one k-point, up to four 128-row tiles at a time
+// sharing each B chunk (the k+q vectors that the rows gather from staged in
+// shared memory when they fit): the complex
 // product as two real GEMMs with K stacked as (real parts, imaginary parts)
 // in groups of 8 plane waves,
 //   D_re = [A_re | A_im] [B_re ; -B_im],  D_im = [A_re | A_im] [B_im ; B_re],
@@ -49,7 +49,8 @@ constexpr unsigned kTPolls = 1u << 26;
 constexpr uint64_t kTWaitNs = 2000000000ull;     // 2 s unless the caller sets a limit
 constexpr int kTABytes = kTM * kTK * 4;          // one of hi / lo: 4 KB
 constexpr int kTBBytes = kOvlTcMaxN * kTK * 4;   // one of hi / lo of one of re / im: 4 KB
-constexpr int kTStage = 2 * kTABytes + 4 * kTBBytes;
+constexpr int kTG = 4;                           // row tiles multiplied together (share the B chunk)
+constexpr int kTStage = kTG * 2 * kTABytes + 4 * kTBBytes;
 constexpr int kAPer = kTM * kTK / kTThr;         // A elements per thread and chunk
 constexpr int kBPer = kOvlTcMaxN * kTK / kTThr;  // B elements per thread and chunk (at most)
 
@@ -80,7 +81,7 @@ __device__ __forceinline__ void tmem_ld4(uint32_t taddr, float (&o)[4]) {
   for (int i = 0; i < 4; ++i) o[i] = __uint_as_float(r[i]);
 }
 
-__global__ void __launch_bounds__(kTThr, 2) overlap_tc_kernel(OverlapTcArgs t, int vsm) {
+__global__ void __launch_bounds__(kTThr, 1) overlap_tc_kernel(OverlapTcArgs t, int vsm) {
   const OverlapArgs& a = t.a;
   const int k = blockIdx.x;
   const int ncd = a.ncd[k], nvd = a.nvd[k];
@@ -93,13 +94,16 @@ __global__ void __launch_bounds__(kTThr, 2) overlap_tc_kernel(OverlapTcArgs t, i
   const int ncol = 4 * S * (c_hi - c_lo);
   int N = 16;  // a power of two, so that each thread's B column is the same in every chunk
   while (N < ncol) N <<= 1;
+  // row tiles per group: each takes 2 N TMEM columns (D_re, D_im)
+  const int GT = min(kTG, 512 / (2 * N));
+  const int ngroups = (nrt + GT - 1) / GT;
   const int kp = (a.npw + kTK - 1) / kTK * kTK;  // plane waves, padded
-  const int nchunks = 2 * kp / kTK;              // per row tile
+  const int nchunks = 2 * kp / kTK;              // per group
   // kind::tf32: D F32, A and B TF32, K-major, N >> 3, M >> 4
   const uint32_t idesc =
       (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(kTM >> 4) << 24);
   uint32_t ncols_alloc = 32;
-  while (ncols_alloc < (uint32_t)(2 * N)) ncols_alloc <<= 1;
+  while (ncols_alloc < (uint32_t)(2 * N * GT)) ncols_alloc <<= 1;
 
   extern __shared__ __align__(1024) uint8_t smem[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * kTStage);  // [2]
@@ -140,13 +144,13 @@ __global__ void __launch_bounds__(kTThr, 2) overlap_tc_kernel(OverlapTcArgs t, i
   const uint64_t limit = t.wait_ns > 0 ? (uint64_t)t.wait_ns : kTWaitNs;
   const int bbytes = N * kTK * 4;
 
-  // chunk J = rt * nchunks + j (row tile rt, chunk j of its K). This
-  // thread's A elements are row tid % 128, k = tid / 128 + 2 i (i < 4); its B
-  // elements column tid % N, k = tid / N + (256 / N) i (while < 8). K order:
-  // plane waves p0 .. p0 + 7, real parts of A (even chunks) then imaginary
-  // parts (odd chunks), so that the FP32 accumulator takes each group's
-  // Re(a) Re(b) and Im(a) Im(b) terms back to back (they largely cancel in
-  // the real part).
+  // chunk J = g * nchunks + j (group g of row tiles, chunk j of its K). This
+  // thread's A elements, in each tile of the group, are row tid % 128,
+  // k = tid / 128 + 2 i (i < 4); its B elements column tid % N,
+  // k = tid / N + (256 / N) i (while < 8). K order: plane waves p0 .. p0 + 7,
+  // real parts of A (even chunks) then imaginary parts (odd chunks), so that
+  // the FP32 accumulator takes each group's Re(a) Re(b) and Im(a) Im(b) terms
+  // back to back (they largely cancel in the real part).
   const int ar = tid % kTM, ak0 = tid / kTM;
   const int bcol = tid % N, bk0 = tid / N, bstep = kTThr / N;
   const bool bcol_ok = bcol < ncol;
@@ -154,39 +158,45 @@ __global__ void __launch_bounds__(kTThr, 2) overlap_tc_kernel(OverlapTcArgs t, i
   const double2* bz = zk + (bcol_ok ? scoff[bc] : 0) + bs;  // element p at bz[p * S]
   const int aoff = ((ar >> 3) * 128 + (ar & 7) * 16);       // tile offset of row ar (k group 0)
   const int boff = ((bcol >> 3) * 128 + (bcol & 7) * 16);
-  // row of this thread in the current row tile
-  int cur_rt = -1, a_sp = 0;
-  bool a_ok = false;
-  const short* a_loc = sloc;
-  const double2* a_vec = sv;
-  auto set_row = [&](int rt) {
-    cur_rt = rt;
-    const int R = rt * kTM + ar;
-    a_ok = R < nrows;
-    const int sp = a_ok ? R % S : 0, v = a_ok ? (R / S) % nvd : 0, m = a_ok ? R / (S * nvd) : 0;
-    a_sp = sp;
-    a_loc = sloc + m * a.npw;
-    a_vec = vsm ? sv + (size_t)v * a.n : zq + (size_t)a.vidx[a.vbase[k] + v] * a.n;
+  // rows of this thread in the current group's tiles
+  int cur_g = -1, a_sp[kTG];
+  bool a_ok[kTG];
+  const short* a_loc[kTG];
+  const double2* a_vec[kTG];
+  auto set_rows = [&](int g) {
+    cur_g = g;
+#pragma unroll
+    for (int tt = 0; tt < kTG; ++tt) {
+      const int R = (g * GT + tt) * kTM + ar;
+      const bool ok = tt < GT && R < nrows;
+      const int sp = ok ? R % S : 0, v = ok ? (R / S) % nvd : 0, m = ok ? R / (S * nvd) : 0;
+      a_ok[tt] = ok;
+      a_sp[tt] = sp;
+      a_loc[tt] = sloc + m * a.npw;
+      a_vec[tt] = vsm ? sv + (size_t)v * a.n : zq + (size_t)a.vidx[a.vbase[k] + v] * a.n;
+    }
   };
-  float av[kAPer], bre[kBPer], bim[kBPer];
+  float av[kTG][kAPer], bre[kBPer], bim[kBPer];
   auto fetch = [&](int J) {
-    const int rt = J / nchunks, j = J - rt * nchunks;
-    if (rt != cur_rt) set_row(rt);
+    const int g = J / nchunks, j = J - g * nchunks;
+    if (g != cur_g) set_rows(g);
     const bool imh = (j & 1) != 0;
     const int p0 = (j >> 1) * kTK;
 #pragma unroll
-    for (int i = 0; i < kAPer; ++i) {
-      const int p = p0 + ak0 + 2 * i;
-      float x = 0.f;
-      if (a_ok && p < a.npw) {
-        const int lp = a_loc[p];
-        if (lp >= 0) {
-          const double2 z = a_vec[S == 2 ? 2 * lp + a_sp : lp];
-          x = (float)(imh ? z.y : z.x);
+    for (int tt = 0; tt < kTG; ++tt)
+#pragma unroll
+      for (int i = 0; i < kAPer; ++i) {
+        const int p = p0 + ak0 + 2 * i;
+        float x = 0.f;
+        if (a_ok[tt] && p < a.npw) {
+          const int lp = a_loc[tt][p];
+          if (lp >= 0) {
+            const double2 z = a_vec[tt][S == 2 ? 2 * lp + a_sp[tt] : lp];
+            x = (float)(imh ? z.y : z.x);
+          }
         }
+        av[tt][i] = x;
       }
-      av[i] = x;
-    }
 #pragma unroll
     for (int i = 0; i < kBPer; ++i) {
       const int kk = bk0 + bstep * i, p = p0 + kk;
@@ -204,12 +214,13 @@ __global__ void __launch_bounds__(kTThr, 2) overlap_tc_kernel(OverlapTcArgs t, i
   };
 
   const int A = 3 * a.neps;
-  const int total = nrt * nchunks;
+  const int total = ngroups * nchunks;
   bool ok = true;
   int last = -1;  // last committed chunk
   fetch(0);
   for (int J = 0; J < total && ok; ++J) {
-    const int s = J & 1, rt = J / nchunks, j = J - rt * nchunks;
+    const int s = J & 1, g = J / nchunks, j = J - g * nchunks;
+    const int gt = min(GT, nrt - g * GT);  // tiles in this group
     uint8_t* st = smem + s * kTStage;
     // the stage is free once the MMAs of chunk J - 2 completed (one thread
     // polls, the others wait at the barrier)
@@ -219,15 +230,21 @@ __global__ void __launch_bounds__(kTThr, 2) overlap_tc_kernel(OverlapTcArgs t, i
       break;
     }
 #pragma unroll
-    for (int i = 0; i < kAPer; ++i) {
-      const int kk = ak0 + 2 * i;
-      uint32_t hi, lo;
-      split_tf32(av[i], hi, lo);
-      const int o = aoff + (kk >> 2) * (kTM / 8) * 128 + (kk & 3) * 4;
-      *reinterpret_cast<uint32_t*>(st + o) = hi;
-      *reinterpret_cast<uint32_t*>(st + kTABytes + o) = lo;
+    for (int tt = 0; tt < kTG; ++tt) {
+      if (tt < gt) {
+        uint8_t* sa = st + tt * 2 * kTABytes;
+#pragma unroll
+        for (int i = 0; i < kAPer; ++i) {
+          const int kk = ak0 + 2 * i;
+          uint32_t hi, lo;
+          split_tf32(av[tt][i], hi, lo);
+          const int o = aoff + (kk >> 2) * (kTM / 8) * 128 + (kk & 3) * 4;
+          *reinterpret_cast<uint32_t*>(sa + o) = hi;
+          *reinterpret_cast<uint32_t*>(sa + kTABytes + o) = lo;
+        }
+      }
     }
-    uint8_t* sb = st + 2 * kTABytes;
+    uint8_t* sb = st + kTG * 2 * kTABytes;
 #pragma unroll
     for (int i = 0; i < kBPer; ++i) {
       const int kk = bk0 + bstep * i;
@@ -247,24 +264,28 @@ __global__ void __launch_bounds__(kTThr, 2) overlap_tc_kernel(OverlapTcArgs t, i
     __syncthreads();
     if (tid == 0) {
       fence_after();
-      const uint32_t sa = smem_u32(st), sbb = sa + 2 * kTABytes;
+      const uint32_t s0 = smem_u32(st), sbb = s0 + kTG * 2 * kTABytes;
       const uint32_t alb = (kTM / 8) * 128, blb = (uint32_t)(N / 8) * 128;
-      const uint64_t ahi = umma_desc(sa, alb, 128), alo = umma_desc(sa + kTABytes, alb, 128);
       const uint64_t rh = umma_desc(sbb, blb, 128), rl = umma_desc(sbb + bbytes, blb, 128);
       const uint64_t ih = umma_desc(sbb + 2 * bbytes, blb, 128), il = umma_desc(sbb + 3 * bbytes, blb, 128);
-      const uint32_t acc0 = j > 0 ? 1u : 0u;  // a row tile's first chunk starts its accumulators
-      mma_tf32(tmem, ahi, rh, idesc, acc0);
-      mma_tf32(tmem, ahi, rl, idesc, 1u);
-      mma_tf32(tmem, alo, rh, idesc, 1u);
-      mma_tf32(tmem + N, ahi, ih, idesc, acc0);
-      mma_tf32(tmem + N, ahi, il, idesc, 1u);
-      mma_tf32(tmem + N, alo, ih, idesc, 1u);
+      const uint32_t acc0 = j > 0 ? 1u : 0u;  // a group's first chunk starts its accumulators
+      for (int tt = 0; tt < gt; ++tt) {
+        const uint32_t sa = s0 + tt * 2 * kTABytes;
+        const uint64_t ahi = umma_desc(sa, alb, 128), alo = umma_desc(sa + kTABytes, alb, 128);
+        const uint32_t dre = tmem + (uint32_t)(tt * 2 * N), dim = dre + N;
+        mma_tf32(dre, ahi, rh, idesc, acc0);
+        mma_tf32(dre, ahi, rl, idesc, 1u);
+        mma_tf32(dre, alo, rh, idesc, 1u);
+        mma_tf32(dim, ahi, ih, idesc, acc0);
+        mma_tf32(dim, ahi, il, idesc, 1u);
+        mma_tf32(dim, alo, ih, idesc, 1u);
+      }
       if (!(t.fault == 4 && J == 0)) mma_commit(&bars[s]);
     }
     last = J;
     if (j != nchunks - 1) continue;
-    // ---- row tile rt complete: every MMA has completed once its last
-    // commit has (bounded wait); warps 0-3 read D (TMEM lane = row)
+    // ---- group g complete: every MMA has completed once its last commit
+    // has (bounded wait); warps 0-3 read D (TMEM lane = row) tile by tile
     const bool done = tid != 0 || tc::mbar_wait(&bars[s], (J >> 1) & 1, limit, kTPolls);
     if (__syncthreads_or(!done)) {
       ok = false;
@@ -272,71 +293,73 @@ __global__ void __launch_bounds__(kTThr, 2) overlap_tc_kernel(OverlapTcArgs t, i
     }
     fence_after();
     if (wid < 4) {
-      const int r = wid * 32 + lane, R = rt * kTM + r;
-      const bool row_ok = R < nrows;
-      const int sp = row_ok ? R % S : 0, v = row_ok ? (R / S) % nvd : 0, m = row_ok ? R / (S * nvd) : 0;
-      const double wx = (a.kpts[3 * k] + a.q[0] / 2) + a.G[3 * m] / 2;
-      const double wy = (a.kpts[3 * k + 1] + a.q[1] / 2) + a.G[3 * m + 1] / 2;
-      const double wz = (a.kpts[3 * k + 2] + a.q[2] / 2) + a.G[3 * m + 2] / 2;
-      for (int c = c_lo; c < c_hi; ++c) {
-        // this row's moments for spin s of the conduction state: D[(c, s, w)]
-        double2 mo[2][4];
-        for (int s2 = 0; s2 < S; ++s2) {
-          float re[4], im[4];
-          const uint32_t col = (uint32_t)(((c - c_lo) * S + s2) * 4);
-          const uint32_t lanes = (uint32_t)(wid * 32) << 16;
-          tmem_ld4(tmem + lanes + col, re);
-          tmem_ld4(tmem + lanes + N + col, im);
+      for (int tt = 0; tt < gt; ++tt) {
+        const int R = (g * GT + tt) * kTM + wid * 32 + lane;
+        const bool row_ok = R < nrows;
+        const int sp = row_ok ? R % S : 0, v = row_ok ? (R / S) % nvd : 0, m = row_ok ? R / (S * nvd) : 0;
+        const double wx = (a.kpts[3 * k] + a.q[0] / 2) + a.G[3 * m] / 2;
+        const double wy = (a.kpts[3 * k + 1] + a.q[1] / 2) + a.G[3 * m + 1] / 2;
+        const double wz = (a.kpts[3 * k + 2] + a.q[2] / 2) + a.G[3 * m + 2] / 2;
+        const uint32_t dbase = tmem + ((uint32_t)(wid * 32) << 16) + (uint32_t)(tt * 2 * N);
+        for (int c = c_lo; c < c_hi; ++c) {
+          // this row's moments for spin s of the conduction state: D[(c, s, w)]
+          double2 mo[2][4];
+          for (int s2 = 0; s2 < S; ++s2) {
+            float re[4], im[4];
+            const uint32_t col = (uint32_t)(((c - c_lo) * S + s2) * 4);
+            tmem_ld4(dbase + col, re);
+            tmem_ld4(dbase + N + col, im);
 #pragma unroll
-          for (int w = 0; w < 4; ++w) mo[s2][w] = make_double2(re[w], im[w]);
-        }
-        if (S == 2 && a.nch == 1) {
-          // spin-summed: this row's own spin plus the partner row's (lane ^ 1)
-#pragma unroll
-          for (int w = 0; w < 4; ++w) {
-            const double2 own = mo[sp][w];
-            const double px = __shfl_xor_sync(0xffffffffu, own.x, 1), py = __shfl_xor_sync(0xffffffffu, own.y, 1);
-            mo[0][w] = make_double2(own.x + px, own.y + py);
+            for (int w = 0; w < 4; ++w) mo[s2][w] = make_double2(re[w], im[w]);
           }
-        }
-        if (!row_ok) continue;
-        const long long dst = a.dest[a.blkoff[k] + (long long)c * nvd + v];
-        if (dst < 0) continue;
-        if (S == 2 && a.nch == 1 && sp != 0) continue;  // the pair's first row writes
-        float2* out = t.M32 + ((size_t)dst * A + 3 * m) * a.nch;
-        for (int i = 0; i < 3; ++i) {
-          const double2* u = a.uvec + ((size_t)m * 3 + i) * 3;
-          const double2 sso = a.ssoc[m * 3 + i];
-          auto orb = [&](const double2* mm) {
-            double2 rr = cmulc(u[0], cadd(mm[1], cscale(mm[0], wx)));
-            rr = cadd(rr, cmulc(u[1], cadd(mm[2], cscale(mm[0], wy))));
-            rr = cadd(rr, cmulc(u[2], cadd(mm[3], cscale(mm[0], wz))));
-            return rr;
-          };
-          auto put = [&](int ch, double2 val) {
-            out[(size_t)i * a.nch + ch] = make_float2((float)val.x, (float)val.y);
-          };
-          if (a.nch == 4) {
-            // row s' = up: channel up (s = up) and downup (conj(c_dn) v_up);
-            // row s' = down: channel down and updown (conj(c_up) v_dn)
-            if (sp == 0) {
-              put(0, orb(mo[0]));
-              put(3, cmul(sso, mo[1][0]));
-            } else {
-              put(1, orb(mo[1]));
-              put(2, cmul(sso, mo[0][0]));
+          if (S == 2 && a.nch == 1) {
+            // spin-summed: this row's own spin plus the partner row's (lane ^ 1)
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+              const double2 own = mo[sp][w];
+              const double px = __shfl_xor_sync(0xffffffffu, own.x, 1), py = __shfl_xor_sync(0xffffffffu, own.y, 1);
+              mo[0][w] = make_double2(own.x + px, own.y + py);
             }
-          } else {
-            const double2* mm = mo[0];
-            if (a.mode == 1)
-              put(0, i == 0 ? mm[0] : cadd(orb(mm), cmul(sso, mm[0])));
-            else
-              put(0, orb(mm));
+          }
+          if (!row_ok) continue;
+          const long long dst = a.dest[a.blkoff[k] + (long long)c * nvd + v];
+          if (dst < 0) continue;
+          if (S == 2 && a.nch == 1 && sp != 0) continue;  // the pair's first row writes
+          float2* out = t.M32 + ((size_t)dst * A + 3 * m) * a.nch;
+          for (int i = 0; i < 3; ++i) {
+            const double2* u = a.uvec + ((size_t)m * 3 + i) * 3;
+            const double2 sso = a.ssoc[m * 3 + i];
+            auto orb = [&](const double2* mm) {
+              double2 rr = cmulc(u[0], cadd(mm[1], cscale(mm[0], wx)));
+              rr = cadd(rr, cmulc(u[1], cadd(mm[2], cscale(mm[0], wy))));
+              rr = cadd(rr, cmulc(u[2], cadd(mm[3], cscale(mm[0], wz))));
+              return rr;
+            };
+            auto put = [&](int ch, double2 val) {
+              out[(size_t)i * a.nch + ch] = make_float2((float)val.x, (float)val.y);
+            };
+            if (a.nch == 4) {
+              // row s' = up: channel up (s = up) and downup (conj(c_dn) v_up);
+              // row s' = down: channel down and updown (conj(c_up) v_dn)
+              if (sp == 0) {
+                put(0, orb(mo[0]));
+                put(3, cmul(sso, mo[1][0]));
+              } else {
+                put(1, orb(mo[1]));
+                put(2, cmul(sso, mo[0][0]));
+              }
+            } else {
+              const double2* mm = mo[0];
+              if (a.mode == 1)
+                put(0, i == 0 ? mm[0] : cadd(orb(mm), cmul(sso, mm[0])));
+              else
+                put(0, orb(mm));
+            }
           }
         }
       }
     }
-    // the next row tile's first MMAs overwrite the accumulators
+    // the next group's first MMAs overwrite the accumulators
     fence_before();
     __syncthreads();
     fence_after();
