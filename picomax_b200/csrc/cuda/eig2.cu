@@ -18,8 +18,11 @@
 //     Each pass reads (and the second writes) the trailing block once per
 //     panel instead of once per column. The panel's reflectors stay in place
 //     below the band (LAPACK layout); T goes into the free upper tile.
+//     Up to ld = 416 the panel V and Y live in shared memory; beyond that
+//     (ld <= 800) Y lives in the item's slot of the reflector buffer (L2).
 //  2. sbtrd_kernel (one CTA per matrix): the band (16 sub-diagonals plus 16
-//     for the bulge) lives in shared memory; sweeps chase their bulges down
+//     for the bulge) lives in shared memory up to ld = 416, beyond that in
+//     the item's slot of the reflector buffer (L1/L2); sweeps chase their bulges down
 //     the band, eight at a time (a pair of warps per sweep), each step of a
 //     sweep waiting only for the previous sweep to leave its rows (progress
 //     words in shared memory, no block-wide barrier). Reflectors go to
@@ -52,7 +55,8 @@ namespace {
 constexpr int kNB = 16;        // panel width = band width
 constexpr int kThr = 256;      // threads per CTA of every stage
 constexpr int kNW = kThr / 32;
-constexpr int kMaxLd = 416;    // largest padded dimension (shared memory of both stages)
+constexpr int kMaxLd = 800;    // largest padded dimension
+constexpr int kSmemLd = 416;   // largest one whose stage-1 Y and stage-2 band fit in shared memory
 constexpr int kVecBlock = 32;  // eigenvectors per back-transform CTA
 
 // element (r, c) of an m x 16 complex panel in shared memory: rows of 16,
@@ -127,6 +131,11 @@ __host__ __device__ __forceinline__ long long ceil_sum(long long M) {
 }
 // index of the first reflector of sweep s
 __host__ __device__ __forceinline__ long long sweep_first(int ld, int s) { return ceil_sum(ld - 1) - ceil_sum(ld - 1 - s); }
+// Slot of an item in the reflector buffer (double2 offsets): the band
+// reflectors [ceil_sum(ld - 1)][16], the tridiagonal (2 ld doubles), and, in
+// launches with ld > kSmemLd, a work area of 32 ld double2: stage 1's Y
+// (16 (ld - 16)), then stage 2's band (32 ld).
+__host__ __device__ __forceinline__ long long band_off(int ld) { return ceil_sum(ld - 1) * kNB + ld; }
 
 // ------------------------------------------------------------------ stage 1
 struct SbSmem {
@@ -143,11 +152,15 @@ struct SbSmem {
 };
 
 // register rows per thread of the panel QR for a padded dimension ld
-inline int sb_rows(int ld) { return ld <= 160 ? 9 : (ld <= 288 ? 17 : 25); }
+inline int sb_rows(int ld) { return ld <= 160 ? 9 : (ld <= 288 ? 17 : (ld <= 416 ? 25 : (ld <= 592 ? 36 : 49))); }
 
-__host__ __device__ inline size_t sb_smem_bytes(int ld) {
+// double2 of the panel QR's work arrays (red, rowj, pvw)
+__host__ __device__ inline int sb_qr_work(int mr) { return 2 * 8 * 16 + 2 * 16 + 16 * mr; }
+// V [mmax][16]; then Y [mmax][16] in shared memory, or (Y in global memory)
+// the panel QR's work arrays after the T/M/P/tau block (ld = 800: 231 KB)
+__host__ __device__ inline size_t sb_smem_bytes(int ld, int mr, bool yg) {
   const int mmax = ld - kNB;
-  return sizeof(double2) * ((size_t)2 * mmax * kNB + 3 * kNB * 17 + kNB);
+  return sizeof(double2) * ((size_t)mmax * kNB + (yg ? (size_t)sb_qr_work(mr) : (size_t)mmax * kNB) + 3 * kNB * 17 + kNB);
 }
 
 // Householder QR of the m x 16 panel (rows r0.. of columns c0..c0+15 of A)
@@ -393,8 +406,23 @@ __device__ void pass_u(double2* __restrict__ A, int ld, int r0, int Mt, const do
 
 }  // namespace
 
-template <int MR>
-__global__ void __launch_bounds__(kThr, 1) sb_kernel(const EigItem* __restrict__ items, double2* __restrict__ hbuf) {
+// Load of Y in global memory kept in program order: with plain loads the
+// compiler hoists the rows' loads of the Y T and P passes far enough ahead to
+// spill ~4 KB of the stage's registers
+__device__ __forceinline__ double2 ld_ordered(const double2* p) {
+  double2 v;
+  asm volatile("ld.global.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p) : "memory");
+  return v;
+}
+template <bool KYG>
+__device__ __forceinline__ double2 ldy(const double2* p) {
+  return KYG ? ld_ordered(p) : *p;
+}
+
+// KYG: Y in the item's work area of the reflector buffer (ld > kSmemLd)
+template <int MR, bool KYG>
+__global__ void __launch_bounds__(kThr, 1) sb_kernel(const EigItem* __restrict__ items, double2* __restrict__ hbuf,
+                                                    double2* __restrict__ rbuf) {
   const EigItem it = items[blockIdx.x];
   const int ld = it.ld;
   const int tid = threadIdx.x;
@@ -403,12 +431,15 @@ __global__ void __launch_bounds__(kThr, 1) sb_kernel(const EigItem* __restrict__
   const int mmax = ld - kNB;
   SbSmem S;
   S.V = reinterpret_cast<double2*>(smraw);
-  S.Y = S.V + (size_t)mmax * kNB;
-  S.T = S.Y + (size_t)mmax * kNB;
+  S.Y = KYG ? rbuf + it.r_off + band_off(ld) : S.V + (size_t)mmax * kNB;
+  S.T = (KYG ? S.V : S.Y) + (size_t)mmax * kNB;
   S.M = S.T + kNB * 17;
   S.P = S.M + kNB * 17;
   S.taus = S.P + kNB * 17;
-  S.part = S.Y;  // 256 + 32 + 16 MR <= 16 mmax double2 for ld >= 96
+  // the panel QR's work arrays: inside Y (free until Y = A V is formed;
+  // 256 + 32 + 16 MR <= 16 mmax double2 for ld >= 96), or after taus (a
+  // region of their own: sharing V's made the compiler spill the panel)
+  S.part = KYG ? S.taus + kNB : S.Y;
   S.rowj = S.part + 2 * 8 * 16;
   S.pvw = S.rowj + 2 * 16;
 
@@ -428,7 +459,7 @@ __global__ void __launch_bounds__(kThr, 1) sb_kernel(const EigItem* __restrict__
     for (int r = tid; r < m; r += kThr) {
       double2 y[kNB];
 #pragma unroll
-      for (int c = 0; c < kNB; ++c) y[c] = S.Y[pidx(r, c)];
+      for (int c = 0; c < kNB; ++c) y[c] = ldy<KYG>(S.Y + pidx(r, c));
 #pragma unroll
       for (int c = kNB - 1; c >= 0; --c) {
         double2 s = make_double2(0, 0);
@@ -443,6 +474,7 @@ __global__ void __launch_bounds__(kThr, 1) sb_kernel(const EigItem* __restrict__
     {  // M = V^H Y
       const int i = tid / kNB, j = tid % kNB;
       double2 s = make_double2(0, 0);
+#pragma unroll 8
       for (int r = i; r < m; ++r) s = cadd(s, cmulc(S.V[pidx(r, i)], S.Y[pidx(r, j)]));
       S.M[i * 17 + j] = s;
     }
@@ -463,7 +495,7 @@ __global__ void __launch_bounds__(kThr, 1) sb_kernel(const EigItem* __restrict__
         double2 s = make_double2(0, 0);
 #pragma unroll
         for (int k = 0; k < kNB; ++k) s = cadd(s, cmul(v[k], S.P[k * 17 + c]));
-        S.Y[pidx(r, c)] = csub(S.Y[pidx(r, c)], cscale(s, 0.5));
+        S.Y[pidx(r, c)] = csub(ldy<KYG>(S.Y + pidx(r, c)), cscale(s, 0.5));
       }
     }
     __syncthreads();
@@ -496,8 +528,9 @@ constexpr int kS2W = kS2Thr / 32;
 constexpr int kProgStride = 64;          // progress word: sweep * 64 + steps done (<= 26)
 constexpr long long kWaitNs = 2000000000LL;  // default limit of one wait
 
-__host__ __device__ inline size_t sbtrd_smem_bytes(int ld) {
-  return sizeof(double2) * ((size_t)ld * kBandLd + kPairs * 2 * 17 + kS2W * 2 * kNB) + sizeof(int) * (kPairs + 4);
+__host__ __device__ inline size_t sbtrd_smem_bytes(int ld, bool bg) {
+  return sizeof(double2) * ((bg ? 0 : (size_t)ld * kBandLd) + kPairs * 2 * 17 + kS2W * 2 * kNB) +
+         sizeof(int) * (kPairs + 4);
 }
 
 __device__ __forceinline__ int ld_acquire_shared(const int* p) {
@@ -537,6 +570,10 @@ __device__ __forceinline__ void wait_progress(const int* flag, int need, int* er
   atomicExch(err, 1);
 }
 
+// KBG: the band in the item's work area of the reflector buffer (ld >
+// kSmemLd; a CTA-private region, so the same CTA-scope ordering as in shared
+// memory applies)
+template <bool KBG>
 __global__ void __launch_bounds__(kS2Thr, 1) sbtrd_kernel(const EigItem* __restrict__ items,
                                                         const double2* __restrict__ hbuf, double2* __restrict__ rbuf) {
   const EigItem it = items[blockIdx.x];
@@ -545,8 +582,9 @@ __global__ void __launch_bounds__(kS2Thr, 1) sbtrd_kernel(const EigItem* __restr
   const double2* A = hbuf + it.h_off;
   double2* R = rbuf + it.r_off;
   extern __shared__ __align__(16) unsigned char smraw[];
-  double2* Bd = reinterpret_cast<double2*>(smraw);
-  double2* slots = Bd + (size_t)ld * kBandLd;  // [pair][2][17]: v (v_0 = 1), tau of the pair's next steps
+  double2* Bd = KBG ? R + band_off(ld) : reinterpret_cast<double2*>(smraw);
+  // [pair][2][17]: v (v_0 = 1), tau of the pair's next steps
+  double2* slots = KBG ? reinterpret_cast<double2*>(smraw) : Bd + (size_t)ld * kBandLd;
   double2* wsm = slots + kPairs * 2 * 17;       // [warp][32]: [0, 16) v, [16, 32) vectors broadcast in a warp
   int* prog = reinterpret_cast<int*>(wsm + kS2W * 2 * kNB);  // [pair]: progress words
   int* err = prog + kPairs;                                  // a wait gave up
@@ -802,8 +840,8 @@ __host__ __device__ inline size_t back_smem_bytes(int ld, int vb) {
   // Z [ld][vb], one sweep's reflectors [2][ceil(ld/16)][16], W [16][vb], T [16][17]
   return sizeof(double2) * ((size_t)ld * vb + 2 * ((ld + kNB - 1) / kNB) * kNB + kNB * vb + kNB * 17);
 }
-// reflector entries of a sweep that one thread stages (ceil(416 / 16) * 16 / 256)
-constexpr int kBackStage = 2;
+// reflector entries of a sweep that one thread stages (ceil(kMaxLd / 16) * 16 / 256)
+constexpr int kBackStage = (kMaxLd + kThr - 1) / kThr;
 // eigenvectors per back-transform CTA: up to kVecBlock, and few enough that
 // two CTAs share an SM (the stage is latency-bound)
 inline int back_vec_block(int ld, int max_nvec) {
@@ -972,7 +1010,9 @@ int heev2_ld(int n) { return (n + kNB - 1) / kNB * kNB; }
 
 bool heev2_supported(int max_n) { return heev2_ld(max_n) >= 96 && heev2_ld(max_n) <= kMaxLd; }
 
-size_t heev2_rbuf_double2(int ld) { return (size_t)ceil_sum(ld - 1) * kNB + (size_t)ld; }
+size_t heev2_rbuf_double2(int ld, int launch_ld) {
+  return (size_t)band_off(ld) + (launch_ld > kSmemLd ? (size_t)kBandLd * ld : 0);
+}
 
 cudaError_t launch_heev2(const EigItem* items, int nitems, int max_n, int max_nval, int max_nvec, double2* hbuf,
                          double* wbuf, double2* zbuf, double* scratch, double2* rbuf, int* info, cudaStream_t st) {
@@ -981,15 +1021,21 @@ cudaError_t launch_heev2(const EigItem* items, int nitems, int max_n, int max_nv
   const int ld = heev2_ld(max_n);
   cudaError_t e;
   const int mr = sb_rows(ld);
-  const size_t s1 = sb_smem_bytes(ld);
-  auto sb = mr == 9 ? sb_kernel<9> : (mr == 17 ? sb_kernel<17> : sb_kernel<25>);
+  const bool big = ld > kSmemLd;  // Y and the band in the reflector buffer's work areas
+  const size_t s1 = sb_smem_bytes(ld, mr, big);
+  auto sb = mr == 9    ? sb_kernel<9, false>
+            : mr == 17 ? sb_kernel<17, false>
+            : mr == 25 ? sb_kernel<25, false>
+            : mr == 36 ? sb_kernel<36, true>
+                       : sb_kernel<49, true>;
   e = cudaFuncSetAttribute(sb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1);
   if (e != cudaSuccess) return e;
-  sb<<<nitems, kThr, s1, st>>>(items, hbuf);
-  const size_t s2 = sbtrd_smem_bytes(ld);
-  e = cudaFuncSetAttribute(sbtrd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2);
+  sb<<<nitems, kThr, s1, st>>>(items, hbuf, rbuf);
+  const size_t s2 = sbtrd_smem_bytes(ld, big);
+  auto tr = big ? sbtrd_kernel<true> : sbtrd_kernel<false>;
+  e = cudaFuncSetAttribute(tr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2);
   if (e != cudaSuccess) return e;
-  sbtrd_kernel<<<nitems, kS2Thr, s2, st>>>(items, hbuf, rbuf);
+  tr<<<nitems, kS2Thr, s2, st>>>(items, hbuf, rbuf);
   const int xsm_ok = tri_smem_xbytes(max_n, max_nval, max_nvec) <= kTriXsmMax ? 1 : 0;
   const size_t s3 = xsm_ok ? tri_smem_xbytes(max_n, max_nval, max_nvec) : tri_smem_bytes(max_n, max_nval, max_nvec);
   e = cudaFuncSetAttribute(tri_eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s3);

@@ -77,13 +77,15 @@ int heev_variants(int max_n, int max_nev);
 int heev_batch_unit(int max_n, int max_nev);
 
 // Two-stage eigensolver (eig2.cu): dense -> band (16 sub-diagonals) on the
-// FP64 tensor cores, band -> tridiagonal by bulge chasing in shared memory,
-// bisection + inverse iteration, back-transforms. Items carry ld =
-// heev2_ld(n) (the workspace padded with zeros, see launch_assemble) and
-// r_off, spaced by at least heev2_rbuf_double2(ld) double2 in rbuf.
+// FP64 tensor cores, band -> tridiagonal by bulge chasing (the band in
+// shared memory up to ld = 416, in rbuf up to 832), bisection + inverse
+// iteration, back-transforms. Items carry ld = heev2_ld(n) (the workspace
+// padded with zeros, see launch_assemble) and r_off, spaced by at least
+// heev2_rbuf_double2(ld, heev2_ld(max_n)) double2 in rbuf (max_n: the
+// launch's largest n).
 int heev2_ld(int n);
 bool heev2_supported(int max_n);
-size_t heev2_rbuf_double2(int ld);
+size_t heev2_rbuf_double2(int ld, int launch_ld);
 cudaError_t launch_heev2(const EigItem* items, int nitems, int max_n, int max_nval, int max_nvec, double2* hbuf,
                          double* wbuf, double2* zbuf, double* scratch, double2* rbuf, int* info, cudaStream_t st);
 

@@ -395,7 +395,7 @@ DevCrystal upload_crystal(pmx_ctx* c, const pmx_problem* P, int force_spinor) {
 }
 
 // Eigensolver dispatch. Where the two-stage solver applies (matrices too
-// large for the shared-memory-resident one-stage kernel, padded size <= 416,
+// large for the shared-memory-resident one-stage kernel, padded size <= 832,
 // and no export of the one-stage reduction for the adjoint) it is schedule 0
 // and the one-stage schedules follow; otherwise only the one-stage schedules
 // are offered. A launch's items then carry the padded leading dimension and
@@ -410,7 +410,8 @@ int eig_variants(int max_n, int max_nval, bool tri) {
 // launch whose largest matrix is max_n
 int eig_ld(int n, int max_n, bool tri) { return use_two_stage(max_n, tri) ? pmx::dev::heev2_ld(n) : n; }
 size_t eig_rstride(int n, int max_n, bool tri) {
-  return use_two_stage(max_n, tri) ? pmx::dev::heev2_rbuf_double2(pmx::dev::heev2_ld(n)) : 0;
+  return use_two_stage(max_n, tri) ? pmx::dev::heev2_rbuf_double2(pmx::dev::heev2_ld(n), pmx::dev::heev2_ld(max_n))
+                                    : 0;
 }
 // the context's wait limit and test fault hooks on an eigensolver item
 void eig_hooks(const pmx_ctx* c, pmx::dev::EigItem& it) {

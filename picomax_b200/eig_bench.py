@@ -5,7 +5,7 @@ python -m picomax_b200.eig_bench [--n 274] [--batch 296] [--nev 17] [--schedule 
 Prints the device time of each call (CUDA events around the eigensolver
 launches) and the largest eigenvalue error of the first matrix against
 numpy. Schedule 0 is the two-stage solver for the sizes it covers (matrices
-beyond the shared-memory-resident kernel, padded size <= 416); 1.. are the
+beyond the shared-memory-resident kernel, padded size <= 800); 1.. are the
 one-stage schedules; -1 lets the autotuner choose (it runs on batches of at
 least 148 matrices).
 """

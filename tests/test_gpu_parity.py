@@ -197,6 +197,23 @@ def test_degenerate_cut_reported(ctx, tmp_path):
     assert ctx.degenerate_cuts() >= 1
 
 
+@pytest.mark.parametrize("n,nev,degenerate", [(420, 20, False), (570, 49, True), (600, 33, False), (800, 24, True)])
+def test_heev_two_stage_beyond_shared_memory(ctx, n, nev, degenerate):
+    """Padded sizes 432-800: the two-stage solver with stage 1's Y and stage 2's
+    band in the reflector buffer's work area (global memory) instead of shared
+    memory; Kramers-degenerate spectra included."""
+    rng = np.random.default_rng(n + 7)
+    A = np.stack([_random_hermitian(rng, n, degenerate) for _ in range(2)])
+    w, Z = ctx.heev(A, nev)
+    for b in range(2):
+        full = np.linalg.eigvalsh(A[b])
+        scale = np.max(np.abs(full))
+        assert np.max(np.abs(w[b] - full[:nev])) < 1e-12 * scale * n
+        R = A[b] @ Z[b] - Z[b] * w[b]
+        assert np.max(np.linalg.norm(R, axis=0)) < 1e-10 * scale
+        assert np.max(np.abs(Z[b].conj().T @ Z[b] - np.eye(nev))) < 1e-10
+
+
 def _qvec(K):
     return ",".join(f"{x:.6f}" for x in np.asarray(K).ravel())
 
