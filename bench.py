@@ -15,7 +15,8 @@ every host<->device copy inside the timed region. With --gpus N each rank runs
 its own spectra (independent (crystal, q) units, no collective on the data
 path; weak scaling) and the slowest rank's time counts. `extra_workloads`
 repeats the measurement (fewer steps) on the wurtzite epsLL workload
-(N_G 401, NEPS 59, 24x24x16 k) unless --no-extra.
+(N_G 401, NEPS 59, 24x24x16 k) and on the Te + SOC epsLL workload (n 570,
+NEPS 15, 10x10x8 k) unless --no-extra.
 
 `--impl reference` times the reference PicoMax (rebuilt from source in
 oracle/_ref, OpenMP on every host core) on a bounded sample of the same
@@ -41,7 +42,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "eps_M(q,w) spectra/s, mixed vs FP64 GPU at <=1e-4 rel err; eigensolve k-pts/s"
-FP64_TFLOPS_NOMINAL = 37.0  # B200 FP64 (HGX spec sheet); no measured FP64 peak on this pool
+FP64_TFLOPS_NOMINAL = 37.0  # B200 FP64 (HGX spec sheet)
 
 
 def parse():
@@ -54,7 +55,7 @@ def parse():
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="leave out the timed reference sample (minutes of host time on the larger workloads)")
-    ap.add_argument("--no-extra", action="store_true", help="leave out the wurtzite epsLL measurement")
+    ap.add_argument("--no-extra", action="store_true", help="leave out the wurtzite and Te epsLL measurements")
     ap.add_argument("--schedule", type=int, default=-1,
                     help="fixed eigensolver schedule (default -1: the autotuner picks; 0 is the two-stage solver "
                          "where it applies) - for profiler runs, whose serialised launches skew the autotuner")
@@ -360,10 +361,35 @@ def measure(name, steps, warmup, fp64_steps, rank, world, dev, with_e2e=True, sc
     return res
 
 
-def heev_roofline(m):
+def fp64_peak_tflops(dev):
+    """FP64 denominator measured in this run: cuBLAS DGEMM (torch.matmul) of
+    8192 x 8192 float64 matrices, 2 warm-up and 5 timed products between CUDA
+    events, best of the five (2 * 8192^3 flop each)."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=f"cuda:{dev}")
+    b = torch.randn(n, n, dtype=torch.float64, device=f"cuda:{dev}")
+    c = torch.empty_like(a)
+    for _ in range(2):
+        torch.matmul(a, b, out=c)
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b, out=c)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def heev_roofline(m, fp64_peak=None):
     """Roofline of the eigensolver (the dominant kernel family): algorithmic
     FP64 work per launch over the event-timed launch duration, against the
-    nominal FP64 peak; DRAM traffic from the committed ncu capture."""
+    FP64 peak measured in this run (cuBLAS DGEMM; the nominal figure beside
+    it); DRAM traffic from the committed ncu capture."""
     info = m["info"]
     n = info.nh if info.soc else info.npw
     nb = info.nband if info.soc else (info.nband + 1) // 2
@@ -373,12 +399,16 @@ def heev_roofline(m):
     ms_launch = per["heev"][0] / nl
     ach = flops / nl / (ms_launch * 1e-3) / 1e12
     bpm = profiled_heev_bytes(n)
+    pk = fp64_peak or FP64_TFLOPS_NOMINAL
     return {"kernel": "heev (two-stage: sb_kernel, sbtrd_kernel, tri_eig_kernel, eig2_back_kernel)",
-            "bound": "fp64", "achieved": ach, "peak": FP64_TFLOPS_NOMINAL, "unit": "TFLOP/s",
-            "frac": ach / FP64_TFLOPS_NOMINAL, "traffic": bpm * m["nsolves"] / nl if bpm else None,
+            "bound": "fp64", "achieved": ach, "peak": pk, "unit": "TFLOP/s",
+            "frac": ach / pk, "frac_of_nominal": ach / FP64_TFLOPS_NOMINAL,
+            "traffic": bpm * m["nsolves"] / nl if bpm else None,
             "traffic_source": "DRAM bytes per matrix of the ncu capture in profiles/heev2_gaas_epsij.md x matrices "
                               "per launch" if bpm else None,
-            "peak_source": "nominal B200 FP64 (no measured FP64 peak in MEASURED_PEAKS.json)",
+            "peak_source": ("cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure); "
+                            "frac_of_nominal against the 37 TFLOP/s spec") if fp64_peak else
+                           "nominal B200 FP64 (no measured FP64 peak)",
             "per_launch_ms": ms_launch, "launches_per_step": per["heev"][1],
             "algorithmic_flop_per_matrix": (16.0 / 3.0) * n ** 3 + 8.0 * n * n * nb}
 
@@ -413,7 +443,8 @@ def ours(args, rank, world):
     per = m["per"]
     dom = max(per, key=lambda f: per[f][0])
     roof_mixed = mixed_roofline(m, peaks)
-    roof = heev_roofline(m) if dom == "heev" else dict(roof_mixed or {"kernel": "mixed_kernel", "bound": "tensor",
+    fp64_pk = fp64_peak_tflops(dev)
+    roof = heev_roofline(m, fp64_pk) if dom == "heev" else dict(roof_mixed or {"kernel": "mixed_kernel", "bound": "tensor",
                                                                        "unit": "TFLOP/s"}, traffic=None)
     n_eig = 1 + 2 * m["info"].nk
     out = {
@@ -428,21 +459,24 @@ def ours(args, rank, world):
         "stage_ms": {f: per[f][0] for f in per},
         "e2e": m["e2e"],
         "gpu_launches": int(m["launches"]),
-        "roofline": roof, "roofline_heev": heev_roofline(m), "roofline_mixed_contraction": roof_mixed,
+        "roofline": roof, "roofline_heev": heev_roofline(m, fp64_pk), "roofline_mixed_contraction": roof_mixed,
         "clocks": m["clocks"], "degenerate_cuts": m["degenerate_cuts"], "autotune": m["autotune"],
     }
     if world == 1 and not args.no_extra:
         # the wurtzite epsLL workload (config 3: N_G 401, NEPS 59, 24x24x16 k), where the mixed path's
-        # tensor-core contraction replaces most of the FP64 path's time
-        w = measure("wz_epsLL", 2, 3, 1, rank, world, dev, with_e2e=False, schedule=args.schedule)
-        shutil.rmtree(w["tmp"], ignore_errors=True)
-        out["extra_workloads"] = {"wz_epsLL": {
-            "value": w["value"], "unit": "spectra/s", "ms_per_step": w["ms_per_step"], "steps": 2, "warmup": 3,
-            "fp64": w["fp64"], "mixed_over_fp64": w["mixed_over_fp64"],
-            "mixed_max_rel_err_vs_fp64": w["mixed_max_rel_err_vs_fp64"],
-            "epsm_max_rel_err_vs_fp64": w["epsm_max_rel_err_vs_fp64"], "config": w["config"],
-            "stage_ms": {f: w["per"][f][0] for f in w["per"]}, "roofline_heev": heev_roofline(w),
-            "roofline_mixed_contraction": mixed_roofline(w, peaks), "clocks": w["clocks"]}}
+        # tensor-core contraction replaces most of the FP64 path's time, and the Te + SOC epsLL workload
+        # (config 5's grid: n 570, NEPS 15, 10x10x8 k), where the FP64 eigensolver is nearly all of it
+        out["extra_workloads"] = {}
+        for name, steps in (("wz_epsLL", 2), ("te_epsLL", 3)):
+            w = measure(name, steps, 3, 1, rank, world, dev, with_e2e=False, schedule=args.schedule)
+            shutil.rmtree(w["tmp"], ignore_errors=True)
+            out["extra_workloads"][name] = {
+                "value": w["value"], "unit": "spectra/s", "ms_per_step": w["ms_per_step"], "steps": steps,
+                "warmup": 3, "fp64": w["fp64"], "mixed_over_fp64": w["mixed_over_fp64"],
+                "mixed_max_rel_err_vs_fp64": w["mixed_max_rel_err_vs_fp64"],
+                "epsm_max_rel_err_vs_fp64": w["epsm_max_rel_err_vs_fp64"], "config": w["config"],
+                "stage_ms": {f: w["per"][f][0] for f in w["per"]}, "roofline_heev": heev_roofline(w, fp64_pk),
+                "roofline_mixed_contraction": mixed_roofline(w, peaks), "clocks": w["clocks"]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_sample(m["argv"], m["nspec"])
     shutil.rmtree(m["tmp"], ignore_errors=True)

@@ -19,7 +19,8 @@
 //     panel instead of once per column. The panel's reflectors stay in place
 //     below the band (LAPACK layout); T goes into the free upper tile.
 //     Up to ld = 416 the panel V and Y live in shared memory; beyond that
-//     (ld <= 800) Y lives in the item's slot of the reflector buffer (L2).
+//     (ld <= 800) Y lives in the item's slot of the reflector buffer (L2),
+//     and beyond ld = 800 (ld <= 1216) V as well.
 //  2. sbtrd_kernel (one CTA per matrix): the band (16 sub-diagonals plus 16
 //     for the bulge) lives in shared memory up to ld = 416, beyond that in
 //     the item's slot of the reflector buffer (L1/L2); sweeps chase their bulges down
@@ -55,7 +56,8 @@ namespace {
 constexpr int kNB = 16;        // panel width = band width
 constexpr int kThr = 256;      // threads per CTA of every stage
 constexpr int kNW = kThr / 32;
-constexpr int kMaxLd = 800;    // largest padded dimension
+constexpr int kMaxLd = 1216;   // largest padded dimension
+constexpr int kVSmemLd = 800;  // largest one whose stage-1 V fits in shared memory
 constexpr int kSmemLd = 416;   // largest one whose stage-1 Y and stage-2 band fit in shared memory
 constexpr int kVecBlock = 32;  // eigenvectors per back-transform CTA
 
@@ -134,7 +136,8 @@ __host__ __device__ __forceinline__ long long sweep_first(int ld, int s) { retur
 // Slot of an item in the reflector buffer (double2 offsets): the band
 // reflectors [ceil_sum(ld - 1)][16], the tridiagonal (2 ld doubles), and, in
 // launches with ld > kSmemLd, a work area of 32 ld double2: stage 1's Y
-// (16 (ld - 16)), then stage 2's band (32 ld).
+// (16 (ld - 16)) and, for ld > kVSmemLd, V after it (16 (ld - 16)); then
+// stage 2's band (32 ld).
 __host__ __device__ __forceinline__ long long band_off(int ld) { return ceil_sum(ld - 1) * kNB + ld; }
 
 // ------------------------------------------------------------------ stage 1
@@ -152,15 +155,19 @@ struct SbSmem {
 };
 
 // register rows per thread of the panel QR for a padded dimension ld
-inline int sb_rows(int ld) { return ld <= 160 ? 9 : (ld <= 288 ? 17 : (ld <= 416 ? 25 : (ld <= 592 ? 36 : 49))); }
+inline int sb_rows(int ld) {
+  return ld <= 160 ? 9 : (ld <= 288 ? 17 : (ld <= 416 ? 25 : (ld <= 592 ? 36 : (ld <= 800 ? 49 : 75))));
+}
 
 // double2 of the panel QR's work arrays (red, rowj, pvw)
 __host__ __device__ inline int sb_qr_work(int mr) { return 2 * 8 * 16 + 2 * 16 + 16 * mr; }
-// V [mmax][16]; then Y [mmax][16] in shared memory, or (Y in global memory)
-// the panel QR's work arrays after the T/M/P/tau block (ld = 800: 231 KB)
-__host__ __device__ inline size_t sb_smem_bytes(int ld, int mr, bool yg) {
+// V [mmax][16] (unless in global memory); then Y [mmax][16] in shared
+// memory, or (Y in global memory) the panel QR's work arrays after the
+// T/M/P/tau block (ld = 800: 231 KB)
+__host__ __device__ inline size_t sb_smem_bytes(int ld, int mr, bool yg, bool vg) {
   const int mmax = ld - kNB;
-  return sizeof(double2) * ((size_t)mmax * kNB + (yg ? (size_t)sb_qr_work(mr) : (size_t)mmax * kNB) + 3 * kNB * 17 + kNB);
+  return sizeof(double2) * ((vg ? 0 : (size_t)mmax * kNB) + (yg ? (size_t)sb_qr_work(mr) : (size_t)mmax * kNB) +
+                            3 * kNB * 17 + kNB);
 }
 
 // Householder QR of the m x 16 panel (rows r0.. of columns c0..c0+15 of A)
@@ -285,6 +292,9 @@ __device__ void panel_qr(double2* __restrict__ A, int ld, int c0, int r0, int m,
 // Y[m x 16] = A22 V: every warp owns 8-row blocks; the upper tiles of the
 // Hermitian trailing block are read as conjugate transposes of the lower ones,
 // the diagonal tiles (kept full) directly.
+// PF: V in global memory, its fragments of column block J + 1 loaded while
+// block J is multiplied
+template <bool PF>
 __device__ void pass_y(const double2* __restrict__ A, int ld, int r0, int Mt, const double2* V, double2* Y) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int gr = lane >> 2, gk = lane & 3;
@@ -305,19 +315,36 @@ __device__ void pass_y(const double2* __restrict__ A, int ld, int r0, int Mt, co
           f[kb] = cconj(A[(size_t)row * ld + col]);
       }
     };
+    double2 bf[4][2], bfn[4][2];
+    auto load_b = [&](int J, double2 (&f)[4][2]) {
+#pragma unroll
+      for (int kb = 0; kb < 4; ++kb)
+#pragma unroll
+        for (int nb = 0; nb < 2; ++nb) f[kb][nb] = V[pidx(16 * J + 4 * kb + gk, 8 * nb + gr)];
+    };
     load_a(0, a);
+    if (PF) load_b(0, bf);
     for (int J = 0; J < Mt; ++J) {
-      if (J + 1 < Mt) load_a(J + 1, an);
+      if (J + 1 < Mt) {
+        load_a(J + 1, an);
+        if (PF) load_b(J + 1, bfn);
+      }
 #pragma unroll
       for (int kb = 0; kb < 4; ++kb) {
 #pragma unroll
         for (int nb = 0; nb < 2; ++nb) {
-          const double2 b = V[pidx(16 * J + 4 * kb + gk, 8 * nb + gr)];
+          const double2 b = PF ? bf[kb][nb] : V[pidx(16 * J + 4 * kb + gk, 8 * nb + gr)];
           cmma(cr[nb], ci[nb], a[kb], b);
         }
       }
 #pragma unroll
-      for (int kb = 0; kb < 4; ++kb) a[kb] = an[kb];
+      for (int kb = 0; kb < 4; ++kb) {
+        a[kb] = an[kb];
+        if (PF) {
+#pragma unroll
+          for (int nb = 0; nb < 2; ++nb) bf[kb][nb] = bfn[kb][nb];
+        }
+      }
     }
 #pragma unroll
     for (int nb = 0; nb < 2; ++nb)
@@ -419,8 +446,9 @@ __device__ __forceinline__ double2 ldy(const double2* p) {
   return KYG ? ld_ordered(p) : *p;
 }
 
-// KYG: Y in the item's work area of the reflector buffer (ld > kSmemLd)
-template <int MR, bool KYG>
+// KYG: Y in the item's work area of the reflector buffer (ld > kSmemLd);
+// KVG: V there too (ld > kVSmemLd)
+template <int MR, bool KYG, bool KVG = false>
 __global__ void __launch_bounds__(kThr, 1) sb_kernel(const EigItem* __restrict__ items, double2* __restrict__ hbuf,
                                                     double2* __restrict__ rbuf) {
   const EigItem it = items[blockIdx.x];
@@ -430,15 +458,15 @@ __global__ void __launch_bounds__(kThr, 1) sb_kernel(const EigItem* __restrict__
   extern __shared__ __align__(16) unsigned char smraw[];
   const int mmax = ld - kNB;
   SbSmem S;
-  S.V = reinterpret_cast<double2*>(smraw);
-  S.Y = KYG ? rbuf + it.r_off + band_off(ld) : S.V + (size_t)mmax * kNB;
-  S.T = (KYG ? S.V : S.Y) + (size_t)mmax * kNB;
+  double2* work = rbuf + it.r_off + band_off(ld);
+  S.V = KVG ? work + (size_t)mmax * kNB : reinterpret_cast<double2*>(smraw);
+  S.Y = KYG ? work : S.V + (size_t)mmax * kNB;
+  S.T = KVG ? reinterpret_cast<double2*>(smraw) : (KYG ? S.V : S.Y) + (size_t)mmax * kNB;
   S.M = S.T + kNB * 17;
   S.P = S.M + kNB * 17;
   S.taus = S.P + kNB * 17;
   // the panel QR's work arrays: inside Y (free until Y = A V is formed;
-  // 256 + 32 + 16 MR <= 16 mmax double2 for ld >= 96), or after taus (a
-  // region of their own: sharing V's made the compiler spill the panel)
+  // 256 + 32 + 16 MR <= 16 mmax double2 for ld >= 96), or after taus
   S.part = KYG ? S.taus + kNB : S.Y;
   S.rowj = S.part + 2 * 8 * 16;
   S.pvw = S.rowj + 2 * 16;
@@ -452,7 +480,7 @@ __global__ void __launch_bounds__(kThr, 1) sb_kernel(const EigItem* __restrict__
       A[(size_t)(r0 + j) * ld + c0 + i] = S.T[i * 17 + j];
     }
     // ---- Y = A22 V on the tensor cores
-    pass_y(A, ld, r0, Mt, S.V, S.Y);
+    pass_y<KVG>(A, ld, r0, Mt, S.V, S.Y);
     __syncthreads();
     // ---- X = Y T - 1/2 V (T^H V^H Y T): Y <- Y T row by row (T upper
     // triangular, columns from the right so that the row can be updated in place)
@@ -489,7 +517,7 @@ __global__ void __launch_bounds__(kThr, 1) sb_kernel(const EigItem* __restrict__
     for (int r = tid; r < m; r += kThr) {
       double2 v[kNB];
 #pragma unroll
-      for (int k = 0; k < kNB; ++k) v[k] = S.V[pidx(r, k)];
+      for (int k = 0; k < kNB; ++k) v[k] = ldy<KVG>(S.V + pidx(r, k));
 #pragma unroll
       for (int c = 0; c < kNB; ++c) {
         double2 s = make_double2(0, 0);
@@ -843,10 +871,13 @@ __host__ __device__ inline size_t back_smem_bytes(int ld, int vb) {
 // reflector entries of a sweep that one thread stages (ceil(kMaxLd / 16) * 16 / 256)
 constexpr int kBackStage = (kMaxLd + kThr - 1) / kThr;
 // eigenvectors per back-transform CTA: up to kVecBlock, and few enough that
-// two CTAs share an SM (the stage is latency-bound)
+// two CTAs share an SM (the stage is latency-bound) up to ld = 800
 inline int back_vec_block(int ld, int max_nvec) {
   int vb = std::min(kVecBlock, std::max(max_nvec, 1));
-  while (vb > 1 && back_smem_bytes(ld, vb) > (size_t)112 * 1024) --vb;
+  // beyond ld = 800 one CTA per SM with more vectors each: every CTA reads all
+  // band reflectors (ld^2 / 2 complex) once
+  const size_t lim = (size_t)(ld > kVSmemLd ? 200 : 112) * 1024;
+  while (vb > 1 && back_smem_bytes(ld, vb) > lim) --vb;
   return vb;
 }
 
@@ -1022,12 +1053,13 @@ cudaError_t launch_heev2(const EigItem* items, int nitems, int max_n, int max_nv
   cudaError_t e;
   const int mr = sb_rows(ld);
   const bool big = ld > kSmemLd;  // Y and the band in the reflector buffer's work areas
-  const size_t s1 = sb_smem_bytes(ld, mr, big);
+  const size_t s1 = sb_smem_bytes(ld, mr, big, ld > kVSmemLd);
   auto sb = mr == 9    ? sb_kernel<9, false>
             : mr == 17 ? sb_kernel<17, false>
             : mr == 25 ? sb_kernel<25, false>
             : mr == 36 ? sb_kernel<36, true>
-                       : sb_kernel<49, true>;
+            : mr == 49 ? sb_kernel<49, true>
+                       : sb_kernel<75, true, true>;
   e = cudaFuncSetAttribute(sb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1);
   if (e != cudaSuccess) return e;
   sb<<<nitems, kThr, s1, st>>>(items, hbuf, rbuf);

@@ -434,6 +434,15 @@ cudaError_t eig_launch(pmx_ctx* c, const pmx::dev::EigItem* items, int nitems, i
                                tri);
 }
 
+// H workspace of one chunk of eigensolves: 2 GB, or up to 8 GB where two
+// waves of 148 matrices of the largest size need more (n > 832), so that the
+// large sizes still fill the GPU; 2 GB with the tridiagonal export, whose
+// callers keep their k-points within one chunk of that size
+size_t h_budget(size_t hbytes_max, bool tri) {
+  const size_t base = (size_t)2 << 30;
+  return tri ? base : std::max(base, std::min((size_t)8 << 30, 296 * hbytes_max));
+}
+
 // Assembles and diagonalises H(k) for every k; the lowest nval eigenvalues
 // go to w (host, [nk][nval]); with zdev the lowest nvec eigenvectors go to
 // zdev ([nk][nvec][n]).
@@ -450,7 +459,7 @@ void solve_k(pmx_ctx* c, const DevCrystal& dc, const std::vector<Vec3>& ks, int 
   const bool tri_req = tri != nullptr;
   const int ld = eig_ld(n, n, tri_req);
   const size_t hbytes = (size_t)ld * ld * sizeof(double2);
-  int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)nk, ((size_t)2 << 30) / hbytes));
+  int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)nk, h_budget(hbytes, tri_req) / hbytes));
   chunk = std::min(chunk, 4096);
   if (nk > chunk) {  // several chunks: each a whole number of waves of CTAs
     const int unit = pmx::dev::heev_batch_unit(n, nval);
@@ -2242,7 +2251,7 @@ int heev_class(int n) {
 
 // All requests in one CUDA graph: the requests are sorted by n and cut into
 // chunks of one eigensolver size class (one template instantiation) and at
-// most 2 GB of H; the assembly + eigensolver launches of every chunk are
+// most h_budget bytes of H; the assembly + eigensolver launches of every chunk are
 // captured into a graph, launched once, and the eigenvalues and status codes
 // of all chunks come back in one copy each.
 void solve_multi(pmx_ctx* c, const pmx::dev::CrystalDev* table, std::vector<SolveReq>& reqs, double2* zbase) {
@@ -2255,11 +2264,12 @@ void solve_multi(pmx_ctx* c, const pmx::dev::CrystalDev* table, std::vector<Solv
   };
   std::vector<Chunk> chunks;
   std::vector<pmx::dev::EigItem> items(reqs.size());
-  const size_t hmax = (size_t)2 << 30;
   long long w = 0, hneed = 0, sneed = 0, rneed = 0;
   size_t i0 = 0;
   while (i0 < order.size()) {
     const int max_n = reqs[order[i0]].n, cls = heev_class(max_n);
+    const size_t ld0 = (size_t)eig_ld(max_n, max_n, false);
+    const size_t hmax = h_budget(ld0 * ld0 * sizeof(double2), false);
     size_t i1 = i0, hb = 0;
     while (i1 < order.size() && i1 - i0 < 4096 && heev_class(reqs[order[i1]].n) == cls) {
       const size_t ldi = (size_t)eig_ld(reqs[order[i1]].n, max_n, false);

@@ -104,12 +104,21 @@ def test_heev_all_eigenpairs(ctx, n, nev):
         assert np.max(np.abs(Z[b].conj().T @ Z[b] - np.eye(nev))) < 1e-10
 
 
+@pytest.mark.parametrize("schedule", [0, 1])
 @pytest.mark.parametrize("n,nev,vectors", [(900, 16, True), (1200, 8, True), (1000, 24, False)])
-def test_heev_large_n(ctx, n, nev, vectors):
-    """n > 832: the per-warp partial sums of the reduction live in global scratch."""
+def test_heev_large_n(n, nev, vectors, schedule):
+    """n > 800: schedule 0 is the two-stage solver with stage 1's V and Y in
+    global memory; schedule 1 the one-stage solver, whose per-warp partial
+    sums live in global scratch above n = 832."""
+    from conftest import gpu_available
+    if not gpu_available():
+        pytest.skip("no CUDA device")
     rng = np.random.default_rng(n)
     A = np.stack([_random_hermitian(rng, n) for _ in range(2)])
-    w, Z = ctx.heev(A, nev, vectors=vectors)
+    c = pm.Context(0)
+    c.set_schedule(schedule)
+    w, Z = c.heev(A, nev, vectors=vectors)
+    c.close()
     for b in range(2):
         full = np.linalg.eigvalsh(A[b])
         scale = np.max(np.abs(full))
