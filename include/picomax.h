@@ -237,7 +237,8 @@ int pmx_chi_device(pmx_ctx* ctx, const pmx_problem* p, int sw, int precision, do
                    double* epsm_dev);
 
 /* pmx_chi plus eps_M(q, w) [nq][nfreq][2] of the (L, L) block, as
- * pmx_eps_macroscopic computes it. */
+ * pmx_eps_macroscopic computes it. re and im may both be NULL: eps_M only,
+ * chi stays on the device (no copy-out of the 9 blocks). */
 int pmx_chi_epsm(pmx_ctx* ctx, const pmx_problem* p, int sw, int precision, double* re, double* im, double* epsm);
 
 /* Macroscopic dielectric function eps_M(q, w) = 1 / [eps^-1]_00 with
@@ -308,8 +309,10 @@ int pmx_band_batch(pmx_ctx* ctx, int count, const pmx_problem* const* problems, 
 
 /* pmx_chi (or pmx_chi_epsm when epsm != NULL and epsm[i] != NULL) of
  * problems[0..count) with one switch and precision; re[i]/im[i] as pmx_chi's
- * outputs for problems[i]. Problems are grouped so that the eigenvectors of
- * one group at k and at k+q stay within 2 x 16 GB. */
+ * outputs for problems[i]. Where eps_M is requested, re and im (the arrays, or
+ * both entries i) may be NULL: eps_M only, as for pmx_chi_epsm. Problems are
+ * grouped so that the eigenvectors of one group at k and at k+q stay within
+ * 2 x 16 GB. */
 int pmx_chi_batch(pmx_ctx* ctx, int count, const pmx_problem* const* problems, int sw, int precision,
                   double* const* re, double* const* im, double* const* epsm);
 

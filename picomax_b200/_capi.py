@@ -373,13 +373,15 @@ class Context:
     def occupation_ties(self) -> int:
         return int(self._lib.pmx_ctx_occupation_ties(self.handle))
 
-    def chi_epsm(self, prob: Problem, switch: int, precision: int = PREC_FP64):
+    def chi_epsm(self, prob: Problem, switch: int, precision: int = PREC_FP64, chi: bool = True):
+        """(re, im, eps_M); chi=False: eps_M only (re, im None; chi stays on the device)."""
         n = prob.info.chi_values
-        re = np.zeros(n, np.float64)
-        im = np.zeros(n, np.float64)
+        re = np.zeros(n, np.float64) if chi else None
+        im = np.zeros(n, np.float64) if chi else None
         eps = np.zeros((prob.info.nq, prob.info.nfreq, 2), np.float64)
-        self._check(self._lib.pmx_chi_epsm(self.handle, prob.handle, switch, precision, _dptr(re), _dptr(im),
-                                           _dptr(eps)), "chi_epsm")
+        self._check(self._lib.pmx_chi_epsm(self.handle, prob.handle, switch, precision,
+                                           _dptr(re) if chi else None, _dptr(im) if chi else None, _dptr(eps)),
+                    "chi_epsm")
         return re, im, eps[..., 0] + 1j * eps[..., 1]
 
     def band_batch(self, probs):
@@ -390,15 +392,18 @@ class Context:
         self._check(self._lib.pmx_band_batch(self.handle, len(probs), ph, op), "band_batch")
         return outs
 
-    def chi_batch(self, probs, switch: int, precision: int = PREC_FP64, epsm: bool = False):
-        """pmx_chi(_epsm) of several problems: list of (re, im[, eps_M])."""
+    def chi_batch(self, probs, switch: int, precision: int = PREC_FP64, epsm: bool = False, chi: bool = True):
+        """pmx_chi(_epsm) of several problems: list of (re, im[, eps_M]);
+        chi=False (with epsm): eps_M only, re and im None."""
         n = len(probs)
-        res = [np.zeros(p.info.chi_values, np.float64) for p in probs]
-        ims = [np.zeros(p.info.chi_values, np.float64) for p in probs]
+        if not chi and not epsm:
+            raise ValueError("chi=False needs epsm=True")
+        res = [np.zeros(p.info.chi_values, np.float64) if chi else None for p in probs]
+        ims = [np.zeros(p.info.chi_values, np.float64) if chi else None for p in probs]
         eps = [np.zeros((p.info.nq, p.info.nfreq, 2), np.float64) for p in probs] if epsm else None
         ph = (c_void_p * n)(*[p.handle for p in probs])
-        rp = (POINTER(c_double) * n)(*[_dptr(x) for x in res])
-        ip = (POINTER(c_double) * n)(*[_dptr(x) for x in ims])
+        rp = (POINTER(c_double) * n)(*[_dptr(x) for x in res]) if chi else None
+        ip = (POINTER(c_double) * n)(*[_dptr(x) for x in ims]) if chi else None
         ep = (POINTER(c_double) * n)(*[_dptr(x) for x in eps]) if epsm else None
         self._check(self._lib.pmx_chi_batch(self.handle, n, ph, switch, precision, rp, ip, ep), "chi_batch")
         if epsm:

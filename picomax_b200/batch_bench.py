@@ -14,8 +14,10 @@ Gaussian broadening 0.1 eV, Kramers-Kronig on.
 Two workloads, each timed both ways with CUDA-synchronising calls:
   band: the 121-point high-symmetry path of every crystal
         (pmx_band_batch vs pmx_band per crystal), eigensolve k-points/s;
-  chi:  eps_M spectra of every (crystal, q) (pmx_chi_batch vs pmx_chi per
-        crystal), spectra/s.
+  chi:  eps_M spectra of every (crystal, q) (pmx_chi_batch vs pmx_chi_epsm per
+        crystal), spectra/s, eps_M only (chi stays on the device: what a
+        plasmon dispersion needs), and once more with every chi block copied
+        to host memory (`chi_to_host_s`).
 One JSON line per workload goes to stdout.
 """
 from __future__ import annotations
@@ -149,17 +151,23 @@ def main(argv=None):
                       "per_crystal_kpts_per_s": nk_band / tl, "speedup": tl / tb, "max_abs_diff_eV": diff,
                       "setup_s": t_setup}), flush=True)
 
-    fam = ("solve_graph", "assemble", "heev", "overlap", "contract_mixed", "contract_f64", "scale", "kk")
+    fam = ("solve_graph", "assemble", "heev", "transitions", "overlap", "overlap_tc", "contract_mixed",
+           "contract_f64", "scale", "kk")
     k0 = {f: ctx.kernel_time(f)[0] for f in fam}
-    tb, cb = timed(lambda: ctx.chi_batch(chi, C.SWITCH_EPSLL, prec, epsm=True))
+    tb, cb = timed(lambda: ctx.chi_batch(chi, C.SWITCH_EPSLL, prec, epsm=True, chi=False))
     kms = {f: round((ctx.kernel_time(f)[0] - k0[f]) / a.repeat, 1) for f in fam}
+    x0 = ctx.transfer_bytes()
+    t = time.perf_counter()
+    ctx.chi_batch(chi, C.SWITCH_EPSLL, prec, epsm=True)
+    t_host = time.perf_counter() - t
+    d2h_gb = (ctx.transfer_bytes()[1] - x0[1]) / 1e9
     cuts = []
 
     def loop():
         cuts.clear()
         out = []
         for p in chi:
-            out.append(ctx.chi_epsm(p, C.SWITCH_EPSLL, prec))
+            out.append(ctx.chi_epsm(p, C.SWITCH_EPSLL, prec, chi=False))
             cuts.append(ctx.degenerate_cuts() + ctx.occupation_ties())
         return out
     tl, cl = timed(loop)
@@ -177,7 +185,9 @@ def main(argv=None):
                       "per_crystal_s": tl, "batch_spectra_per_s": spectra / tb,
                       "per_crystal_spectra_per_s": spectra / tl, "speedup": tl / tb,
                       "max_rel_diff_epsM_clean": rel, "crystals_ill_posed": int(sum(c > 0 for c in cuts)),
-                      "batch_kernel_ms": kms, "neps": sorted({m["neps"] for m in meta})}), flush=True)
+                      "batch_kernel_ms": kms, "batch_kernel_sum_s": round(sum(kms.values()) / 1e3, 3),
+                      "chi_to_host_s": t_host, "chi_to_host_d2h_gb": round(d2h_gb, 3),
+                      "neps": sorted({m["neps"] for m in meta})}), flush=True)
     for p in band + chi:
         p.close()
     ctx.close()

@@ -1292,9 +1292,11 @@ void chi_process_q(pmx_ctx* ctx, const Problem& p, const ChiPlan& pl, const DevC
     const double* res = p.kk ? ctx->chi2.as<double>() : ctx->chi.as<double>();
     const size_t row = (size_t)np * nf * sizeof(double);
     const cudaMemcpyKind kind = device_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-    CK(cudaMemcpy2DAsync(re + (size_t)q * np * nf, row * nq, res, row, row, 9, kind, st));
-    CK(cudaMemcpy2DAsync(im + (size_t)q * np * nf, row * nq, res + blkvals, row, row, 9, kind, st));
-    if (!device_out) ctx->d2h += (long long)(2 * 9 * row);
+    if (re) {  // NULL: eps_M only
+      CK(cudaMemcpy2DAsync(re + (size_t)q * np * nf, row * nq, res, row, row, 9, kind, st));
+      CK(cudaMemcpy2DAsync(im + (size_t)q * np * nf, row * nq, res + blkvals, row, row, 9, kind, st));
+      if (!device_out) ctx->d2h += (long long)(2 * 9 * row);
+    }
     if (epsm) {
       // eps_M of this q from the (L, L) block: [i=0][j=0] rows of res
       CK(ctx->epsm.ensure(sizeof(double2) * nf));
@@ -1318,7 +1320,8 @@ static int run_chi(pmx_ctx* ctx, const pmx_problem* P, int sw, int precision, do
     const Problem& p = P->p;
     cudaStream_t st = ctx->stream;
     for (double& t : ctx->stage_ms) t = 0;
-    if (!re || !im) return (int)PMX_ERR_INVALID;
+    // re/im may both be NULL when eps_M is requested (eps_M only, no chi copy-out)
+    if ((!re || !im) && !(epsm && !re && !im)) return (int)PMX_ERR_INVALID;
     DevCrystal dc;
     double off;
     std::vector<double> wk;
@@ -2478,12 +2481,17 @@ extern "C" int pmx_band_batch(pmx_ctx* ctx, int count, const pmx_problem* const*
 
 extern "C" int pmx_chi_batch(pmx_ctx* ctx, int count, const pmx_problem* const* problems, int sw, int precision,
                              double* const* re, double* const* im, double* const* epsm) {
-  if (count < 0 || (count > 0 && (!problems || !re || !im))) return PMX_ERR_INVALID;
+  if (count < 0 || (count > 0 && !problems)) return PMX_ERR_INVALID;
   if (sw != PMX_SWITCH_EPSIJ && sw != PMX_SWITCH_EPSLL && sw != PMX_SWITCH_EPSXYZ) return PMX_ERR_INVALID;
   if (precision != PMX_PREC_FP64 && precision != PMX_PREC_MIXED) return PMX_ERR_INVALID;
   if (epsm && sw == PMX_SWITCH_EPSXYZ) return PMX_ERR_INVALID;
-  for (int i = 0; i < count; ++i)
-    if (!problems[i] || !re[i] || !im[i] || (epsm && epsm[i] && problems[i]->p.neps > 64)) return PMX_ERR_INVALID;
+  for (int i = 0; i < count; ++i) {
+    const bool e = epsm && epsm[i];
+    const double* r = re ? re[i] : nullptr;
+    const double* m = im ? im[i] : nullptr;
+    // chi to host (re and im), or eps_M only (neither, eps_M requested)
+    if (!problems[i] || ((!r || !m) && !(e && !r && !m)) || (e && problems[i]->p.neps > 64)) return PMX_ERR_INVALID;
+  }
   return guarded(ctx, [&]() -> int {
     for (double& t : ctx->stage_ms) t = 0;
     ctx->degenerate_cuts = 0;
@@ -2556,8 +2564,8 @@ extern "C" int pmx_chi_batch(pmx_ctx* ctx, int count, const pmx_problem* const* 
           chi_tables(ctx, p);
           chi_buffers(ctx, pl[i]);
           chi_process_q(ctx, p, pl[i], set.dc[i], q, off[i], wk[i], wq[i], ctx->zk.as<double2>() + zo[i - g0],
-                        ctx->zq.as<double2>() + zo[i - g0], precision, re[i], im[i], false,
-                        epsm ? epsm[i] : nullptr);
+                        ctx->zq.as<double2>() + zo[i - g0], precision, re ? re[i] : nullptr,
+                        im ? im[i] : nullptr, false, epsm ? epsm[i] : nullptr);
         }
       }
       g0 = g1;

@@ -52,3 +52,29 @@ def test_chi_batch_matches_single(ctx, tmp_path, precision):
             assert np.max(np.abs(im - i0)) < tol * scale
     for p in probs:
         p.close()
+
+
+def test_epsm_only_outputs(ctx, tmp_path):
+    """eps_M without the chi copy-out (re/im NULL): the same eps_M as with it,
+    per problem and merged; NULL re with non-NULL im is rejected."""
+    import ctypes
+    import picomax_b200 as pm
+    probs = []
+    for nm in ("si_epsLL", "gaas_soc_epsLL_pv"):
+        (tmp_path / nm).mkdir(exist_ok=True)
+        probs.append(pm.Problem(golden_args(load_golden(nm), tmp_path / nm)))
+    for precision in (0, 1):
+        full = ctx.chi_batch(probs, pm.SWITCH_EPSLL, precision, epsm=True)
+        only = ctx.chi_batch(probs, pm.SWITCH_EPSLL, precision, epsm=True, chi=False)
+        for p, (re, im, e_full), (r2, i2, e_only) in zip(probs, full, only):
+            assert r2 is None and i2 is None
+            assert np.array_equal(e_full, e_only)
+            _, _, e1 = ctx.chi_epsm(p, pm.SWITCH_EPSLL, precision, chi=False)
+            assert np.array_equal(e1, ctx.chi_epsm(p, pm.SWITCH_EPSLL, precision)[2])
+    im = np.zeros(probs[0].info.chi_values)
+    eps = np.zeros((probs[0].info.nq, probs[0].info.nfreq, 2))
+    dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    st = ctx._lib.pmx_chi_epsm(ctx.handle, probs[0].handle, pm.SWITCH_EPSLL, 0, None, dp(im), dp(eps))
+    assert st == pm.PMX_ERR_INVALID
+    for p in probs:
+        p.close()
