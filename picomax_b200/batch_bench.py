@@ -1,6 +1,11 @@
 """Batch of crystals of uneven size: merged launches against one call per crystal.
 
 python -m picomax_b200.batch_bench [--crystals 64] [--grid 4] [--nq 4] [--nfreq 1000] [--precision mixed]
+                                   [--merged-only]
+
+--merged-only times only the merged eps_M-only chi call, once (for the
+configuration's full 12^3 k x 32 q shape, whose eigensolves alone take
+minutes).
 
 The crystals are drawn from one seed: structure zb / rs / wz, lattice constant
 ~ U(4, 6.5) A, atomic form factors ~ U(-0.3, 0.3) Ry on the first |G|^2 shells,
@@ -112,6 +117,28 @@ def build(ncrystal: int, grid: int, nq: int, nfreq: int, workdir: str, seed: int
     return band, chi, meta
 
 
+def merged_only(ctx, chi, meta, prec, a, t_setup):
+    fam = ("solve_graph", "transitions", "overlap", "overlap_tc", "contract_mixed", "contract_f64", "scale", "kk")
+    t = time.perf_counter()
+    out = ctx.chi_batch(chi, C.SWITCH_EPSLL, prec, epsm=True, chi=False)
+    tb = time.perf_counter() - t
+    kms = {f: round(ctx.kernel_time(f)[0], 1) for f in fam}
+    spectra = sum(p.info.nq for p in chi)
+    solves = sum(p.info.nk * (1 + p.info.nq) + 1 for p in chi)
+    finite = all(bool(np.isfinite(e).all()) for (_, _, e) in out)
+    print(json.dumps({"workload": "chi_epsLL_merged", "precision": a.precision, "crystals": len(chi),
+                      "grid": a.grid, "nq": a.nq, "nfreq": a.nfreq, "spectra": spectra, "solves": solves,
+                      "nh_min": min(m["nh"] for m in meta), "nh_max": max(m["nh"] for m in meta),
+                      "batch_s": tb, "batch_spectra_per_s": spectra / tb, "eig_solves_per_s": solves / tb,
+                      "kernel_ms": kms, "kernel_sum_s": round(sum(kms.values()) / 1e3, 3),
+                      "eps_m_finite": finite, "setup_s": t_setup,
+                      "neps": sorted({m["neps"] for m in meta})}), flush=True)
+    for p in chi:
+        p.close()
+    ctx.close()
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--crystals", type=int, default=64)
@@ -120,6 +147,7 @@ def main(argv=None):
     ap.add_argument("--nfreq", type=int, default=1000)
     ap.add_argument("--precision", choices=("fp64", "mixed"), default="mixed")
     ap.add_argument("--repeat", type=int, default=2)
+    ap.add_argument("--merged-only", action="store_true")
     a = ap.parse_args(argv)
     prec = C.PREC_MIXED if a.precision == "mixed" else C.PREC_FP64
     tmp = tempfile.mkdtemp()
@@ -128,6 +156,8 @@ def main(argv=None):
     t_setup = time.perf_counter() - t0
     ctx = C.Context(0)
     nh = [m["nh"] for m in meta]
+    if a.merged_only:
+        return merged_only(ctx, chi, meta, prec, a, t_setup)
     # warm-up (module loading, autotuning of the per-crystal path)
     ctx.band_batch(band[:2])
     for p in band[:2]:
