@@ -27,7 +27,7 @@ typedef enum {
   PMX_ERR_NOCONV = 3,      /* eigensolver did not converge (reference: abort() at src/pmx_epm.cpp:233) */
   PMX_ERR_TIMEOUT = 4,     /* a bounded device wait ran out */
   PMX_ERR_NO_DEVICE = 5,   /* no CUDA device: this library has no CPU path */
-  PMX_ERR_UNSUPPORTED = 6, /* input outside what this build implements */
+  PMX_ERR_UNSUPPORTED = 6, /* input outside what this library implements */
   PMX_ERR_LIMIT = 7        /* size beyond the fixed maximum of pmx_heev_batched_noalloc */
 } pmx_status;
 
@@ -152,14 +152,17 @@ int pmx_ctx_overlap_error(const pmx_ctx* ctx, double* max_abs2_err, double* max_
  * hi*lo and lo*hi counted separately) issued by the mixed contractions of
  * this context so far. New diagnostic (no reference counterpart). */
 int pmx_ctx_mixed_mmas(const pmx_ctx* ctx, long long* mmas);
-/* Autotuner of the batched eigensolver schedule (on by default): the first
- * batch of at least 148 matrices of a given size times every schedule once,
- * keeps the fastest for the rest of the context's life. New in this build. */
+/* Autotuner (on by default): the first batch of at least 148 matrices of a
+ * given size times every eigensolver schedule once, and the first FP64
+ * overlap launch over at least 148 k-points of a given shape times every tile
+ * shape of pmx::dev::overlap_tile_candidates once (all give the same
+ * overlaps); the fastest is kept for the rest of the context's life. No
+ * reference counterpart. */
 int pmx_ctx_set_autotune(pmx_ctx* ctx, int on);
 /* Fixes the eigensolver schedule (0 = direct loads, then the prefetch and
  * shared-memory-partials schedules the matrix size allows; an index beyond
  * the last one means the last) for every later batch; -1 returns to the
- * autotuner. For tests that compare the schedules. New in this build. */
+ * autotuner. For tests that compare the schedules. No reference counterpart. */
 int pmx_ctx_set_schedule(pmx_ctx* ctx, int schedule);
 /* The autotuner's choices and trial times as JSON text (NUL-terminated,
  * truncated at len; full length in *needed). */

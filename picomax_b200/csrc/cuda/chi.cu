@@ -162,6 +162,24 @@ bool overlap_tiles(int ncd_max, int nvd_max, int n, int npw, int& cchunk, int& v
   return overlap_smem_bytes(cchunk, vchunk, n, npw) <= lim;
 }
 
+int overlap_tile_candidates(int ncd_max, int nvd_max, int n, int npw, int* cc, int* vc, int maxc) {
+  int c0 = 1, v0 = 1;
+  if (!overlap_tiles(ncd_max, nvd_max, n, npw, c0, v0) || maxc < 1) return 0;
+  const int cs[2] = {c0, (c0 + 1) / 2}, vs[2] = {v0, (v0 + 1) / 2};
+  int cnt = 0;
+  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 2; ++j) {
+      bool dup = false;
+      for (int q = 0; q < cnt; ++q) dup = dup || (cc[q] == cs[i] && vc[q] == vs[j]);
+      if (!dup && cnt < maxc) {
+        cc[cnt] = cs[i];
+        vc[cnt] = vs[j];
+        ++cnt;
+      }
+    }
+  return cnt;
+}
+
 // ------------------------------------------------------------ broadening
 // src/pmx_chi.cpp:90-164; delta model 0 gauss, 1 lorentz, 2 triangle, 3 rect.
 __device__ __forceinline__ double broaden(int model, double eps, double x) {

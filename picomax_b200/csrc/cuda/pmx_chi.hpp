@@ -129,6 +129,12 @@ size_t overlap_smem_bytes(int cchunk, int vchunk, int n, int npw);
 // Largest conduction / valence chunks whose staged eigenvectors fit 200 KB of
 // shared memory; false when even one of each does not fit.
 bool overlap_tiles(int ncd_max, int nvd_max, int n, int npw, int& cchunk, int& vchunk);
+// Tile shapes the autotuner may try for overlap_kernel (at most maxc): first
+// the largest chunks (overlap_tiles), then those with the conduction and/or
+// valence chunk halved (more CTAs per k-point, fewer eigenvectors staged per
+// CTA, more CTAs per SM). Every shape computes the same M. Returns the count
+// (0: no shape fits).
+int overlap_tile_candidates(int ncd_max, int nvd_max, int n, int npw, int* cc, int* vc, int maxc);
 cudaError_t launch_contract_f64(const ContractArgs& a, cudaStream_t st);
 int contract_ftile();
 cudaError_t launch_scale(const ScaleArgs& s, cudaStream_t st);

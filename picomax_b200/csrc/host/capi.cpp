@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <complex>
@@ -255,6 +256,15 @@ struct pmx_ctx {
                             // 3 tensor cores
   std::map<long long, int> heev_choice;
   std::map<long long, std::vector<float>> heev_trials;
+  // autotuner of the FP64 overlap kernel's tile shape per (n, npw, largest
+  // conduction / valence counts, neps, channels | soc | mode): the shapes tried,
+  // their device times, the chosen one
+  struct OvlTune {
+    int cchunk = 1, vchunk = 1;
+    std::vector<int> cc, vc;
+    std::vector<float> ms;
+  };
+  std::map<std::array<int, 6>, OvlTune> ovl_tune;
   // named workspaces
   DevBuf crystal, g, hkl, vloc, vso, items, hbuf, wbuf, zk, zq, scratch, info, rbuf, kgrid;
   DevBuf loci, kpts, uvec, ssoc, qgn, ncd, nvd, cbase, vbase, cidx, vidx, blkoff, dest;
@@ -1196,6 +1206,41 @@ void chi_process_q(pmx_ctx* ctx, const Problem& p, const ChiPlan& pl, const DevC
     oa.ssoc = ctx->ssoc.as<double2>();
     if (f64_ovl) {
       oa.M = ctx->M.as<double2>();
+      // tile shape: cached per shape key, or timed once on a k grid of at
+      // least 148 points (every candidate computes the same M; the chosen one
+      // runs last)
+      const std::array<int, 6> okey{n, dc.npw, oa.ncd_max, oa.nvd_max, neps, (nch << 4) | (oa.soc << 2) | oa.mode};
+      auto ot = ctx->ovl_tune.find(okey);
+      if (ot != ctx->ovl_tune.end()) {
+        oa.cchunk = ot->second.cchunk;
+        oa.vchunk = ot->second.vchunk;
+      } else if (ctx->autotune && nk >= 148) {
+        int cc[4], vc[4];
+        const int ncand = pmx::dev::overlap_tile_candidates(oa.ncd_max, oa.nvd_max, n, dc.npw, cc, vc, 4);
+        if (ncand > 1) {
+          pmx_ctx::OvlTune t;
+          t.ms.assign(ncand, 0.f);
+          for (int i = 0; i < ncand; ++i) {
+            pmx::dev::OverlapArgs ob = oa;
+            ob.cchunk = cc[i];
+            ob.vchunk = vc[i];
+            CK(cudaEventRecord(ctx->ev[2], st));
+            CK(pmx::dev::launch_overlap(ob, nk, st));
+            CK(cudaEventRecord(ctx->ev[3], st));
+            CK(cudaEventSynchronize(ctx->ev[3]));
+            CK(cudaEventElapsedTime(&t.ms[i], ctx->ev[2], ctx->ev[3]));
+            ctx->launches += 1;
+            t.cc.push_back(cc[i]);
+            t.vc.push_back(vc[i]);
+          }
+          const int best = (int)(std::min_element(t.ms.begin(), t.ms.end()) - t.ms.begin());
+          t.cchunk = cc[best];
+          t.vchunk = vc[best];
+          oa.cchunk = t.cchunk;
+          oa.vchunk = t.vchunk;
+          ctx->ovl_tune[okey] = t;
+        }
+      }
       KTime kt(ctx, "overlap");
       CK(pmx::dev::launch_overlap(oa, nk, st));
       ctx->launches += 1;
@@ -1551,6 +1596,20 @@ extern "C" int pmx_ctx_tuning(const pmx_ctx* c, char* buf, size_t len, size_t* n
     auto t = c->heev_trials.find(key);
     if (t != c->heev_trials.end())
       for (size_t i = 0; i < t->second.size(); ++i) os << (i ? ", " : "") << t->second[i];
+    os << "]}";
+    first = false;
+  }
+  os << "], \"overlap\": [";
+  first = true;
+  for (auto& kv : c->ovl_tune) {
+    const auto& k = kv.first;
+    const auto& t = kv.second;
+    os << (first ? "" : ", ") << "{\"n\": " << k[0] << ", \"npw\": " << k[1] << ", \"ncd_max\": " << k[2]
+       << ", \"nvd_max\": " << k[3] << ", \"neps\": " << k[4] << ", \"cchunk\": " << t.cchunk
+       << ", \"vchunk\": " << t.vchunk << ", \"tiles\": [";
+    for (size_t i = 0; i < t.cc.size(); ++i) os << (i ? ", " : "") << "[" << t.cc[i] << ", " << t.vc[i] << "]";
+    os << "], \"trial_ms\": [";
+    for (size_t i = 0; i < t.ms.size(); ++i) os << (i ? ", " : "") << t.ms[i];
     os << "]}";
     first = false;
   }

@@ -155,7 +155,7 @@ extern "C" int pmx_main(int argc, const char* const* argv) {
   pmx_ctx* ctx = nullptr;
   int st = pmx_ctx_create(0, &ctx);
   if (st != PMX_OK) {
-    std::cout << "ERROR: no usable CUDA device (status " << st << "); this build has no CPU path" << std::endl;
+    std::cout << "ERROR: no usable CUDA device (status " << st << "); this library has no CPU path" << std::endl;
     pmx_problem_destroy(P);
     return 1;
   }

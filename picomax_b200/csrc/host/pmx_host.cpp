@@ -173,7 +173,7 @@ static void init_crystal(const ArgParser& inp, Problem& p) {
     lat.atomic = {{0, 0, 0}, {0.5, 0, 5 * s3}};
   } else {
     // The reference leaves the lattice empty and later reads reciprocal[0]
-    // out of bounds; this build reports the bad preset instead.
+    // out of bounds; this library reports the bad preset instead.
     fail("unknown -crystal '" + lat.name + "' (expected zb, rs, wz, te or hex)");
   }
   inp.fill_int("-gsym", lat.gsym);
@@ -377,7 +377,7 @@ void generate_loci(Problem& p) {
 // Reads the kpointfile format of import_kpt (src/pmx_basis.cpp:200-245):
 // total count, listed count, then "kx ky kz w" per point. The reference
 // leaves the points a short or malformed file does not list at k = 0 with
-// weight 0 and divides by a zero total; this build rejects such files.
+// weight 0 and divides by a zero total; this library rejects such files.
 void import_kpoints(Problem& p) {
   std::ifstream in(p.kpointfile);
   if (!in.is_open()) fail("cannot open kpointfile '" + p.kpointfile + "'");

@@ -78,3 +78,32 @@ def test_epsm_only_outputs(ctx, tmp_path):
     assert st == pm.PMX_ERR_INVALID
     for p in probs:
         p.close()
+
+
+def test_band_batch_large_spin_orbit_sizes(ctx):
+    """Spin-orbit H of n = 2 N_G around 900 next to a small crystal in one
+    merged call: chunks of the two-stage solver beyond shared memory (V and Y
+    in global memory) inside the captured graph, against the per-problem call
+    and the oracle's spectrum."""
+    import picomax_b200 as pm
+    import pmx_oracle as O
+    from picomax_b200.workloads import gaas_form_factors
+    vg, soc = gaas_form_factors()
+    rng = np.random.default_rng(23)
+    K = rng.uniform(-0.5, 0.5, (3, 3))
+    qv = ",".join(f"{x:.6f}" for x in K.ravel())
+    big = ["-switch", "band", "-crystal", "zb", "-a", "5.65", "-vg", vg, "-encut", "275", "-qvec", qv,
+           "-nband", "24", "-nvalence", "8"] + soc
+    small = ["-switch", "band", "-crystal", "zb", "-a", "5.65", "-vg", vg, "-encut", "60", "-qvec", qv,
+             "-nband", "16", "-nvalence", "8"] + soc
+    probs = [pm.Problem(big), pm.Problem(small)]
+    assert 2 * probs[0].info.npw > 832, probs[0].info.npw
+    got = ctx.band_batch(probs)
+    for p, g in zip(probs, got):
+        assert np.max(np.abs(g - ctx.band(p))) < 1e-9
+    cr, mat, gcut, o = O.from_args(big)
+    G, _ = probs[0].gvectors()
+    ref = O.band(cr, mat, G, probs[0].qpoints(), 24, 8)
+    assert np.max(np.abs(got[0] - ref)) < 1e-9
+    for p in probs:
+        p.close()
