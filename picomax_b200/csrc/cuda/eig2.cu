@@ -482,48 +482,78 @@ __global__ void __launch_bounds__(kThr, 1) sb_kernel(const EigItem* __restrict__
     // ---- Y = A22 V on the tensor cores
     pass_y<KVG>(A, ld, r0, Mt, S.V, S.Y);
     __syncthreads();
-    // ---- X = Y T - 1/2 V (T^H V^H Y T): Y <- Y T row by row (T upper
-    // triangular, columns from the right so that the row can be updated in place)
-    for (int r = tid; r < m; r += kThr) {
-      double2 y[kNB];
+    // ---- X = Y T - 1/2 V (T^H V^H Y T) on the tensor cores. X1 = Y T in
+    // place: a warp owns 8-row blocks of Y (A fragments: its rows; B: T);
+    // the lanes' reads of a block end before its writes (__syncwarp)
+    {
+      const int lane = tid & 31, wid = tid >> 5, gr = lane >> 2, gk = lane & 3;
+      for (int I8 = wid; I8 < 2 * Mt; I8 += kNW) {
+        double cr[2][2] = {{0, 0}, {0, 0}}, ci[2][2] = {{0, 0}, {0, 0}};
 #pragma unroll
-      for (int c = 0; c < kNB; ++c) y[c] = ldy<KYG>(S.Y + pidx(r, c));
+        for (int kb = 0; kb < 4; ++kb) {
+          const double2 a = ldy<KYG>(S.Y + pidx(8 * I8 + gr, 4 * kb + gk));
 #pragma unroll
-      for (int c = kNB - 1; c >= 0; --c) {
-        double2 s = make_double2(0, 0);
+          for (int nb = 0; nb < 2; ++nb) cmma(cr[nb], ci[nb], a, S.T[(4 * kb + gk) * 17 + 8 * nb + gr]);
+        }
+        __syncwarp();
 #pragma unroll
-        for (int k = 0; k <= c; ++k) s = cadd(s, cmul(y[k], S.T[k * 17 + c]));
-        y[c] = s;
+        for (int nb = 0; nb < 2; ++nb)
+#pragma unroll
+          for (int i = 0; i < 2; ++i) S.Y[pidx(8 * I8 + gr, 8 * nb + 2 * gk + i)] = make_double2(cr[nb][i], ci[nb][i]);
       }
+      __syncthreads();
+      // M = V^H X1: warp w computes the 8 x 8 block (w & 3) of M over one half
+      // of the rows (w >> 2); the second half's partials pass through P (free
+      // until P = T^H M) and are added by the first half's warps in a fixed
+      // order
+      {
+        const int ib = (wid & 3) >> 1, jb = wid & 1, half = wid >> 2;
+        double cr[2] = {0, 0}, ci[2] = {0, 0};
+        for (int kb = half * 2 * Mt; kb < (half + 1) * 2 * Mt; ++kb) {
+          const int k = 4 * kb + gk;
+          const double2 a = cconj(ldy<KVG>(S.V + pidx(k, 8 * ib + gr)));
+          const double2 b = ldy<KYG>(S.Y + pidx(k, 8 * jb + gr));
+          cmma(cr, ci, a, b);
+        }
+        const int mi = 8 * ib + gr;
+        if (half == 1) {
 #pragma unroll
-      for (int c = 0; c < kNB; ++c) S.Y[pidx(r, c)] = y[c];
-    }
-    __syncthreads();
-    {  // M = V^H Y
-      const int i = tid / kNB, j = tid % kNB;
-      double2 s = make_double2(0, 0);
-#pragma unroll 8
-      for (int r = i; r < m; ++r) s = cadd(s, cmulc(S.V[pidx(r, i)], S.Y[pidx(r, j)]));
-      S.M[i * 17 + j] = s;
-    }
-    __syncthreads();
-    {  // P = T^H M
-      const int i = tid / kNB, j = tid % kNB;
-      double2 s = make_double2(0, 0);
-      for (int k = 0; k <= i; ++k) s = cadd(s, cmulc(S.T[k * 17 + i], S.M[k * 17 + j]));
-      S.P[i * 17 + j] = s;
-    }
-    __syncthreads();
-    for (int r = tid; r < m; r += kThr) {
-      double2 v[kNB];
+          for (int i = 0; i < 2; ++i) S.P[mi * 17 + 8 * jb + 2 * gk + i] = make_double2(cr[i], ci[i]);
+        }
+        __syncthreads();
+        if (half == 0) {
 #pragma unroll
-      for (int k = 0; k < kNB; ++k) v[k] = ldy<KVG>(S.V + pidx(r, k));
+          for (int i = 0; i < 2; ++i) {
+            const double2 o = S.P[mi * 17 + 8 * jb + 2 * gk + i];
+            S.M[mi * 17 + 8 * jb + 2 * gk + i] = make_double2(cr[i] + o.x, ci[i] + o.y);
+          }
+        }
+      }
+      __syncthreads();
+      {  // P = T^H M
+        const int i = tid / kNB, j = tid % kNB;
+        double2 sacc = make_double2(0, 0);
+        for (int k = 0; k <= i; ++k) sacc = cadd(sacc, cmulc(S.T[k * 17 + i], S.M[k * 17 + j]));
+        S.P[i * 17 + j] = sacc;
+      }
+      __syncthreads();
+      // X = X1 - 1/2 V P: each lane updates the entries of its own D fragment
+      for (int I8 = wid; I8 < 2 * Mt; I8 += kNW) {
+        double cr[2][2] = {{0, 0}, {0, 0}}, ci[2][2] = {{0, 0}, {0, 0}};
 #pragma unroll
-      for (int c = 0; c < kNB; ++c) {
-        double2 s = make_double2(0, 0);
+        for (int kb = 0; kb < 4; ++kb) {
+          const double2 a = ldy<KVG>(S.V + pidx(8 * I8 + gr, 4 * kb + gk));
 #pragma unroll
-        for (int k = 0; k < kNB; ++k) s = cadd(s, cmul(v[k], S.P[k * 17 + c]));
-        S.Y[pidx(r, c)] = csub(ldy<KYG>(S.Y + pidx(r, c)), cscale(s, 0.5));
+          for (int nb = 0; nb < 2; ++nb) cmma(cr[nb], ci[nb], a, S.P[(4 * kb + gk) * 17 + 8 * nb + gr]);
+        }
+#pragma unroll
+        for (int nb = 0; nb < 2; ++nb)
+#pragma unroll
+          for (int i = 0; i < 2; ++i) {
+            double2* y = S.Y + pidx(8 * I8 + gr, 8 * nb + 2 * gk + i);
+            const double2 x1 = ldy<KYG>(y);
+            *y = make_double2(x1.x - 0.5 * cr[nb][i], x1.y - 0.5 * ci[nb][i]);
+          }
       }
     }
     __syncthreads();
