@@ -235,7 +235,8 @@ int pmx_chi(pmx_ctx* ctx, const pmx_problem* p, int sw, int precision, double* r
 
 /* pmx_chi with the spectra left in device memory: re_dev/im_dev are device
  * pointers with the same layout; epsm_dev (device, [nq][nfreq][2]) receives
- * eps_M of every (q, w) when non-NULL (requires neps <= 64). */
+ * eps_M of every (q, w) when non-NULL (requires neps <= 64), in which case
+ * re_dev and im_dev may both be NULL (eps_M only). */
 int pmx_chi_device(pmx_ctx* ctx, const pmx_problem* p, int sw, int precision, double* re_dev, double* im_dev,
                    double* epsm_dev);
 
