@@ -679,17 +679,15 @@ __global__ void __launch_bounds__(kS2Thr, 1) sbtrd_kernel(const EigItem* __restr
       if (j == 0) {
         // from column s, rows p .. p + len - 1 (both warps)
         const double2* cs = Bd + (size_t)s * kBandLd + 1;  // A(p + k, s) = cs[k]
-        double xq[4] = {0.0, 0.0, 0.0, 0.0};
+        // |x_1..|^2 over the 16 lanes of a half (lane i holds cs[i])
+        const double2 xi = i < len ? cs[i] : make_double2(0, 0);
+        double xx = i >= 1 ? xi.x * xi.x + xi.y * xi.y : 0.0;
 #pragma unroll
-        for (int k = 1; k < kNB; ++k)
-          if (k < len) {
-            const double2 x = cs[k];
-            xq[k & 3] += x.x * x.x + x.y * x.y;
-          }
-        const Refl Rf = make_refl(cs[0], (xq[0] + xq[1]) + (xq[2] + xq[3]));
+        for (int o = 8; o > 0; o >>= 1) xx += __shfl_xor_sync(0xffffffffu, xx, o);
+        const Refl Rf = make_refl(cs[0], xx);
         tau = Rf.tau;
         beta = Rf.beta;
-        vi = i == 0 ? make_double2(1, 0) : (i < len ? cmul(cs[i], Rf.scal) : make_double2(0, 0));
+        vi = i == 0 ? make_double2(1, 0) : (i < len ? cmul(xi, Rf.scal) : make_double2(0, 0));
         if (h == 0) wv[i] = vi;
         if (!ewarp && h == 0) R[ridx * kNB + i] = i == 0 ? tau : vi;
         __syncwarp();
@@ -724,15 +722,13 @@ __global__ void __launch_bounds__(kS2Thr, 1) sbtrd_kernel(const EigItem* __restr
         y.x += __shfl_xor_sync(0xffffffffu, y.x, 16);
         y.y += __shfl_xor_sync(0xffffffffu, y.y, 16);
         if (h == 0) wv[kNB + i] = y;
-        __syncwarp();
-        // v^H y = v^H D v (real), w = tau y - 1/2 |tau|^2 (v^H y) v
-        double sq[4] = {0.0, 0.0, 0.0, 0.0};
+        // v^H y = v^H D v (real; lane i holds row i's term, summed over the
+        // half's 16 lanes), w = tau y - 1/2 |tau|^2 (v^H y) v
+        double vy = vi.x * y.x + vi.y * y.y;
 #pragma unroll
-        for (int k = 0; k < kNB; ++k) {
-          const double2 yk = wv[kNB + k], vk = vsrc[k];
-          sq[k & 3] += vk.x * yk.x + vk.y * yk.y;
-        }
-        const double al = -0.5 * (tau.x * tau.x + tau.y * tau.y) * ((sq[0] + sq[1]) + (sq[2] + sq[3]));
+        for (int o = 8; o > 0; o >>= 1) vy += __shfl_xor_sync(0xffffffffu, vy, o);
+        __syncwarp();
+        const double al = -0.5 * (tau.x * tau.x + tau.y * tau.y) * vy;
         const double2 w = cadd(cmul(tau, y), cscale(vi, al));
 #pragma unroll
         for (int cc = 0; cc < 8; ++cc) {
@@ -764,15 +760,12 @@ __global__ void __launch_bounds__(kS2Thr, 1) sbtrd_kernel(const EigItem* __restr
         for (int cc = 0; cc < 8; ++cc) e[cc] = csub(e[cc], cmul(tu, cconj(vc[cc])));
         // E's first column x (lane (i, half 0) holds x_i) to every lane
         if (h == 0) wv[kNB + i] = e[0];
-        __syncwarp();
-        double xq[4] = {0.0, 0.0, 0.0, 0.0};
+        // |x_1..|^2: lane (i, half 0) holds x_i = e[0] (zero for i >= len2)
+        double xx = (h == 0 && i >= 1) ? e[0].x * e[0].x + e[0].y * e[0].y : 0.0;
 #pragma unroll
-        for (int k = 1; k < kNB; ++k)
-          if (k < len2) {
-            const double2 x = wv[kNB + k];
-            xq[k & 3] += x.x * x.x + x.y * x.y;
-          }
-        const Refl Rf = make_refl(wv[kNB], (xq[0] + xq[1]) + (xq[2] + xq[3]));
+        for (int o = 16; o > 0; o >>= 1) xx += __shfl_xor_sync(0xffffffffu, xx, o);
+        __syncwarp();
+        const Refl Rf = make_refl(wv[kNB], xx);
         if (h == 0) e[0] = i == 0 ? make_double2(Rf.beta, 0) : make_double2(0, 0);
 #pragma unroll
         for (int cc = 0; cc < 8; ++cc) {
