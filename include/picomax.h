@@ -28,7 +28,8 @@ typedef enum {
   PMX_ERR_TIMEOUT = 4,     /* a bounded device wait ran out */
   PMX_ERR_NO_DEVICE = 5,   /* no CUDA device: this library has no CPU path */
   PMX_ERR_UNSUPPORTED = 6, /* input outside what this library implements */
-  PMX_ERR_LIMIT = 7        /* size beyond the fixed maximum of pmx_heev_batched_noalloc */
+  PMX_ERR_LIMIT = 7,       /* size beyond the fixed maximum of pmx_heev_batched_noalloc, or of pmx_write_npz */
+  PMX_ERR_IO = 8           /* a file could not be written */
 } pmx_status;
 
 typedef enum {
@@ -90,6 +91,19 @@ int pmx_problem_qpoints(const pmx_problem* p, double* Q);
 int pmx_problem_dump(const pmx_problem* p, char* buf, size_t len, size_t* needed);
 /* Writes ${wdir}/${out}.gpt (export_gpt, src/pmx_io.cpp:816-826). */
 int pmx_problem_write_gpt(const pmx_problem* p);
+/* Reusable output in place of the reference's planned HDF5 export
+ * (src/pmx_io.cpp:744-807, commented out there; no HDF5 library here): count
+ * float64 arrays in C order written to path as an uncompressed NumPy .npz
+ * (a ZIP archive of NPY 1.0 files, readable by numpy.load). names[i] is the
+ * array name (".npy" is appended), ndims[i] its rank, shapes the ranks'
+ * extents one array after another. Files beyond 4 GB (no ZIP64) return
+ * PMX_ERR_LIMIT, a failed write PMX_ERR_IO. The CLI writes ${out}.npz with
+ * `-npz 1` (band: eband [nq][nband], qpoints [nq][3]; chi: ReXij and ImXij in
+ * the .dat layout [3][3][nq][neps (neps + 1) / 2][nfreq], pairs [...][2] =
+ * (m, n <= m) of the packed index, freq [nfreq] eV, qvec [nq][3], gvec
+ * [neps][3] in 2 pi / a). No reference counterpart in working code. */
+int pmx_write_npz(const char* path, int count, const char* const* names, const double* const* data, const int* ndims,
+                  const long long* shapes);
 
 /* ---------------------------------------------------------------- context */
 

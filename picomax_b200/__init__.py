@@ -9,6 +9,6 @@ from ._capi import (  # noqa: F401
     KGRID_TIME_REVERSAL, KGRID_LITTLE_GROUP_Q,
     PREC_FP64, PREC_MIXED, SWITCH_BAND, SWITCH_EPSIJ, SWITCH_EPSLL, SWITCH_EPSXYZ, CLI_PATH, LIB_PATH, Context,
     PicomaxError, Problem, load, run_main, PMX_OK, PMX_ERR_INVALID, PMX_ERR_CUDA, PMX_ERR_NOCONV, PMX_ERR_TIMEOUT,
-    PMX_ERR_NO_DEVICE, PMX_ERR_UNSUPPORTED, PMX_ERR_LIMIT)
+    PMX_ERR_NO_DEVICE, PMX_ERR_UNSUPPORTED, PMX_ERR_LIMIT, PMX_ERR_IO, write_npz)
 from .kgrid import gamma_grid, make_kfile, write_kfile  # noqa: F401
 from . import dat  # noqa: F401

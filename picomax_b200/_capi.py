@@ -25,6 +25,7 @@ PMX_ERR_TIMEOUT = 4
 PMX_ERR_NO_DEVICE = 5
 PMX_ERR_UNSUPPORTED = 6
 PMX_ERR_LIMIT = 7
+PMX_ERR_IO = 8
 
 SWITCH_NONE, SWITCH_BAND, SWITCH_EPSIJ, SWITCH_EPSLL, SWITCH_EPSXYZ = 0, 1, 2, 3, 4
 PREC_FP64, PREC_MIXED = 0, 1
@@ -50,6 +51,7 @@ EXPORTS = (
     "pmx_problem_symmetry",
     "pmx_kgrid_reduce",
     "pmx_ctx_set_overlap_mode",
+    "pmx_write_npz",
 )
 
 KGRID_TIME_REVERSAL, KGRID_LITTLE_GROUP_Q = 1, 2
@@ -93,6 +95,7 @@ def load() -> ctypes.CDLL:
         "pmx_problem_qpoints": (c_int, [c_void_p, dp]),
         "pmx_problem_dump": (c_int, [c_void_p, c_char_p, c_size_t, POINTER(c_size_t)]),
         "pmx_problem_write_gpt": (c_int, [c_void_p]),
+        "pmx_write_npz": (c_int, [c_char_p, c_int, POINTER(c_char_p), POINTER(dp), ip, POINTER(c_longlong)]),
         "pmx_ctx_create": (c_int, [c_int, POINTER(c_void_p)]),
         "pmx_ctx_destroy": (None, [c_void_p]),
         "pmx_ctx_last_error": (c_char_p, [c_void_p]),
@@ -480,6 +483,21 @@ class Context:
         rows, nf = re.shape
         self._check(self._lib.pmx_kk(self.handle, rows, nf, dfreq, _dptr(re), _dptr(im)), "kk")
         return re, im
+
+
+def write_npz(path: str, arrays: dict) -> None:
+    """pmx_write_npz: float64 arrays (C order) into an uncompressed .npz."""
+    lib = load()
+    items = [(k, np.require(np.asarray(v, np.float64), requirements="C")) for k, v in arrays.items()]
+    n = len(items)
+    names = (c_char_p * n)(*[k.encode() for k, _ in items])
+    data = (POINTER(c_double) * n)(*[_dptr(a) for _, a in items])
+    nd = np.array([a.ndim for _, a in items], np.int32)
+    shp = np.array([d for _, a in items for d in a.shape] or [0], np.int64)
+    st = lib.pmx_write_npz(path.encode(), n, names, data, _iptr(nd),
+                           shp.ctypes.data_as(POINTER(c_longlong)))
+    if st != PMX_OK:
+        raise PicomaxError(st, "pmx_write_npz")
 
 
 def run_main(args) -> int:

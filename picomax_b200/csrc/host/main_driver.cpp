@@ -3,7 +3,9 @@
 #include <cuda_runtime.h>
 #include <unistd.h>
 
+#include <algorithm>
 #include <chrono>
+#include <vector>
 #include <cstdio>
 #include <cstring>
 #include <ctime>
@@ -94,6 +96,9 @@ extern "C" int pmx_main(int argc, const char* const* argv) {
   }
   int logfile = 0;
   inp.fill_int("-logfile", logfile);
+  // -npz 1: the results also as ${out}.npz (reusable output; see pmx_write_npz)
+  int npz = 0;
+  inp.fill_int("-npz", npz);
   if (logfile) {
     const std::string lf = wdir + "/" + outname + ".log";
     std::cout << "Output is redirected to logfile, " << lf << std::endl;
@@ -177,6 +182,19 @@ extern "C" int pmx_main(int argc, const char* const* argv) {
       } else {
         f.write(reinterpret_cast<const char*>(eb.data()), eb.size() * sizeof(double));
       }
+      if (npz && rc == 0) {
+        std::vector<double> qp((size_t)info.nq * 3);
+        pmx_problem_qpoints(P, qp.data());
+        const char* names[2] = {"eband", "qpoints"};
+        const double* data[2] = {eb.data(), qp.data()};
+        const int nd[2] = {2, 2};
+        const long long shp[4] = {info.nq, std::max(info.nband, 0), info.nq, 3};
+        const std::string zp = wdir + "/" + outname + ".npz";
+        if (pmx_write_npz(zp.c_str(), 2, names, data, nd, shp) != PMX_OK) {
+          std::cout << "ERROR: cannot write " << zp << std::endl;
+          rc = 1;
+        }
+      }
     }
   } else {
     std::cout << "Susceptibility tensor matrix solver" << std::endl;
@@ -199,6 +217,40 @@ extern "C" int pmx_main(int argc, const char* const* argv) {
         f.write(reinterpret_cast<const char*>(im.data()), im.size() * sizeof(double));
         f.close();
         if (pmx_problem_write_gpt(P) != PMX_OK) rc = 1;
+      }
+      if (npz && rc == 0) {
+        // the .dat blocks as [3][3][nq][pairs][nfreq] with their (m, n <= m)
+        // pairs, the frequencies, q vectors and local-field G vectors
+        const long long npair = (long long)info.neps * (info.neps + 1) / 2;
+        std::vector<double> pairs((size_t)npair * 2), freq(std::max(info.nfreq, 0)), qp((size_t)info.nq * 3),
+            G((size_t)info.npw * 3), gl((size_t)info.neps * 3);
+        for (long long m = 0, k = 0; m < info.neps; ++m)
+          for (long long n = 0; n <= m; ++n, ++k) {
+            pairs[2 * k] = (double)m;
+            pairs[2 * k + 1] = (double)n;
+          }
+        for (int f2 = 0; f2 < info.nfreq; ++f2) freq[f2] = info.dfreq * f2;
+        pmx_problem_qpoints(P, qp.data());
+        pmx_problem_gvectors(P, G.data(), nullptr);
+        std::copy(G.begin(), G.begin() + gl.size(), gl.begin());
+        const bool blocks = 9LL * info.nq * npair * info.nfreq == info.chi_values;
+        const char* names[7] = {"ReXij", "ImXij", "pairs", "freq", "qvec", "gvec", nullptr};
+        const double* data[6] = {re.data(), im.data(), pairs.data(), freq.data(), qp.data(), gl.data()};
+        const int r = blocks ? 5 : 1;
+        const int nd[6] = {r, r, 2, 1, 2, 2};
+        std::vector<long long> shp;
+        for (int a = 0; a < 2; ++a) {
+          if (blocks)
+            shp.insert(shp.end(), {3, 3, info.nq, npair, info.nfreq});
+          else
+            shp.push_back(info.chi_values);
+        }
+        shp.insert(shp.end(), {npair, 2, info.nfreq, info.nq, 3, info.neps, 3});
+        const std::string zp = wdir + "/" + outname + ".npz";
+        if (pmx_write_npz(zp.c_str(), 6, names, data, nd, shp.data()) != PMX_OK) {
+          std::cout << "ERROR: cannot write " << zp << std::endl;
+          rc = 1;
+        }
       }
       std::cout << "  Elapsed time: " << std::chrono::duration<double>(clock::now() - ts).count() << " s"
                 << std::endl;
